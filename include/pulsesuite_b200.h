@@ -1,0 +1,229 @@
+/*
+ * pulsesuite_b200.h -- C ABI of the B200 (sm_100a) quantum-wire SBE step.
+ *
+ * Drop-in boundary for the reference's SBE hot path (pulsesuite, pure
+ * Python).  The reference binds its kernels through Python call signatures;
+ * each entry point below names the reference interface it replaces
+ * (file:line, paths relative to the reference project's src/pulsesuite).
+ * The Python facade (pulsesuite_b200/SBEs.py, coulomb.py) binds these with
+ * ctypes, as a maintainer of the reference would.
+ *
+ * Conventions
+ *   - Every function returns PSB_OK (0) or a negative PSB_ERR_* code and never
+ *     aborts; psb_last_error() returns a thread-local message for the last
+ *     failure.
+ *   - Pointers named d_* are device pointers (CUDA global memory on the
+ *     current device); the caller allocates and owns every buffer, and the
+ *     step entry points allocate nothing.
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default).
+ *     Calls are asynchronous with respect to the host unless stated.
+ *   - All arithmetic of the *_f64 entry points is IEEE binary64.
+ *
+ * Diagonal SBE model (what the reference's full-matrix SBEs reduce to when
+ * p, C, D and the drive are diagonal in k; SBEs.py:843-935, 1958-1975,
+ * 2325-2337, 2623-2636):
+ *   Omega_k = M(t) + sum_{k'!=k} Veh(|k-k'|) p_k'
+ *   Se_k    = Ee_k + gap - sum_{k'!=k} Vee(|k-k'|) ne_k'
+ *   Sh_k    = Eh_k       - sum_{k'!=k} Vhh(|k-k'|) nh_k'
+ *   i hbar dp_k/dt  = (Se_k+Sh_k) p_k - Omega_k (ne_k+nh_k) + Omega_k - i hbar gamma p_k
+ *   i hbar dne_k/dt = i hbar dnh_k/dt = Omega_k p_k^* - Omega_k^* p_k
+ *   M(t) = -mscale * E(t)
+ * V(q) may be statically screened per wire and per right-hand-side
+ * evaluation: V_n(q) <- V_n(q) / eps(q; n1D)  (coulomb.py:1195-1230).
+ */
+#ifndef PULSESUITE_B200_H
+#define PULSESUITE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PSB_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+#define PSB_OK 0
+#define PSB_ERR_INVALID (-1)     /* bad argument (null pointer, bad size)      */
+#define PSB_ERR_CUDA (-2)        /* CUDA runtime error (message in last_error)  */
+#define PSB_ERR_SIZE (-3)        /* size beyond the supported maximum           */
+#define PSB_ERR_NONFINITE (-4)   /* per-wire status: state became NaN/Inf       */
+#define PSB_ERR_UNSUPPORTED (-5) /* feature not available on this device/build  */
+
+/* Largest k grid one wire may have (one CTA holds a wire's state). */
+#define PSB_MAX_NK 1024
+
+/* ---- table flags --------------------------------------------------------- */
+#define PSB_TAB_EXCITONS 1 /* include the Hartree-Fock exchange sums (mb.params Excitons) */
+#define PSB_TAB_SCREENED 2 /* screen V per wire and per RHS (mb.params Screened)         */
+
+/*
+ * One k grid with its Coulomb/energy tables.  The doubles live in a packed
+ * device array `tabdata`, starting at `off`, each block nk long:
+ *   [0] Veh(q)  [1] Vee(q)  [2] Vhh(q)   q = index distance 0..nk-1
+ *       (the q = 0 entry is never used: the reference excludes q = 0,
+ *        SBEs.py:829-834, 876-878)
+ *   [3] Ee(k)   [4] Eh(k)                band energies (J), SBEs.py:4834-4835
+ *   [5] chi_e(q) [6] chi_h(q) [7] qe(q) [8] qh(q)
+ *       screening blocks, read only with PSB_TAB_SCREENED
+ *       (coulomb.py:302-333 MakeQs and 580-630 CalcChi1D at [q, 0]).
+ */
+typedef struct PsbTable {
+  int32_t nk;       /* k points (even, 2..PSB_MAX_NK)                              */
+  int32_t flags;    /* PSB_TAB_*                                                   */
+  int64_t off;      /* offset (doubles) of this table's blocks in tabdata          */
+  double L;         /* wire length (m): n1D = sum_k(ne_k+nh_k)/2/L (coulomb.py:1221) */
+  double dens_max;  /* n1D clamp min(qe[1,1],qh[1,1])/pi*0.99 (coulomb.py:1222)    */
+} PsbTable;
+
+/*
+ * One wire.  The wire's k block occupies state elements [off, off+nk) of
+ * the packed state, each element 4 doubles {p_re, p_im, ne, nh}.
+ * Analytic drive (RK4 entry points):
+ *   E(t) = sum_{j<npulse} amp_j exp(-4 ln2 (t-t0_j)^2 / fwhm_j^2) exp(i phase_j)
+ * The leapfrog entry point takes sampled E(t_n) instead (field array).
+ */
+typedef struct PsbWire {
+  int32_t table;     /* index of this wire's PsbTable                               */
+  int32_t npulse;    /* Gaussian pulses in the analytic drive, 0..2                 */
+  int64_t off;       /* first state element of this wire                            */
+  double gap;        /* energy added to Ee (J); rotating frame: gap - hbar*omega_L  */
+  double gamma;      /* gam_e + gam_h (1/s); dephasing of p (SBEs.py:1974)           */
+  double mscale;     /* M_k(t) = -mscale * E(t)                                     */
+  double pscale;     /* P(t) = pscale * sum_k p_k                                   */
+  double t;          /* time (s) at the start of the next step; advanced by calls   */
+  double amp[2];     /* pulse amplitudes (V/m)                                      */
+  double t0[2];      /* pulse centres (s)                                           */
+  double fwhm[2];    /* pulse intensity FWHM of the field envelope (s)              */
+  double phase[2];   /* pulse carrier-envelope phases (rad)                         */
+  int64_t p_off;     /* first P(t) record (complex sample) of this wire             */
+  int32_t status;    /* PSB_OK, or PSB_ERR_NONFINITE once the state is not finite   */
+  int32_t steps;     /* steps taken so far; indexes the P(t) record                  */
+} PsbWire;
+
+/* Model constants shared by every wire of a call. */
+typedef struct PsbModel {
+  double hbar;       /* reduced Planck constant (J s)                               */
+  int32_t flags;     /* reserved, 0                                                 */
+  int32_t reserved;
+} PsbModel;
+
+/* ---- library ------------------------------------------------------------ */
+int psb_abi_version(void);
+/* Message of the last failing call on this thread ("" when none). */
+const char* psb_last_error(void);
+/* Compute capability of the current device, e.g. 100 for sm_100a. */
+int psb_device_arch(int* arch);
+
+/* ---- Coulomb tables (init-time, FP64) ------------------------------------ */
+/*
+ * Unscreened 1D Coulomb matrix elements with Gaussian confinement,
+ *   out[i] = prefactor * Vint(qy[i], y, alpha1, alpha2, delta0)
+ * Replaces coulomb.py:69-104 (_Vint_jit, with its _K03_jit Bessel
+ * approximation, coulomb.py:38-66) as called by CalcCoulombArrays
+ * (coulomb.py:548-557).  prefactor = e^2/(2 pi eps0 epsr L).
+ */
+int psb_coulomb_vint(const double* d_qy, int nq, const double* d_y, int ny, double alpha1,
+                     double alpha2, double delta0, double prefactor, double* d_out,
+                     void* stream);
+/*
+ * Regularised wire potential out[i] = prefactor * K0(|q_i| * radius)
+ * (K0 by the Zhang & Jin series/asymptotic method that the reference's
+ * K03 uses, usefulsubs.py:1669-1820).  Entries with q_i == 0 are set to 0.
+ */
+int psb_coulomb_k0(const double* d_q, int nq, double radius, double prefactor, double* d_out,
+                   void* stream);
+/*
+ * 1D susceptibility at momentum transfers qc[i] (already clamped at alpha/2,
+ * coulomb.py:325-331): out[i] = scale * mass * K03(qc[i]*R)/qc[i] with
+ * R = sqrt((2/alpha)^2 + delta0^2).  Replaces CalcChi1D (coulomb.py:580-630).
+ */
+int psb_chi1d(const double* d_qc, int nq, double alpha, double delta0, double mass,
+              double scale, double* d_out, void* stream);
+/*
+ * Static screening of every wire for its current densities:
+ *   d_eps[w*ldeps + q] = eps(q; n1D_w), q < nk of the wire's table,
+ * n1D_w = min(sum_k(ne+nh)/(2L), dens_max).  Replaces Eps1D / the
+ * screening branch of CalcScreenedArrays (coulomb.py:1172-1193, 1218-1230).
+ */
+int psb_screen_f64(const PsbTable* d_tables, int ntab, const double* d_tabdata,
+                   const PsbWire* d_wires, int nw, const double* d_y, double* d_eps, int ldeps,
+                   void* stream);
+
+/* ---- SBE right-hand side and steps (FP64) -------------------------------- */
+/*
+ * Shared arguments of the SBE entry points:
+ *   d_tables[ntab], d_tabdata[n_tabdata]  device tables (PsbTable doc)
+ *   d_wires[nw]                           device wire descriptors (PsbWire doc)
+ *   d_order                               optional processing order (int32[nw],
+ *                                         a permutation; largest grids first
+ *                                         balances uneven batches), or NULL
+ *   d_y (and d_y1)                        packed state, n_state elements of
+ *                                         4 doubles {p_re, p_im, ne, nh}
+ *   nkmax                                 largest table nk (sizes shared memory)
+ *   screened                              nonzero if any table has
+ *                                         PSB_TAB_SCREENED
+ * Descriptors are validated on the device: a wire whose table index, grid
+ * size or state range is invalid is skipped and its status set to
+ * PSB_ERR_INVALID / PSB_ERR_SIZE.  A wire whose state stops being finite gets
+ * PSB_ERR_NONFINITE; other wires of the launch are unaffected (each wire's
+ * arithmetic is independent of its neighbours, so results are bitwise the
+ * same alone and in any batch).
+ */
+
+/*
+ * Right-hand side of every wire at the wire's own t: d_dy = f(t_w, d_y).
+ * Replaces the diagonal action of CalcH + dpdt + dCdt + dDdt
+ * (SBEs.py:669-935, 1850-1975, 2221-2337, 2513-2636) including the per-call
+ * screening of _preparation (SBEs.py:5185-5238).
+ */
+int psb_rhs_f64(const PsbTable* d_tables, int ntab, const double* d_tabdata, int64_t n_tabdata,
+                const PsbWire* d_wires, int nw, const double* d_y, double* d_dy,
+                int64_t n_state, int nkmax, int screened, const PsbModel* model, void* stream);
+/*
+ * nsteps classical RK4 steps of size dt on every wire, in the stage order of
+ * the reference integrator (libpulsesuite/integrator.py:143-157, rk4_dpc),
+ * the whole step fused in one kernel with the wire's state resident on chip.
+ * Advances each wire's t and steps.  Every p_stride-th step (counted by the
+ * wire's `steps`) writes P(t) = pscale * sum_k p_k to
+ * d_P[p_off + steps/p_stride - 1] (complex: 2 doubles) while that index is
+ * < p_cap and inside d_P[0, n_P) (qwoptics.py:815-946, diagonal form).
+ */
+int psb_rk4_f64(const PsbTable* d_tables, int ntab, const double* d_tabdata, int64_t n_tabdata,
+                PsbWire* d_wires, int nw, const int32_t* d_order, double* d_y, int64_t n_state,
+                int nkmax, int screened, int nsteps, double dt, double* d_P, int64_t n_P,
+                int p_stride, int p_cap, const PsbModel* model, void* stream);
+/*
+ * nsteps steps of the reference's own integrator (SBEs.py:5681-5718):
+ *   X3 = X1 + 2 dt f(X2);  ne3 = |ne3|, nh3 = |nh3| rescaled to a common
+ *   total;  X1 <- (X1 + X3)/2;  X2 <- X3.
+ * d_y1 / d_y2 are the two stored levels (YY2/CC2/DD2 and YY3/CC3/DD3 of
+ * SBESolver, SBEs.py:5073-5092).  The drive of a wire's step n is the
+ * sampled field d_field[w*field_stride + 2*steps_n] (re, im; n_field doubles
+ * in all), the q = 0 component the reference passes as Ey[NQ0] to CalcMeh
+ * (SBEs.py:5165-5175).  P(t) of the new level X3 is recorded as in
+ * psb_rk4_f64 (QWPolarization3 of p3, SBEs.py:5729-5742).
+ */
+int psb_leapfrog_f64(const PsbTable* d_tables, int ntab, const double* d_tabdata,
+                     int64_t n_tabdata, PsbWire* d_wires, int nw, const int32_t* d_order,
+                     double* d_y1, double* d_y2, int64_t n_state, int nkmax, int screened,
+                     const double* d_field, int64_t field_stride, int64_t n_field, int nsteps,
+                     double dt, double* d_P, int64_t n_P, int p_stride, int p_cap,
+                     const PsbModel* model, void* stream);
+/* Dynamic shared memory (bytes) one CTA of the FP64 step kernels uses for a
+ * grid of nk points (for capacity planning). */
+int psb_f64_smem_bytes(int nk);
+
+/* ---- measurement --------------------------------------------------------- */
+/*
+ * FP64 FMA throughput of the current device: runs an in-register FMA loop
+ * (iters per thread) on blocks x 256 threads and returns the elapsed device
+ * time in *ms (CUDA events on `stream`).  Flops = 2 * 8 * iters * blocks * 256.
+ * Used as the measured FP64 roofline peak.
+ */
+int psb_probe_fp64_fma(int blocks, int iters, double* d_sink, float* ms, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PULSESUITE_B200_H */

@@ -1,0 +1,404 @@
+"""Generate the golden vectors of tests/golden by running the reference itself.
+
+Run in a container that holds the reference source (default
+/root/reference/src, override with PULSESUITE_REF_SRC):
+
+    python tests/golden/make_golden.py            # small cases (a minute)
+    python tests/golden/make_golden.py --full-c0  # + the 4000-step Nk=128 RK4 run (~10 min)
+
+The reference does not import cleanly in this image, so three shims are set
+up first, exactly the minimum needed:
+  * ``pyfftw`` is absent: a package mapping ``pyfftw.interfaces.numpy_fft`` to
+    ``numpy.fft`` with a no-op ``cache.enable()`` (FFTs are off the diagonal
+    SBE path);
+  * ``pulsesuite.PSTD3D.benchmark`` does not exist in the reference but the
+    legacy path imports it: a stub module;
+  * numba 0.65 mis-compiles the parallel ``_CalcH_jit`` (it drops the exchange
+    sums); it is replaced by the serial compile of its own Python source,
+    checked against the reference's ``_CalcH_fallback`` before use.
+Numba-CUDA / CuPy are disabled (PULSESUITE_USE_CUDA=0): the goldens are the
+reference's Numba CPU path.
+
+Cases (all stored as .npz next to this script):
+  tables_*.npz    reference Coulomb V(q), chi1D, qe/qh, Eps1D, screened VC
+  rhs_*.npz       CalcH + dpdt/dCdt/dDdt on random diagonal states
+  rk4_*.npz       reference RHS integrated by libpulsesuite.integrator.rk4_dpc
+                  (rotating-frame drive, the benchmark configurations' physics)
+  leapfrog_*.npz  SBESolver._sbe_calculator, the reference's own driver
+"""
+
+import argparse
+import os
+import sys
+import tempfile
+import time
+import types
+
+os.environ["PULSESUITE_USE_CUDA"] = "0"
+_TMP = tempfile.mkdtemp(prefix="psb_golden_")
+os.environ.setdefault("NUMBA_CACHE_DIR", os.path.join(_TMP, "numba_cache"))
+
+import numpy as np  # noqa: E402
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, REPO)
+
+from pulsesuite_b200 import grid as pgrid  # noqa: E402
+
+REF_SRC = os.environ.get("PULSESUITE_REF_SRC", "/root/reference/src")
+
+
+def import_reference():
+    shim = os.path.join(_TMP, "shim")
+    os.makedirs(os.path.join(shim, "pyfftw", "interfaces"), exist_ok=True)
+    with open(os.path.join(shim, "pyfftw", "__init__.py"), "w") as f:
+        f.write("from . import interfaces\n")
+    with open(os.path.join(shim, "pyfftw", "interfaces", "__init__.py"), "w") as f:
+        f.write("import numpy.fft as numpy_fft\n\n\nclass cache:\n"
+                "    enable = staticmethod(lambda: None)\n")
+    sys.path.insert(0, shim)
+    sys.path.insert(0, REF_SRC)
+    bench = types.ModuleType("pulsesuite.PSTD3D.benchmark")
+    bench.profile_start = time.perf_counter
+    bench.profile_record = lambda name, t0: None
+    sys.modules["pulsesuite.PSTD3D.benchmark"] = bench
+
+    import numba
+
+    from pulsesuite.libpulsesuite import integrator
+    from pulsesuite.PSTD3D import SBEs, coulomb, qwoptics, usefulsubs
+
+    SBEs._CalcH_jit = numba.njit(parallel=False)(SBEs._CalcH_jit.py_func)
+    _selftest_calch(SBEs)
+    return types.SimpleNamespace(SBEs=SBEs, coulomb=coulomb, usefulsubs=usefulsubs,
+                                 qwoptics=qwoptics, integrator=integrator)
+
+
+def _selftest_calch(SBEs):
+    rng = np.random.default_rng(7)
+    nk = 16
+    for lf in (False, True):
+        args = [rng.standard_normal((nk, nk)) + 1j * rng.standard_normal((nk, nk))
+                for _ in range(6)]
+        VC = rng.standard_normal((nk, nk, 3))
+        Ee, Eh = rng.standard_normal(nk), rng.standard_normal(nk)
+        outs = []
+        for fn in (SBEs._CalcH_jit, SBEs._CalcH_fallback):
+            H = [np.zeros((nk, nk), complex) for _ in range(3)]
+            fn(*args, VC, *H, nk, Ee, Eh, 0.3, True, lf, False)
+            outs.append(H)
+        for a, b in zip(*outs):
+            if np.max(np.abs(a - b)) > 1e-12 * max(1.0, np.max(np.abs(b))):
+                raise RuntimeError("patched _CalcH_jit disagrees with _CalcH_fallback")
+
+
+def kkp_of(kr, dkr, NQ0):
+    nk = kr.size
+    kkp = np.zeros((nk, nk), dtype=int)
+    for k in range(nk):
+        for kp in range(nk):
+            kkp[k, kp] = int(np.round((kr[k] - kr[kp]) / dkr)) + NQ0
+    return kkp
+
+
+def reference_coulomb(R, g):
+    """Reference Coulomb arrays of one reference grid, column [:, 0]."""
+    c = R.coulomb
+    nr = g.y.size
+    Qr = R.SBEs.GetKArray(nr, 2 * g.L)
+    Qr = np.roll(Qr, nr // 2)
+    Qr[0] = -Qr[0]
+    NQ0 = R.usefulsubs.GetArray0Index(Qr)
+    kkp = kkp_of(g.kr, g.dk, NQ0)
+    Veh0, Vee0, Vhh0 = c.CalcCoulombArrays(g.y, g.kr, g.epsr, g.alphae, g.alphah, g.L,
+                                           g.delta0, Qr, kkp)
+    qe, qh = c.MakeQs(g.kr, g.alphae, g.alphah)
+    Chi1De, Chi1Dh = c.CalcChi1D(g.kr, g.alphae, g.alphah, g.delta0, g.epsr, g.me, g.mh, qe, qh)
+    inst = object.__new__(c.CoulombModule)
+    inst.qe, inst.qh, inst.Chi1De, inst.Chi1Dh = qe, qh, Chi1De, Chi1Dh
+    inst.Veh0, inst.Vee0, inst.Vhh0 = Veh0, Vee0, Vhh0
+    return inst, Qr, NQ0, kkp
+
+
+def reference_k0_vc(R, g):
+    """VC[:, :, n] whose [q, 0] column is the synthetic wire's V(q) (K0 via
+    the reference's own K03 = cik01)."""
+    nk = g.nk
+    v = np.array([0.0] + [g.vprefactor * R.usefulsubs.K03(abs(g.kr[q] - g.kr[0]) * g.radius)
+                          for q in range(1, nk)])
+    VC = np.zeros((nk, nk, 3))
+    for n in range(3):
+        VC[:, 0, n] = v
+    return VC, v
+
+
+def ref_rhs(R, nk, Ee, Eh, gap, VC, M, p, ne, nh, gamma):
+    """Reference diagonal RHS: patched CalcH + dpdt/dCdt/dDdt."""
+    S = R.SBEs
+    Meh = np.diag(np.full(nk, M, dtype=complex))
+    C = np.diag(ne.astype(complex))
+    D = np.diag(nh.astype(complex))
+    P = np.diag(p.astype(complex))
+    Heh, Hee, Hhh = (np.zeros((nk, nk), complex) for _ in range(3))
+    Z = np.zeros((nk, nk), complex)
+    S._CalcH_jit(Meh, Z, Z, C, D, P, VC, Heh, Hee, Hhh, nk, Ee, Eh, gap, True, False, False)
+    G = np.full(nk, gamma / 2.0)
+    hb = S.hbar
+    dp = S._dpdt_jit(C, D, P, Heh, Hee, Hhh, G, G, Z, 1j, hb)
+    dC = S._dCdt_jit(C, D, P, Heh, Hee, Hhh, G, G, Z, 1j, hb)
+    dD = S._dDdt_jit(C, D, P, Heh, Hee, Hhh, G, G, Z, 1j, hb)
+    off = max(np.max(np.abs(dp - np.diag(np.diag(dp)))), np.max(np.abs(dC - np.diag(np.diag(dC)))))
+    return np.diag(dp).copy(), np.diag(dC).copy(), np.diag(dD).copy(), off
+
+
+def grid_meta(g):
+    return dict(nk=g.nk, dk=g.dk, kr=g.kr, L=g.L, me=g.me, mh=g.mh, epsr=g.epsr,
+                delta0=g.delta0, alphae=g.alphae, alphah=g.alphah, radius=g.radius,
+                gap=g.gap, dcv=g.dcv, ehint=g.ehint, area=g.area)
+
+
+# ----------------------------------------------------------------------------
+def make_tables(R, out):
+    rng = np.random.default_rng(11)
+    for L in (2.85e-8, 1e-7):
+        g = pgrid.reference_grid(L=L)
+        inst, Qr, NQ0, kkp = reference_coulomb(R, g)
+        ne = rng.uniform(0, 0.3, g.nk)
+        nh = rng.uniform(0, 0.3, g.nk)
+        VC = np.zeros((g.nk, g.nk, 3))
+        E1D = np.zeros((g.nk, g.nk))
+        inst.CalcScreenedArrays(True, g.L, ne.astype(complex), nh.astype(complex), VC, E1D)
+        dens = [1e5, 1e7, 0.5 * g.dens_max * np.pi]
+        eps = np.array([inst.Eps1D(d)[:, 0] for d in dens])
+        np.savez_compressed(
+            os.path.join(out, f"tables_ref_nk{g.nk}.npz"), **grid_meta(g), y=g.y, Qr=Qr,
+            NQ0=NQ0, Veh=inst.Veh0[:, 0], Vee=inst.Vee0[:, 0], Vhh=inst.Vhh0[:, 0],
+            chie=inst.Chi1De[:, 0], chih=inst.Chi1Dh[:, 0], qe=inst.qe[:, 0], qh=inst.qh[:, 0],
+            dens=np.array(dens), eps=eps, ne=ne, nh=nh, VCs=VC[:, 0, :].copy(),
+            E1D=E1D[:, 0].copy())
+        print(f"tables_ref_nk{g.nk}: done")
+    # K0 of the reference (cik01) at a spread of arguments
+    xs = np.concatenate([np.geomspace(1e-6, 1.0, 40), np.linspace(1.0, 99.0, 120)])
+    k0 = np.array([R.usefulsubs.K03(x) for x in xs])
+    k03j = np.array([R.coulomb._K03_jit(x) for x in xs])
+    np.savez_compressed(os.path.join(out, "k0_ref.npz"), x=xs, K03=k0, K03_jit=k03j)
+    print("k0_ref: done")
+
+
+def make_rhs(R, out):
+    rng = np.random.default_rng(12)
+    cases = []
+    for nk in (16, 32, 64, 128):
+        g = pgrid.wire_grid(nk)
+        VC, v = reference_k0_vc(R, g)
+        cases.append(("k0", g, VC, v, None))
+    gr = pgrid.reference_grid(L=2.85e-8)
+    inst, *_ = reference_coulomb(R, gr)
+    cases.append(("ref", gr, None, None, inst))
+    for kind, g, VC, v, inst in cases:
+        nk = g.nk
+        p = 0.05 * (rng.standard_normal(nk) + 1j * rng.standard_normal(nk))
+        ne = rng.uniform(0, 0.2, nk)
+        nh = rng.uniform(0, 0.2, nk)
+        M = complex(rng.standard_normal(), rng.standard_normal()) * 1e-21
+        gap = float(rng.uniform(-0.05, 0.05)) * 1.602176634e-19
+        gamma = 1.0 / 100e-15
+        if kind == "ref":
+            VC = np.zeros((nk, nk, 3))
+            E1D = np.zeros((nk, nk))
+            inst.CalcScreenedArrays(False, g.L, ne.astype(complex), nh.astype(complex), VC, E1D)
+            VCs = np.zeros((nk, nk, 3))
+            inst.CalcScreenedArrays(True, g.L, ne.astype(complex), nh.astype(complex), VCs, E1D)
+            dps, dCs, dDs, offs = ref_rhs(R, nk, g.Ee, g.Eh, gap, VCs, M, p, ne, nh, gamma)
+        dp, dC, dD, off = ref_rhs(R, nk, g.Ee, g.Eh, gap, VC, M, p, ne, nh, gamma)
+        extra = {}
+        if kind == "ref":
+            extra = dict(dp_s=dps, dC_s=dCs, dD_s=dDs, VCs=VCs[:, 0, :].copy(),
+                         chie=inst.Chi1De[:, 0], chih=inst.Chi1Dh[:, 0])
+        np.savez_compressed(
+            os.path.join(out, f"rhs_{kind}_nk{nk}.npz"), **grid_meta(g), VC=VC[:, 0, :].copy(),
+            p=p, ne=ne, nh=nh, M=M, gap_eff=gap, gamma=gamma, dp=dp, dC=dC, dD=dD,
+            offdiag=off, **extra)
+        print(f"rhs_{kind}_nk{nk}: off-diagonal |d/dt| = {off:.1e}")
+
+
+def rwa_case(nk, nsteps, theta=0.5 * np.pi, fwhm=50e-15, T2=100e-15, det_meV=0.0,
+             dt=1e-15, screened=False):
+    g = pgrid.wire_grid(nk)
+    mscale = g.ehint * g.dcv / 2.0
+    amp = pgrid.gaussian_amplitude(theta, fwhm, mscale)
+    return dict(g=g, nsteps=nsteps, dt=dt, amp=amp, t0=3.0 * fwhm, fwhm=fwhm, mscale=mscale,
+                gamma=1.0 / T2, gap_eff=-det_meV * 1e-3 * 1.602176634e-19, screened=screened)
+
+
+def make_rk4(R, out, name, case):
+    """Oracle A: reference RHS kernels + reference rk4_dpc (SURVEY harness)."""
+    g = case["g"]
+    nk = g.nk
+    S = R.SBEs
+    Ee, Eh = g.Ee, g.Eh
+    VC0, v = reference_k0_vc(R, g)
+    inst = None
+    if case["screened"]:
+        qe, qh = R.coulomb.MakeQs(g.kr, g.alphae, g.alphah)
+        Chi1De, Chi1Dh = R.coulomb.CalcChi1D(g.kr, g.alphae, g.alphah, g.delta0, g.epsr, g.me,
+                                             g.mh, qe, qh)
+        inst = object.__new__(R.coulomb.CoulombModule)
+        inst.qe, inst.qh, inst.Chi1De, inst.Chi1Dh = qe, qh, Chi1De, Chi1Dh
+        inst.Veh0 = VC0[:, :, 0]
+        inst.Vee0 = VC0[:, :, 1]
+        inst.Vhh0 = VC0[:, :, 2]
+    amp, t0, fwhm, mscale = case["amp"], case["t0"], case["fwhm"], case["mscale"]
+    gamma, gap = case["gamma"], case["gap_eff"]
+
+    def D(t, y):
+        p, ne, nh = y[:nk], y[nk:2 * nk].real, y[2 * nk:].real
+        E = amp * np.exp(-4.0 * np.log(2.0) * ((t - t0) / fwhm) ** 2)
+        M = -mscale * E
+        VC = VC0
+        if inst is not None:
+            VC = np.zeros((nk, nk, 3))
+            E1D = np.zeros((nk, nk))
+            inst.CalcScreenedArrays(True, g.L, ne.astype(complex), nh.astype(complex), VC, E1D)
+        dp, dC, dD, _ = ref_rhs(R, nk, Ee, Eh, gap, VC, M, p, ne, nh, gamma)
+        return np.concatenate([dp, dC, dD])
+
+    y = np.zeros(3 * nk, dtype=complex)
+    t = 0.0
+    P = np.zeros(case["nsteps"], dtype=complex)
+    pscale = g.pscale
+    t_start = time.time()
+    for n in range(case["nsteps"]):
+        dydt = D(t, y)
+        t = R.integrator.rk4_dpc(y, dydt, t, case["dt"], D)
+        P[n] = pscale * np.sum(y[:nk])
+    el = time.time() - t_start
+    np.savez_compressed(os.path.join(out, f"{name}.npz"), **grid_meta(g), V=v, amp=amp, t0=t0,
+                        fwhm=fwhm, mscale=mscale, gamma=gamma, gap_eff=gap, dt=case["dt"],
+                        nsteps=case["nsteps"], screened=case["screened"], P=P, p=y[:nk],
+                        ne=y[nk:2 * nk].real, nh=y[2 * nk:].real, imag_n=np.max(np.abs(
+                            y[nk:].imag)), pscale=pscale, seconds=el)
+    print(f"{name}: {case['nsteps']} steps in {el:.1f} s, max|P| = {np.max(np.abs(P)):.3e}, "
+          f"max ne = {np.max(y[nk:2 * nk].real):.3e}")
+
+
+QW_PARAMS = """{L}     # L
+5e-9       # Delta0
+1.5        # gap
+0.07       # me
+0.45       # mh
+100e-3     # HO
+{gam}      # gam_e
+{gam}      # gam_h
+{gam}      # gam_eh
+9.1        # epsr
+36e-3      # Oph
+3e-3       # Gph
+0.0        # Edc
+1000000    # jmax
+20000      # ntmax
+"""
+
+MB_PARAMS = "1\n1\n0\n{scr}\n0\n0\n0\n0\n0\n0\n0\n0\n0\n0\n0\n"
+
+
+def make_leapfrog(R, out, name, L=2.85e-8, screened=False, nsteps=3000, dt=10e-18):
+    """Oracle B: the reference's own SBESolver driver with a diagonal drive."""
+    cwd = os.getcwd()
+    run = tempfile.mkdtemp(prefix="lf_", dir=_TMP)
+    os.makedirs(os.path.join(run, "params"))
+    gam = 5e12
+    with open(os.path.join(run, "params", "qw.params"), "w") as f:
+        f.write(QW_PARAMS.format(L=L, gam=gam))
+    with open(os.path.join(run, "params", "mb.params"), "w") as f:
+        f.write(MB_PARAMS.format(scr=1 if screened else 0))
+    os.chdir(run)
+    try:
+        rr = np.linspace(-5e-7, 5e-7, 64)
+        qrr = R.SBEs.GetKArray(64, 64 * (rr[1] - rr[0]))
+        s = R.SBEs.SBESolver(qrr, rr, 0.0, 1e7, 800e-9, 1, True)
+        nk, nr = s.Nk, s.Nr
+        y1 = np.stack([np.diag(s.YY2[:, :, 0]).real, np.diag(s.YY2[:, :, 0]).imag,
+                       np.diag(s.CC2[:, :, 0]).real, np.diag(s.DD2[:, :, 0]).real], 1)
+        y2 = np.stack([np.diag(s.YY3[:, :, 0]).real, np.diag(s.YY3[:, :, 0]).imag,
+                       np.diag(s.CC3[:, :, 0]).real, np.diag(s.DD3[:, :, 0]).real], 1)
+        E0, tw, tp = 2e8, 4e-15, 12e-15
+        wl = (s.gap + 0.05 * 1.602176634e-19) / R.SBEs.hbar
+        field = np.zeros(nsteps, dtype=complex)
+        P = np.zeros(nsteps, dtype=complex)
+        pscale = 2.0 * s.ehint / s.area / s.L * s.dcv
+        Px, Py, Pz = (np.zeros(nr, complex) for _ in range(3))
+        Re_, Rh_ = np.zeros(nr, complex), np.zeros(nr, complex)
+        t_start = time.time()
+        for n in range(nsteps):
+            t = n * dt
+            E = E0 * np.exp(-(((t - tp) / tw) ** 2)) * np.cos(wl * (t - tp))
+            field[n] = E
+            Ex = np.zeros(nr, complex)
+            Ey = np.zeros(nr, complex)
+            Ez = np.zeros(nr, complex)
+            Vr = np.zeros(nr, complex)
+            Ey[s.NQ0] = E
+            s._sbe_calculator(Ex, Ey, Ez, Vr, dt, Px, Py, Pz, Re_, Rh_, False, 1)
+            P[n] = pscale * np.sum(np.diag(s.YY3[:, :, 0]))
+        el = time.time() - t_start
+        Py_space = Py.copy()
+        R.usefulsubs.iFFTG(Py_space)
+        off = np.max(np.abs(s.YY3[:, :, 0] - np.diag(np.diag(s.YY3[:, :, 0]))))
+        z1 = np.stack([np.diag(s.YY2[:, :, 0]).real, np.diag(s.YY2[:, :, 0]).imag,
+                       np.diag(s.CC2[:, :, 0]).real, np.diag(s.DD2[:, :, 0]).real], 1)
+        z2 = np.stack([np.diag(s.YY3[:, :, 0]).real, np.diag(s.YY3[:, :, 0]).imag,
+                       np.diag(s.CC3[:, :, 0]).real, np.diag(s.DD3[:, :, 0]).real], 1)
+        g = pgrid.reference_grid(L=L)
+        assert g.nk == nk and np.array_equal(g.kr, s.kr)
+        VCt = np.zeros((nk, nk, 3))
+        E1Dt = np.zeros((nk, nk))
+        R.coulomb.CalcScreenedArrays(False, s.L, np.zeros(nk, complex), np.zeros(nk, complex),
+                                     VCt, E1Dt)
+        chie = R.coulomb._instance.Chi1De[:, 0].copy()
+        chih = R.coulomb._instance.Chi1Dh[:, 0].copy()
+        np.savez_compressed(
+            os.path.join(out, f"{name}.npz"), **grid_meta(g), y=g.y, gam=gam, screened=screened,
+            dt=dt, nsteps=nsteps, field=field, y1_init=y1, y2_init=y2, y1=z1, y2=z2, P=P,
+            pscale=pscale, mscale=s.ehint * s.dcv, Py_last=Py.copy(), Py_space=Py_space,
+            r=s.r.copy(), NQ0=s.NQ0,
+            Veh=VCt[:, 0, 0], Vee=VCt[:, 0, 1], Vhh=VCt[:, 0, 2], chie=chie, chih=chih,
+            offdiag=off, seconds=el)
+        print(f"{name}: Nk={nk} {nsteps} steps in {el:.1f} s, off-diag |p| = {off:.1e}, "
+              f"max|P| = {np.max(np.abs(P)):.3e}, max ne = {np.max(z2[:, 2]):.3e}")
+    finally:
+        os.chdir(cwd)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--full-c0", action="store_true")
+    ap.add_argument("--only", default="")
+    a = ap.parse_args()
+    R = import_reference()
+    out = HERE
+    only = set(a.only.split(",")) if a.only else None
+
+    def want(k):
+        return only is None or k in only
+
+    if want("tables"):
+        make_tables(R, out)
+    if want("rhs"):
+        make_rhs(R, out)
+    if want("rk4"):
+        make_rk4(R, out, "rk4_c0_nk32", rwa_case(32, 600))
+        make_rk4(R, out, "rk4_c0_nk64", rwa_case(64, 400, theta=1.5 * np.pi, det_meV=20.0,
+                                                 fwhm=30e-15, T2=60e-15))
+        make_rk4(R, out, "rk4_screened_nk32", rwa_case(32, 400, theta=1.2 * np.pi,
+                                                       screened=True))
+    if want("leapfrog"):
+        make_leapfrog(R, out, "leapfrog_nk32", screened=False)
+        make_leapfrog(R, out, "leapfrog_screened_nk32", screened=True, nsteps=2000)
+    if a.full_c0:
+        make_rk4(R, out, "rk4_c0_nk128_full", rwa_case(128, 4000))
+
+
+if __name__ == "__main__":
+    main()
