@@ -1,0 +1,331 @@
+#!/usr/bin/env python
+"""Benchmark of the quantum-wire SBE step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload c1] [--chunk S]
+
+A bench step advances every wire of the workload by S time steps (one launch
+of the fused step kernel); the metric counts wire*k*steps, i.e.
+sum_w Nk_w * S per bench step.  Default workload: configuration 1 (1024
+wires, Nk ~ U[64,512] rounded to 32, RK4 with dt = 1 fs), plain FP64 form.
+
+Timing: W untimed bench steps, then K bench steps each bracketed by CUDA
+events on the launching stream, with a 256 MiB write between them (L2 is
+126 MB) outside the events; barrier + synchronize around the whole loop;
+max over ranks.  `e2e` repeats the measurement through the public API with
+the state copied in from pinned host memory and P(t) + state copied back
+inside the timed region.  `--impl reference` times the CPU oracle (the
+restatement of the reference's Numba path) on the host cores instead.
+"""
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c1", choices=["c1", "c2", "c3"])
+    ap.add_argument("--chunk", type=int, default=100, help="time steps per bench step")
+    ap.add_argument("--nwires", type=int, default=0, help="override the workload's wire count")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def make_workload(name, rank, nwires):
+    from pulsesuite_b200 import workloads
+
+    kw = {"seed": 1 + 1000 * rank + {"c1": 0, "c2": 1, "c3": 2}[name]}
+    if nwires:
+        kw["nwires"] = nwires
+    return workloads.CONFIGS[name](**kw)
+
+
+# ---------------------------------------------------------------------------
+# Clock sampling during the timed region.
+# ---------------------------------------------------------------------------
+class Clocks:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is None:
+            return
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        self.rows = [r.split(",") for r in out.strip().splitlines() if r.strip()]
+
+    def summary(self):
+        if self.proc is None or not getattr(self, "rows", None):
+            return None
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[0]))
+                mx.append(float(r[1]))
+            except (ValueError, IndexError):
+                continue
+            for nm, v in zip(names, r[4:8]):
+                if v.strip().lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle (restatement of the reference's Numba path).
+# ---------------------------------------------------------------------------
+def cpu_baseline(wl, seconds, threads):
+    from scipy.constants import hbar
+
+    from oracle import oracle as orc
+    from pulsesuite_b200 import grid as pgrid
+
+    rng = np.random.default_rng(7)
+    blocks = [orc.grid_tables(g, screened=wl.screened) for g in wl.grids]
+    tables, tabdata = pgrid.pack_tables(wl.grids, blocks, screened=wl.screened)
+
+    def run(nw, nsteps):
+        idx = rng.choice(len(wl.wires), size=min(nw, len(wl.wires)), replace=False)
+        w = wl.wires[idx].copy()
+        nks = tables["nk"][w["table"]].astype(np.int64)
+        w["off"] = np.concatenate([[0], np.cumsum(nks)[:-1]])
+        y = np.zeros(4 * int(nks.sum()))
+        t0 = time.perf_counter()
+        orc.rk4(tables, tabdata, w, y, nsteps, wl.dt, hbar, nthreads=threads)
+        el = time.perf_counter() - t0
+        return float(nks.sum()) * nsteps / el, el, len(w)
+
+    # calibrate with a short run, then size the sample to ~`seconds`
+    rate, el, _ = run(2 * threads, 4)
+    units_per_wire_step = float(np.mean(wl.nks))
+    nsteps = 20
+    nw = int(max(threads, min(len(wl.wires), rate * seconds / (units_per_wire_step * nsteps))))
+    rate, el, nw = run(nw, nsteps)
+    return {"value": rate, "unit": "wire*k*steps/s", "cores": threads, "kind": "port",
+            "sample": f"{nw} wires drawn from the workload x {nsteps} RK4 steps "
+                      f"({el:.1f} s, OpenMP over wires)"}
+
+
+# ---------------------------------------------------------------------------
+def fp64_peak_tflops(torch, _lib, device):
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    sink = torch.zeros(sms * 8, dtype=torch.float64, device="cuda")
+    import ctypes
+
+    ms = ctypes.c_float(0.0)
+    best = 0.0
+    iters = 20000
+    for _ in range(3):
+        _lib.call("psb_probe_fp64_fma", sms * 8, iters, device.ptr(sink), ctypes.byref(ms),
+                  device.stream_ptr())
+        flops = 2.0 * 8 * iters * sms * 8 * 256
+        best = max(best, flops / (ms.value * 1e-3) / 1e12)
+    return best
+
+
+def run_ours(a):
+    import torch
+    import torch.distributed as dist
+
+    from pulsesuite_b200 import _lib, device
+    from pulsesuite_b200.batch import WireBatch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    wl = make_workload(a.workload, rank, a.nwires)
+    S = a.chunk
+    b = WireBatch(wl.grids, wl.wires, screened=wl.screened, p_cap=S)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    units = wl.units_per_step * S
+    flops_launch = wl.flops_per_step() * S
+
+    def step(p_stride=1):
+        b.rk4(S, wl.dt, p_stride=p_stride, stream=stream)
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+
+    # -- device-resident timing --------------------------------------------
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(a.steps)]
+    with Clocks(local) as clk:
+        torch.cuda.synchronize()
+        for i in range(a.steps):
+            flush.fill_(float(i))
+            evs[i][0].record(stream)
+            b.rk4(S, wl.dt, p_stride=1, stream=stream)
+            evs[i][1].record(stream)
+        torch.cuda.synchronize()
+    times = [e0.elapsed_time(e1) for e0, e1 in evs]
+    total_ms = float(sum(times))
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    value = units * a.steps * world / (total_ms * 1e-3)
+    status = b.wires()["status"]
+
+    # -- end to end through the public API: pinned host state in, P + state out
+    y_host = torch.zeros((b.n_state, 4), dtype=torch.float64).pin_memory()
+    y_out = torch.empty_like(y_host).pin_memory()
+    P_out = torch.empty(tuple(b.P.shape), dtype=torch.float64).pin_memory()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2e_ms = 0.0
+    torch.cuda.synchronize()
+    for i in range(a.steps):
+        flush.fill_(float(i))
+        e0.record(stream)
+        b.y.copy_(y_host, non_blocking=True)
+        b.rk4(S, wl.dt, p_stride=1, stream=stream)
+        P_out.copy_(b.P, non_blocking=True)
+        y_out.copy_(b.y, non_blocking=True)
+        e1.record(stream)
+        e1.synchronize()
+        e2e_ms += e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    h2d = y_host.numel() * 8
+    d2h = (P_out.numel() + y_out.numel()) * 8
+
+    peak = fp64_peak_tflops(torch, _lib, device)
+    avg_launch_ms = total_ms / a.steps
+    achieved = flops_launch / (avg_launch_ms * 1e-3) / 1e12
+
+    line = {
+        "metric": "SBE wire*k*steps/s (plain FP64 RK4)",
+        "value": value,
+        "unit": "wire*k*steps/s",
+        "n_gpus": world,
+        "steps": a.steps,
+        "warmup": a.warmup,
+        "ms_per_step": total_ms / a.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded configuration draws)",
+        "config": {"workload": wl.name, "wires_per_gpu": len(wl.wires),
+                   "wire_k_per_time_step": wl.units_per_step, "time_steps_per_bench_step": S,
+                   "form": "plain f64", "l2": "256 MiB write between timed steps",
+                   "parallelism": f"wires sharded, {world} independent GPU(s)"},
+        "e2e": {"value": units * a.steps * world / (e2e_ms * 1e-3), "unit": "wire*k*steps/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "peak_source": "measured in this run: psb_probe_fp64_fma (FMA loop)",
+                     "flops_per_launch": flops_launch},
+        "gpu_launches": a.steps,
+        "clocks": clk.summary(),
+        "wire_status_ok": bool((status == 0).all()),
+    }
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(wl, a.cpu_seconds, os.cpu_count() or 1)
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    wl = make_workload(a.workload, 0, a.nwires)
+    threads = os.cpu_count() or 1
+    vals = []
+    for _ in range(max(1, a.warmup)):
+        cpu_baseline(wl, 1.0, threads)
+    for _ in range(a.steps):
+        vals.append(cpu_baseline(wl, min(a.cpu_seconds, 60.0 / max(1, a.steps)), threads))
+    v = float(np.mean([x["value"] for x in vals]))
+    cb = dict(vals[-1])
+    cb["value"] = v
+    line = {
+        "impl": "reference",
+        "metric": "SBE wire*k*steps/s (plain FP64 RK4)",
+        "value": v,
+        "unit": "wire*k*steps/s",
+        "n_gpus": world,
+        "steps": a.steps,
+        "warmup": a.warmup,
+        "ms_per_step": None,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded configuration draws)",
+        "config": {"workload": wl.name, "form": "CPU oracle (restatement of the reference's "
+                   "Numba path), all host threads"},
+        "cpu_baseline": cb,
+        "e2e": {"value": v, "unit": "wire*k*steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

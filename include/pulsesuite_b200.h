@@ -98,7 +98,7 @@ typedef struct PsbWire {
   double phase[2];   /* pulse carrier-envelope phases (rad)                         */
   int64_t p_off;     /* first P(t) record (complex sample) of this wire             */
   int32_t status;    /* PSB_OK, or PSB_ERR_NONFINITE once the state is not finite   */
-  int32_t steps;     /* steps taken so far; indexes the P(t) record                  */
+  int32_t steps;     /* steps taken so far (advanced by the step entry points)      */
 } PsbWire;
 
 /* Model constants shared by every wire of a call. */
@@ -184,10 +184,12 @@ int psb_rhs_f64(const PsbTable* d_tables, int ntab, const double* d_tabdata, int
  * nsteps classical RK4 steps of size dt on every wire, in the stage order of
  * the reference integrator (libpulsesuite/integrator.py:143-157, rk4_dpc),
  * the whole step fused in one kernel with the wire's state resident on chip.
- * Advances each wire's t and steps.  Every p_stride-th step (counted by the
- * wire's `steps`) writes P(t) = pscale * sum_k p_k to
- * d_P[p_off + steps/p_stride - 1] (complex: 2 doubles) while that index is
- * < p_cap and inside d_P[0, n_P) (qwoptics.py:815-946, diagonal form).
+ * Advances each wire's t and steps.  Every p_stride-th step of the call
+ * (s = 1..nsteps, counted from the start of this call) writes
+ * P(t) = pscale * sum_k p_k to d_P[p_off + s/p_stride - 1] (complex: 2
+ * doubles) while s/p_stride <= p_cap and the record lies inside d_P[0, n_P)
+ * (qwoptics.py:815-946, diagonal form).  A caller advancing a solve in
+ * chunks copies each chunk's records out before the next call.
  */
 int psb_rk4_f64(const PsbTable* d_tables, int ntab, const double* d_tabdata, int64_t n_tabdata,
                 PsbWire* d_wires, int nw, const int32_t* d_order, double* d_y, int64_t n_state,

@@ -309,9 +309,11 @@ int orc_rhs(const PsbTable* tables, int ntab, const double* td, const PsbWire* w
   return PSB_OK;
 }
 
-static void record_P(PsbWire* w, int nk, const double* y, double* P, int p_stride, int p_cap) {
-  if (!P || p_stride <= 0 || (w->steps % p_stride) != 0) return;
-  int r = w->steps / p_stride - 1;
+/* P(t) record of the call-local step s (0-based): every p_stride-th step. */
+static void record_P(const PsbWire* w, int s, int nk, const double* y, double* P, int p_stride,
+                     int p_cap) {
+  if (!P || p_stride <= 0 || ((s + 1) % p_stride) != 0) return;
+  int r = (s + 1) / p_stride - 1;
   if (r < 0 || r >= p_cap) return;
   double sr = 0.0, si = 0.0;
   for (int k = 0; k < nk; ++k) {
@@ -371,7 +373,7 @@ int orc_rk4(const PsbTable* tables, int ntab, const double* td, PsbWire* wires, 
         for (int j = 0; j < n; ++j) yw[j] = yw[j] + (h / 6.0) * (k1[j] + k4[j] + 2.0 * k3[j]);
         w->t = t + h;
         w->steps += 1;
-        record_P(w, nk, yw, P, p_stride, p_cap);
+        record_P(w, s, nk, yw, P, p_stride, p_cap);
       }
       check_finite(w, nk, yw);
     }
@@ -430,7 +432,7 @@ int orc_leapfrog(const PsbTable* tables, int ntab, const double* td, PsbWire* wi
         }
         w->t = w->t + dt;
         w->steps += 1;
-        record_P(w, nk, b, P, p_stride, p_cap);
+        record_P(w, s, nk, b, P, p_stride, p_cap);
       }
       check_finite(w, nk, b);
     }

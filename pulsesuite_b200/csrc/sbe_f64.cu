@@ -455,8 +455,8 @@ __global__ void __launch_bounds__(kThreads, 1) sbe_f64_kernel(Batch bt) {
     t = t + h;
     steps += 1;
     // P(t) record (qwoptics.py:815-946, diagonal: pscale * sum_k p_k).
-    if (bt.P && bt.p_stride > 0 && steps % bt.p_stride == 0) {
-      int r = steps / bt.p_stride - 1;
+    if (bt.P && bt.p_stride > 0 && (s + 1) % bt.p_stride == 0) {
+      int r = (s + 1) / bt.p_stride - 1;
       double v[2] = {0.0, 0.0};
 #pragma unroll
       for (int e = 0; e < EPT; ++e) {
