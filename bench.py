@@ -139,8 +139,9 @@ def cpu_baseline(wl, seconds, threads):
     # calibrate with a short run, then size the sample to ~`seconds`
     rate, el, _ = run(2 * threads, 4)
     units_per_wire_step = float(np.mean(wl.nks))
-    nsteps = 20
-    nw = int(max(threads, min(len(wl.wires), rate * seconds / (units_per_wire_step * nsteps))))
+    budget = rate * seconds / units_per_wire_step  # wire*steps that fit the budget
+    nw = int(max(threads, min(len(wl.wires), budget / 20)))
+    nsteps = int(max(4, min(400, budget / nw)))
     rate, el, nw = run(nw, nsteps)
     return {"value": rate, "unit": "wire*k*steps/s", "cores": threads, "kind": "port",
             "sample": f"{nw} wires drawn from the workload x {nsteps} RK4 steps "
@@ -269,7 +270,7 @@ def run_ours(a):
                      "frac": achieved / peak, "traffic": None,
                      "peak_source": "measured in this run: psb_probe_fp64_fma (FMA loop)",
                      "flops_per_launch": flops_launch},
-        "gpu_launches": a.steps,
+        "gpu_launches": a.steps * b.launches_per_call,
         "clocks": clk.summary(),
         "wire_status_ok": bool((status == 0).all()),
     }

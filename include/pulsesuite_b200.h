@@ -56,6 +56,7 @@ extern "C" {
 /* ---- table flags --------------------------------------------------------- */
 #define PSB_TAB_EXCITONS 1 /* include the Hartree-Fock exchange sums (mb.params Excitons) */
 #define PSB_TAB_SCREENED 2 /* screen V per wire and per RHS (mb.params Screened)         */
+#define PSB_TAB_SHARED_V 4 /* Veh == Vee == Vhh (one table serves all three sums)        */
 
 /*
  * One k grid with its Coulomb/energy tables.  The doubles live in a packed
@@ -155,14 +156,19 @@ int psb_screen_f64(const PsbTable* d_tables, int ntab, const double* d_tabdata,
  * Shared arguments of the SBE entry points:
  *   d_tables[ntab], d_tabdata[n_tabdata]  device tables (PsbTable doc)
  *   d_wires[nw]                           device wire descriptors (PsbWire doc)
- *   d_order                               optional processing order (int32[nw],
- *                                         a permutation; largest grids first
- *                                         balances uneven batches), or NULL
  *   d_y (and d_y1)                        packed state, n_state elements of
  *                                         4 doubles {p_re, p_im, ne, nh}
- *   nkmax                                 largest table nk (sizes shared memory)
- *   screened                              nonzero if any table has
- *                                         PSB_TAB_SCREENED
+ *   d_order, n_order                      optional list of wire indices to
+ *                                         advance (one CTA each, in this
+ *                                         order; largest grids first balances
+ *                                         uneven batches), or NULL for all nw
+ *   nkmax                                 largest table nk of the wires
+ *                                         launched (sizes shared memory and
+ *                                         registers: launch size classes
+ *                                         separately for speed)
+ *   tab_flags                             PSB_TAB_SCREENED if any launched
+ *                                         table is screened; PSB_TAB_SHARED_V
+ *                                         only if every launched table has it
  * Descriptors are validated on the device: a wire whose table index, grid
  * size or state range is invalid is skipped and its status set to
  * PSB_ERR_INVALID / PSB_ERR_SIZE.  A wire whose state stops being finite gets
@@ -179,7 +185,7 @@ int psb_screen_f64(const PsbTable* d_tables, int ntab, const double* d_tabdata,
  */
 int psb_rhs_f64(const PsbTable* d_tables, int ntab, const double* d_tabdata, int64_t n_tabdata,
                 const PsbWire* d_wires, int nw, const double* d_y, double* d_dy,
-                int64_t n_state, int nkmax, int screened, const PsbModel* model, void* stream);
+                int64_t n_state, int nkmax, int tab_flags, const PsbModel* model, void* stream);
 /*
  * nsteps classical RK4 steps of size dt on every wire, in the stage order of
  * the reference integrator (libpulsesuite/integrator.py:143-157, rk4_dpc),
@@ -192,9 +198,9 @@ int psb_rhs_f64(const PsbTable* d_tables, int ntab, const double* d_tabdata, int
  * chunks copies each chunk's records out before the next call.
  */
 int psb_rk4_f64(const PsbTable* d_tables, int ntab, const double* d_tabdata, int64_t n_tabdata,
-                PsbWire* d_wires, int nw, const int32_t* d_order, double* d_y, int64_t n_state,
-                int nkmax, int screened, int nsteps, double dt, double* d_P, int64_t n_P,
-                int p_stride, int p_cap, const PsbModel* model, void* stream);
+                PsbWire* d_wires, int nw, const int32_t* d_order, int n_order, double* d_y,
+                int64_t n_state, int nkmax, int tab_flags, int nsteps, double dt, double* d_P,
+                int64_t n_P, int p_stride, int p_cap, const PsbModel* model, void* stream);
 /*
  * nsteps steps of the reference's own integrator (SBEs.py:5681-5718):
  *   X3 = X1 + 2 dt f(X2);  ne3 = |ne3|, nh3 = |nh3| rescaled to a common
@@ -208,13 +214,13 @@ int psb_rk4_f64(const PsbTable* d_tables, int ntab, const double* d_tabdata, int
  */
 int psb_leapfrog_f64(const PsbTable* d_tables, int ntab, const double* d_tabdata,
                      int64_t n_tabdata, PsbWire* d_wires, int nw, const int32_t* d_order,
-                     double* d_y1, double* d_y2, int64_t n_state, int nkmax, int screened,
-                     const double* d_field, int64_t field_stride, int64_t n_field, int nsteps,
-                     double dt, double* d_P, int64_t n_P, int p_stride, int p_cap,
-                     const PsbModel* model, void* stream);
+                     int n_order, double* d_y1, double* d_y2, int64_t n_state, int nkmax,
+                     int tab_flags, const double* d_field, int64_t field_stride,
+                     int64_t n_field, int nsteps, double dt, double* d_P, int64_t n_P,
+                     int p_stride, int p_cap, const PsbModel* model, void* stream);
 /* Dynamic shared memory (bytes) one CTA of the FP64 step kernels uses for a
- * grid of nk points (for capacity planning). */
-int psb_f64_smem_bytes(int nk);
+ * grid of nk points (for capacity planning; tab_flags as above). */
+int psb_f64_smem_bytes(int nk, int tab_flags);
 
 /* ---- measurement --------------------------------------------------------- */
 /*

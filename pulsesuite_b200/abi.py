@@ -22,6 +22,7 @@ PSB_MAX_NK = 1024
 
 PSB_TAB_EXCITONS = 1
 PSB_TAB_SCREENED = 2
+PSB_TAB_SHARED_V = 4
 
 # Blocks of a table in the packed tabdata array (each nk doubles).
 TAB_VEH, TAB_VEE, TAB_VHH, TAB_EE, TAB_EH, TAB_CHIE, TAB_CHIH, TAB_QE, TAB_QH = range(9)

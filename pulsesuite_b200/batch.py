@@ -48,9 +48,28 @@ class WireBatch:
         self.y1 = None
         self.P = torch.zeros((max(1, self.nw * self.p_cap), 2), dtype=torch.float64,
                              device="cuda")
-        # Largest grids first: balances uneven batches on the CTA scheduler.
+        # Launch classes by grid size (registers and shared memory are sized
+        # for a class's largest grid); largest grids first inside a class
+        # balances uneven batches on the CTA scheduler.
+        self.classes = []
         order = np.argsort(-nks, kind="stable").astype(np.int32)
-        self.d_order = torch.as_tensor(order, device="cuda")
+        for lo, hi in ((0, 256), (256, 512), (512, abi.PSB_MAX_NK)):
+            sel = order[(nks[order] > lo) & (nks[order] <= hi)]
+            if sel.size == 0:
+                continue
+            tabs = np.unique(w["table"][sel])
+            tf = self.h_tables["flags"][tabs]
+            flags = 0
+            if (tf & abi.PSB_TAB_SCREENED).any():
+                flags |= abi.PSB_TAB_SCREENED
+            if (tf & abi.PSB_TAB_SHARED_V).all():
+                flags |= abi.PSB_TAB_SHARED_V
+            self.classes.append((torch.as_tensor(sel, device="cuda"), int(nks[sel].max()), flags))
+        self.tab_flags = 0
+        if (self.h_tables["flags"] & abi.PSB_TAB_SCREENED).any():
+            self.tab_flags |= abi.PSB_TAB_SCREENED
+        if (self.h_tables["flags"] & abi.PSB_TAB_SHARED_V).all():
+            self.tab_flags |= abi.PSB_TAB_SHARED_V
         self.model = abi.model_array(hbar)
 
     # -- state --------------------------------------------------------------
@@ -82,26 +101,33 @@ class WireBatch:
                 self.tabdata.numel(), device.ptr(self.d_wires), self.nw)
 
     # -- entry points -----------------------------------------------------------
+    @property
+    def launches_per_call(self):
+        """Kernel launches one rk4/leapfrog call issues (one per size class)."""
+        return len(self.classes)
+
     def rhs(self, stream=None):
         dy = torch.empty_like(self.y)
         _lib.call("psb_rhs_f64", *self._common(), device.ptr(self.y), device.ptr(dy),
-                  self.n_state, self.nkmax, int(self.screened), abi.as_ptr(self.model),
+                  self.n_state, self.nkmax, self.tab_flags, abi.as_ptr(self.model),
                   device.stream_ptr(stream))
         return dy
 
     def rk4(self, nsteps, dt, p_stride=1, stream=None):
-        _lib.call("psb_rk4_f64", *self._common(), device.ptr(self.d_order), device.ptr(self.y),
-                  self.n_state, self.nkmax, int(self.screened), int(nsteps), float(dt),
-                  device.ptr(self.P), self.P.shape[0], int(p_stride), self.p_cap,
-                  abi.as_ptr(self.model), device.stream_ptr(stream))
+        for order, nkmax, flags in self.classes:
+            _lib.call("psb_rk4_f64", *self._common(), device.ptr(order), order.numel(),
+                      device.ptr(self.y), self.n_state, nkmax, flags, int(nsteps), float(dt),
+                      device.ptr(self.P), self.P.shape[0], int(p_stride), self.p_cap,
+                      abi.as_ptr(self.model), device.stream_ptr(stream))
 
     def leapfrog(self, field, nsteps, dt, p_stride=1, stream=None):
         """field: device float64 tensor (nw, 2*n_samples) of sampled E(t_n)."""
         if self.y1 is None:
             self.y1 = self.y.clone()
         assert field.is_cuda and field.dtype == torch.float64 and field.dim() == 2
-        _lib.call("psb_leapfrog_f64", *self._common(), device.ptr(self.d_order),
-                  device.ptr(self.y1), device.ptr(self.y), self.n_state, self.nkmax,
-                  int(self.screened), device.ptr(field), field.shape[1], field.numel(),
-                  int(nsteps), float(dt), device.ptr(self.P), self.P.shape[0], int(p_stride),
-                  self.p_cap, abi.as_ptr(self.model), device.stream_ptr(stream))
+        for order, nkmax, flags in self.classes:
+            _lib.call("psb_leapfrog_f64", *self._common(), device.ptr(order), order.numel(),
+                      device.ptr(self.y1), device.ptr(self.y), self.n_state, nkmax, flags,
+                      device.ptr(field), field.shape[1], field.numel(), int(nsteps), float(dt),
+                      device.ptr(self.P), self.P.shape[0], int(p_stride), self.p_cap,
+                      abi.as_ptr(self.model), device.stream_ptr(stream))

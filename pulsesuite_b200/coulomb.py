@@ -219,7 +219,12 @@ def grid_tables(grids, screened=False, excitons=True):
     """Device tables for a list of grids: (host table descriptors, device
     tabdata tensor)."""
     blocks = [table_block(g, screened) for g in grids]
-    tables, _ = pgrid.pack_tables(grids, [np.zeros(9 * g.nk) for g in grids], screened=screened,
-                                  excitons=excitons)
+    # descriptors from host copies of the V rows (flags need them)
+    host = []
+    for g, b in zip(grids, blocks):
+        h = np.zeros((9, g.nk))
+        h[0:3] = b.reshape(9, g.nk)[0:3].cpu().numpy()
+        host.append(h.reshape(-1))
+    tables, _ = pgrid.pack_tables(grids, host, screened=screened, excitons=excitons)
     tabdata = torch.cat(blocks) if blocks else torch.zeros(0, dtype=torch.float64, device="cuda")
     return tables, tabdata.contiguous()

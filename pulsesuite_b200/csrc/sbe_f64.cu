@@ -14,9 +14,11 @@
 // entry per k', so one new table value per table and k' is loaded.  The
 // symmetric tables Vs[d + doff] = V(|d|) (0 at d = 0, the excluded q = 0 term,
 // and beyond the grid) are stored with one pad double every R entries, which
-// makes the stride-R reads of a warp bank-conflict free.  Partial sums of the
-// kc chunks meet in shared memory and are added in a fixed order, so a wire's
-// result never depends on the other wires of the launch.
+// makes the stride-R reads of a warp bank-conflict free.  When the three
+// tables are equal (PSB_TAB_SHARED_V, the regularised-wire potential) only one
+// window is kept.  Partial sums of the kc chunks meet in shared memory and are
+// added in a fixed order, so a wire's result never depends on the other wires
+// of the launch.
 #include <math.h>
 
 #include "psb_common.cuh"
@@ -52,19 +54,19 @@ __host__ __device__ inline Geo geometry(int nk) {
 }
 
 // Shared-memory layout (doubles) of one wire.
-template <int R>
 struct Smem {
-  int ys, red, v, eps, scratch, total;
+  int ys, red, v, eps, stage, scratch, total;
 };
 
 template <int R>
-__host__ __device__ inline Smem<R> smem_layout(const Geo& g) {
-  Smem<R> s;
-  s.ys = 0;                                  // 4 SoA arrays of yslen: p_re, p_im, ne, nh
-  s.red = s.ys + 4 * g.yslen;                // [kc][4][nkp] partial exchange sums
-  s.v = s.red + 4 * g.kc * g.nkp;            // 3 skewed symmetric tables of vphys
-  s.eps = s.v + 3 * g.vphys;                 // eps(q) when screened (nk)
-  s.scratch = s.eps + g.nkp;                 // block reductions: kWarps*4 + 4
+__host__ __device__ inline Smem smem_layout(const Geo& g, int ntab) {
+  Smem s;
+  s.ys = 0;                          // 4 SoA arrays of yslen: p_re, p_im, ne, nh
+  s.red = s.ys + 4 * g.yslen;        // [kc][4][nkp] partial exchange sums
+  s.v = s.red + 4 * g.kc * g.nkp;    // ntab skewed symmetric tables of vphys
+  s.eps = s.v + ntab * g.vphys;      // eps(q) when screened (nkp)
+  s.stage = s.eps + g.nkp;           // [8][nkp]: RK4 k1 and k2/k2+k3, leapfrog X3
+  s.scratch = s.stage + 8 * g.nkp;   // block reductions: kWarps*4 + 4
   s.total = s.scratch + kWarps * 4 + 4;
   return s;
 }
@@ -129,39 +131,32 @@ __device__ __forceinline__ void drive(const PsbWire& w, double t, double& er, do
   }
 }
 
-// Fill the three symmetric tables of a wire, screened by eps when given.
-template <int R, bool SCREEN>
+// Fill the symmetric tables of a wire, screened by eps when given.
+template <int R, int NT, bool SCREEN>
 __device__ void fill_tables(const Geo& g, const double* __restrict__ blk, double* vs,
                             const double* eps) {
   for (int i = threadIdx.x; i < g.vlen; i += kThreads) {
     int d = i - g.doff;
     d = d < 0 ? -d : d;
-    double ve = 0.0, vw = 0.0, vh = 0.0;
-    if (d > 0 && d < g.nk) {
-      ve = blk[d];
-      vw = blk[g.nk + d];
-      vh = blk[2 * g.nk + d];
-      if (SCREEN) {
-        double e = eps[d];
-        ve = ve / e;
-        vw = vw / e;
-        vh = vh / e;
-      }
+    const bool in = d > 0 && d < g.nk;
+    const double e = (SCREEN && in) ? eps[d] : 1.0;
+    const int p = skew<R>(i);
+#pragma unroll
+    for (int t = 0; t < NT; ++t) {
+      double v = in ? blk[t * g.nk + d] : 0.0;
+      if (SCREEN) v = v / e;
+      vs[t * g.vphys + p] = v;
     }
-    int p = skew<R>(i);
-    vs[p] = ve;
-    vs[g.vphys + p] = vw;
-    vs[2 * g.vphys + p] = vh;
   }
 }
 
 // Static screening of the current stage state (coulomb.py:1218-1230): n1D
 // from the stage densities, then eps(q) for q < nk.
-template <int R>
 __device__ void screen_stage(const Geo& g, const PsbTable& tb, const double* __restrict__ blk,
                              const double* ys, double* eps, double* scratch) {
   double s[1] = {0.0};
-  for (int k = threadIdx.x; k < g.nk; k += kThreads) s[0] += ys[2 * g.yslen + k] + ys[3 * g.yslen + k];
+  for (int k = threadIdx.x; k < g.nk; k += kThreads)
+    s[0] += ys[2 * g.yslen + k] + ys[3 * g.yslen + k];
   block_sum(s, 1, scratch);
   double n1d = s[0] / 2.0 / tb.L;
   n1d = n1d < tb.dens_max ? n1d : tb.dens_max;
@@ -178,7 +173,7 @@ __device__ void screen_stage(const Geo& g, const PsbTable& tb, const double* __r
 
 // Exchange sums of one stage into red[kc][c][k] (c: Omega_re, Omega_im,
 // sum Vee ne, sum Vhh nh).
-template <int R>
+template <int R, int NT>
 __device__ __forceinline__ void exchange(const Geo& g, const double* ys, const double* vs,
                                          double* red) {
   const int t = threadIdx.x;
@@ -188,8 +183,8 @@ __device__ __forceinline__ void exchange(const Geo& g, const double* ys, const d
   const int k0 = kc * g.chunk;
   const int kout0 = ob * R;
   const double* __restrict__ VE = vs;
-  const double* __restrict__ VW = vs + g.vphys;
-  const double* __restrict__ VH = vs + 2 * g.vphys;
+  const double* __restrict__ VW = vs + (NT == 3 ? g.vphys : 0);
+  const double* __restrict__ VH = vs + (NT == 3 ? 2 * g.vphys : 0);
   const double* __restrict__ A = ys;
   const double* __restrict__ B = ys + g.yslen;
   const double* __restrict__ NE = ys + 2 * g.yslen;
@@ -197,16 +192,16 @@ __device__ __forceinline__ void exchange(const Geo& g, const double* ys, const d
   double ar[R], ai[R], ae[R], ah[R];
   double we[R], ww[R], wh[R];
 #pragma unroll
-  for (int r = 0; r < R; ++r) {
-    ar[r] = ai[r] = ae[r] = ah[r] = 0.0;
-  }
+  for (int r = 0; r < R; ++r) ar[r] = ai[r] = ae[r] = ah[r] = 0.0;
   int j = kout0 - k0 + g.doff;  // table index of r = 0 at k' = k0
 #pragma unroll
   for (int r = 0; r < R; ++r) {
-    int p = skew<R>(j + r);
+    const int p = skew<R>(j + r);
     we[r] = VE[p];
-    ww[r] = VW[p];
-    wh[r] = VH[p];
+    if (NT == 3) {
+      ww[r] = VW[p];
+      wh[r] = VH[p];
+    }
   }
   for (int kk = 0; kk < g.chunk; kk += R) {
 #pragma unroll
@@ -217,20 +212,24 @@ __device__ __forceinline__ void exchange(const Geo& g, const double* ys, const d
       for (int r = 0; r < R; ++r) {
         ar[r] = fma(we[r], a, ar[r]);
         ai[r] = fma(we[r], b, ai[r]);
-        ae[r] = fma(ww[r], ne, ae[r]);
-        ah[r] = fma(wh[r], nh, ah[r]);
+        ae[r] = fma(NT == 3 ? ww[r] : we[r], ne, ae[r]);
+        ah[r] = fma(NT == 3 ? wh[r] : we[r], nh, ah[r]);
       }
 #pragma unroll
       for (int r = R - 1; r > 0; --r) {
         we[r] = we[r - 1];
-        ww[r] = ww[r - 1];
-        wh[r] = wh[r - 1];
+        if (NT == 3) {
+          ww[r] = ww[r - 1];
+          wh[r] = wh[r - 1];
+        }
       }
       --j;
       const int p = skew<R>(j);
       we[0] = VE[p];
-      ww[0] = VW[p];
-      wh[0] = VH[p];
+      if (NT == 3) {
+        ww[0] = VW[p];
+        wh[0] = VH[p];
+      }
     }
   }
   double* rr = red + (size_t)kc * 4 * g.nkp;
@@ -282,13 +281,13 @@ __device__ __forceinline__ void rhs_element(const Geo& g, int k, const double* y
   f[3] = dn;
 }
 
-template <int R, int EPT, int MODE, bool SCREEN>
-__global__ void __launch_bounds__(kThreads, 1) sbe_f64_kernel(Batch bt) {
+template <int R, int EPT, int MODE, bool SCREEN, int NT>
+__global__ void __launch_bounds__(kThreads, EPT <= 2 ? 2 : 1) sbe_f64_kernel(Batch bt) {
   extern __shared__ double smem[];
   const int wi = bt.order ? bt.order[blockIdx.x] : (int)blockIdx.x;
   if (wi < 0 || wi >= bt.nw) return;
   PsbWire* wp = bt.wires + wi;
-  PsbWire w = *wp;
+  const PsbWire w = *wp;
   if (w.table < 0 || w.table >= bt.ntab) {
     if (threadIdx.x == 0) wp->status = PSB_ERR_INVALID;
     return;
@@ -299,12 +298,17 @@ __global__ void __launch_bounds__(kThreads, 1) sbe_f64_kernel(Batch bt) {
     if (threadIdx.x == 0) wp->status = PSB_ERR_SIZE;
     return;
   }
+  if (NT == 1 && (tb.flags & PSB_TAB_SHARED_V) == 0) {
+    if (threadIdx.x == 0) wp->status = PSB_ERR_INVALID;
+    return;
+  }
   const Geo g = geometry<R>(tb.nk);
-  const Smem<R> L = smem_layout<R>(g);
+  const Smem L = smem_layout<R>(g, NT);
   double* ys = smem + L.ys;
   double* red = smem + L.red;
   double* vs = smem + L.v;
   double* eps = smem + L.eps;
+  double* stage = smem + L.stage;
   double* scratch = smem + L.scratch;
   const double* blk = bt.tabdata + tb.off;
   const double* Ee = blk + 3 * tb.nk;
@@ -314,12 +318,12 @@ __global__ void __launch_bounds__(kThreads, 1) sbe_f64_kernel(Batch bt) {
   const double hbar = bt.hbar;
   const double hg = hbar * w.gamma;
   const int tid = threadIdx.x;
+  const int nkp = g.nkp;
 
   // Zero the padded sources, load the state.
   for (int i = tid; i < 4 * g.yslen; i += kThreads) ys[i] = 0.0;
   __syncthreads();
   double yb[EPT][4];  // RK4 base state / leapfrog X1
-  double k1[EPT][4], dym[EPT][4];
   const double2* y2 = reinterpret_cast<const double2*>(bt.y + 4 * w.off);
   const double2* y1g = MODE == kLeapfrog ? reinterpret_cast<const double2*>(bt.y1 + 4 * w.off)
                                          : nullptr;
@@ -346,7 +350,7 @@ __global__ void __launch_bounds__(kThreads, 1) sbe_f64_kernel(Batch bt) {
       }
     }
   }
-  if (exc && !scr) fill_tables<R, false>(g, blk, vs, eps);
+  if (exc && !scr) fill_tables<R, NT, false>(g, blk, vs, eps);
   __syncthreads();
 
   const int nst = MODE == kRhs ? 1 : bt.nsteps;
@@ -366,11 +370,11 @@ __global__ void __launch_bounds__(kThreads, 1) sbe_f64_kernel(Batch bt) {
     for (int st = 0; st < nstage; ++st) {
       if (exc) {
         if (scr) {
-          screen_stage<R>(g, tb, blk, ys, eps, scratch);
-          fill_tables<R, true>(g, blk, vs, eps);
+          screen_stage(g, tb, blk, ys, eps, scratch);
+          fill_tables<R, NT, true>(g, blk, vs, eps);
           __syncthreads();
         }
-        exchange<R>(g, ys, vs, red);
+        exchange<R, NT>(g, ys, vs, red);
       }
       __syncthreads();
       double er, ei;
@@ -384,7 +388,7 @@ __global__ void __launch_bounds__(kThreads, 1) sbe_f64_kernel(Batch bt) {
       const double mr = -w.mscale * er, mi = -w.mscale * ei;
 #pragma unroll
       for (int e = 0; e < EPT; ++e) {
-        int k = tid + e * kThreads;
+        const int k = tid + e * kThreads;
         if (k >= g.nk) continue;
         double f[4];
         rhs_element(g, k, ys, red, Ee, Eh, w.gap, hg, hbar, mr, mi, exc, f);
@@ -393,29 +397,32 @@ __global__ void __launch_bounds__(kThreads, 1) sbe_f64_kernel(Batch bt) {
           d2[2 * k] = make_double2(f[0], f[1]);
           d2[2 * k + 1] = make_double2(f[2], f[3]);
         } else if (MODE == kRk4) {
-          // Stage order of integrator.py:143-157.
+          // Stage order of integrator.py:143-157; k1 in stage[c], k2 and
+          // then k3 + k2 in stage[4 + c] (owner-thread slots, no sync needed).
 #pragma unroll
           for (int c = 0; c < 4; ++c) {
+            double* k1 = stage + c * nkp + k;
+            double* dym = stage + (4 + c) * nkp + k;
             double v;
             if (st == 0) {
-              k1[e][c] = f[c];
+              *k1 = f[c];
               v = yb[e][c] + (h / 2.0) * f[c];
             } else if (st == 1) {
-              dym[e][c] = f[c];
+              *dym = f[c];
               v = yb[e][c] + (h / 2.0) * f[c];
             } else if (st == 2) {
               v = yb[e][c] + h * f[c];
-              dym[e][c] = f[c] + dym[e][c];
+              *dym = f[c] + *dym;
             } else {
-              yb[e][c] = yb[e][c] + (h / 6.0) * ((k1[e][c] + f[c]) + 2.0 * dym[e][c]);
+              yb[e][c] = yb[e][c] + (h / 6.0) * ((*k1 + f[c]) + 2.0 * *dym);
               v = yb[e][c];
             }
             ys[c * g.yslen + k] = v;
           }
         } else {
-          // Leapfrog X3 = X1 + 2 dt f(X2) (SBEs.py:5685-5687); X3 kept in k1.
+          // Leapfrog X3 = X1 + 2 dt f(X2) (SBEs.py:5685-5687), kept in stage[c].
 #pragma unroll
-          for (int c = 0; c < 4; ++c) k1[e][c] = yb[e][c] + f[c] * h * 2.0;
+          for (int c = 0; c < 4; ++c) stage[c * nkp + k] = yb[e][c] + f[c] * h * 2.0;
         }
       }
       __syncthreads();
@@ -426,12 +433,13 @@ __global__ void __launch_bounds__(kThreads, 1) sbe_f64_kernel(Batch bt) {
       double v[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
       for (int e = 0; e < EPT; ++e) {
-        int k = tid + e * kThreads;
+        const int k = tid + e * kThreads;
         if (k < g.nk) {
-          k1[e][2] = fabs(k1[e][2]);
-          k1[e][3] = fabs(k1[e][3]);
-          v[0] += k1[e][2];
-          v[1] += k1[e][3];
+          double a = fabs(stage[2 * nkp + k]), b = fabs(stage[3 * nkp + k]);
+          stage[2 * nkp + k] = a;
+          stage[3 * nkp + k] = b;
+          v[0] += a;
+          v[1] += b;
         }
       }
       block_sum(v, 2, scratch);
@@ -439,14 +447,15 @@ __global__ void __launch_bounds__(kThreads, 1) sbe_f64_kernel(Batch bt) {
       const double small = 1e-200;
 #pragma unroll
       for (int e = 0; e < EPT; ++e) {
-        int k = tid + e * kThreads;
+        const int k = tid + e * kThreads;
         if (k < g.nk) {
-          k1[e][2] = k1[e][2] * total / (v[0] + small);
-          k1[e][3] = k1[e][3] * total / (v[1] + small);
+          stage[2 * nkp + k] = stage[2 * nkp + k] * total / (v[0] + small);
+          stage[3 * nkp + k] = stage[3 * nkp + k] * total / (v[1] + small);
 #pragma unroll
           for (int c = 0; c < 4; ++c) {
-            yb[e][c] = (yb[e][c] + k1[e][c]) / 2.0;
-            ys[c * g.yslen + k] = k1[e][c];
+            const double x3 = stage[c * nkp + k];
+            yb[e][c] = (yb[e][c] + x3) / 2.0;
+            ys[c * g.yslen + k] = x3;
           }
         }
       }
@@ -456,18 +465,18 @@ __global__ void __launch_bounds__(kThreads, 1) sbe_f64_kernel(Batch bt) {
     steps += 1;
     // P(t) record (qwoptics.py:815-946, diagonal: pscale * sum_k p_k).
     if (bt.P && bt.p_stride > 0 && (s + 1) % bt.p_stride == 0) {
-      int r = (s + 1) / bt.p_stride - 1;
+      const int r = (s + 1) / bt.p_stride - 1;
       double v[2] = {0.0, 0.0};
 #pragma unroll
       for (int e = 0; e < EPT; ++e) {
-        int k = tid + e * kThreads;
+        const int k = tid + e * kThreads;
         if (k < g.nk) {
           v[0] += ys[k];
           v[1] += ys[g.yslen + k];
         }
       }
       block_sum(v, 2, scratch);
-      if (tid == 0 && r >= 0 && r < bt.p_cap && w.p_off >= 0 && w.p_off + r < bt.n_P) {
+      if (tid == 0 && r < bt.p_cap && w.p_off >= 0 && w.p_off + r < bt.n_P) {
         bt.P[2 * (w.p_off + r)] = w.pscale * v[0];
         bt.P[2 * (w.p_off + r) + 1] = w.pscale * v[1];
       }
@@ -481,7 +490,7 @@ __global__ void __launch_bounds__(kThreads, 1) sbe_f64_kernel(Batch bt) {
   double2* y1o = MODE == kLeapfrog ? reinterpret_cast<double2*>(bt.y1 + 4 * w.off) : nullptr;
 #pragma unroll
   for (int e = 0; e < EPT; ++e) {
-    int k = tid + e * kThreads;
+    const int k = tid + e * kThreads;
     if (k < g.nk) {
       double a = ys[k], b = ys[g.yslen + k], c = ys[2 * g.yslen + k], d = ys[3 * g.yslen + k];
       if (MODE == kRk4) {
@@ -511,60 +520,66 @@ __global__ void __launch_bounds__(kThreads, 1) sbe_f64_kernel(Batch bt) {
 
 constexpr int kR = 4;
 
-size_t smem_bytes_for(int nk) {
+size_t smem_bytes_for(int nk, int ntab) {
   Geo g = geometry<kR>(nk);
-  return sizeof(double) * (size_t)smem_layout<kR>(g).total;
+  return sizeof(double) * (size_t)smem_layout<kR>(g, ntab).total;
 }
 
-template <int MODE, bool SCREEN>
-static int launch_ept(const Batch& bt, int ept, size_t smem, cudaStream_t st) {
+template <int MODE, bool SCREEN, int NT>
+static int launch_ept(const Batch& bt, int ept, int grid, size_t smem, cudaStream_t st) {
   void (*kern)(Batch) = nullptr;
   switch (ept) {
-    case 1: kern = sbe_f64_kernel<kR, 1, MODE, SCREEN>; break;
-    case 2: kern = sbe_f64_kernel<kR, 2, MODE, SCREEN>; break;
-    case 4: kern = sbe_f64_kernel<kR, 4, MODE, SCREEN>; break;
+    case 1: kern = sbe_f64_kernel<kR, 1, MODE, SCREEN, NT>; break;
+    case 2: kern = sbe_f64_kernel<kR, 2, MODE, SCREEN, NT>; break;
+    case 4: kern = sbe_f64_kernel<kR, 4, MODE, SCREEN, NT>; break;
     default: return set_error(PSB_ERR_SIZE, "unsupported elements per thread %d", ept);
   }
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess)
     return set_error(PSB_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
-  kern<<<bt.nw, kThreads, smem, st>>>(bt);
+  kern<<<grid, kThreads, smem, st>>>(bt);
   return check_cuda("sbe_f64_kernel");
 }
 
-// Host-side launch: sizes shared memory for the largest grid of the tables.
-int launch_sbe_f64(Batch bt, int mode, const PsbTable* h_tables_or_null, int nkmax,
-                   bool screened, cudaStream_t st) {
-  (void)h_tables_or_null;
+template <int MODE>
+static int launch_mode(const Batch& bt, int ept, int grid, size_t smem, bool screened,
+                       bool shared, cudaStream_t st) {
+  if (screened)
+    return shared ? launch_ept<MODE, true, 1>(bt, ept, grid, smem, st)
+                  : launch_ept<MODE, true, 3>(bt, ept, grid, smem, st);
+  return shared ? launch_ept<MODE, false, 1>(bt, ept, grid, smem, st)
+                : launch_ept<MODE, false, 3>(bt, ept, grid, smem, st);
+}
+
+// Host-side launch: sizes shared memory for the largest grid of the launch.
+int launch_sbe_f64(Batch bt, int mode, int n_order, int nkmax, int tab_flags, cudaStream_t st) {
   if (nkmax < 2 || nkmax > PSB_MAX_NK)
     return set_error(PSB_ERR_SIZE, "nk %d outside [2, %d]", nkmax, PSB_MAX_NK);
+  const bool screened = (tab_flags & PSB_TAB_SCREENED) != 0;
+  const bool shared = (tab_flags & PSB_TAB_SHARED_V) != 0;
   bt.nk_limit = nkmax;
   size_t smem = 0;
   for (int nk = 2; nk <= nkmax; ++nk) {
-    size_t b = smem_bytes_for(nk);
+    size_t b = smem_bytes_for(nk, shared ? 1 : 3);
     if (b > smem) smem = b;
   }
   int ept = (nkmax + kThreads - 1) / kThreads;
   if (ept == 3) ept = 4;
-  if (bt.nw == 0) return PSB_OK;
-  if (mode == kRhs)
-    return screened ? launch_ept<kRhs, true>(bt, ept, smem, st)
-                    : launch_ept<kRhs, false>(bt, ept, smem, st);
-  if (mode == kRk4)
-    return screened ? launch_ept<kRk4, true>(bt, ept, smem, st)
-                    : launch_ept<kRk4, false>(bt, ept, smem, st);
-  return screened ? launch_ept<kLeapfrog, true>(bt, ept, smem, st)
-                  : launch_ept<kLeapfrog, false>(bt, ept, smem, st);
+  const int grid = bt.order ? n_order : bt.nw;
+  if (grid <= 0) return PSB_OK;
+  if (mode == kRhs) return launch_mode<kRhs>(bt, ept, grid, smem, screened, shared, st);
+  if (mode == kRk4) return launch_mode<kRk4>(bt, ept, grid, smem, screened, shared, st);
+  return launch_mode<kLeapfrog>(bt, ept, grid, smem, screened, shared, st);
 }
 
 }  // namespace psb
 
 using namespace psb;
 
-extern "C" int psb_f64_smem_bytes(int nk) {
+extern "C" int psb_f64_smem_bytes(int nk, int tab_flags) {
   if (nk < 2 || nk > PSB_MAX_NK) return set_error(PSB_ERR_SIZE, "nk %d out of range", nk);
-  return (int)smem_bytes_for(nk);
+  return (int)smem_bytes_for(nk, (tab_flags & PSB_TAB_SHARED_V) ? 1 : 3);
 }
 
 static int common_checks(const PsbTable* d_tables, int ntab, const double* d_tabdata,
@@ -580,7 +595,7 @@ static int common_checks(const PsbTable* d_tables, int ntab, const double* d_tab
 
 extern "C" int psb_rhs_f64(const PsbTable* d_tables, int ntab, const double* d_tabdata,
                            int64_t n_tabdata, const PsbWire* d_wires, int nw, const double* d_y,
-                           double* d_dy, int64_t n_state, int nkmax, int screened,
+                           double* d_dy, int64_t n_state, int nkmax, int tab_flags,
                            const PsbModel* model, void* stream) {
   int rc = common_checks(d_tables, ntab, d_tabdata, d_wires, nw, d_y, model, nkmax);
   if (rc) return rc;
@@ -597,17 +612,18 @@ extern "C" int psb_rhs_f64(const PsbTable* d_tables, int ntab, const double* d_t
   bt.n_state = n_state;
   bt.nsteps = 1;
   bt.hbar = model->hbar;
-  return launch_sbe_f64(bt, kRhs, nullptr, nkmax, screened != 0, (cudaStream_t)stream);
+  return launch_sbe_f64(bt, kRhs, 0, nkmax, tab_flags, (cudaStream_t)stream);
 }
 
 extern "C" int psb_rk4_f64(const PsbTable* d_tables, int ntab, const double* d_tabdata,
                            int64_t n_tabdata, PsbWire* d_wires, int nw, const int32_t* d_order,
-                           double* d_y, int64_t n_state, int nkmax, int screened, int nsteps,
-                           double dt, double* d_P, int64_t n_P, int p_stride, int p_cap,
-                           const PsbModel* model, void* stream) {
+                           int n_order, double* d_y, int64_t n_state, int nkmax, int tab_flags,
+                           int nsteps, double dt, double* d_P, int64_t n_P, int p_stride,
+                           int p_cap, const PsbModel* model, void* stream) {
   int rc = common_checks(d_tables, ntab, d_tabdata, d_wires, nw, d_y, model, nkmax);
   if (rc) return rc;
-  if (nsteps < 0) return set_error(PSB_ERR_INVALID, "nsteps < 0");
+  if (nsteps < 0 || (d_order && n_order < 0))
+    return set_error(PSB_ERR_INVALID, "nsteps or n_order < 0");
   if (nsteps == 0) return PSB_OK;
   Batch bt{};
   bt.tables = d_tables;
@@ -626,20 +642,21 @@ extern "C" int psb_rk4_f64(const PsbTable* d_tables, int ntab, const double* d_t
   bt.p_stride = p_stride;
   bt.p_cap = p_cap;
   bt.hbar = model->hbar;
-  return launch_sbe_f64(bt, kRk4, nullptr, nkmax, screened != 0, (cudaStream_t)stream);
+  return launch_sbe_f64(bt, kRk4, n_order, nkmax, tab_flags, (cudaStream_t)stream);
 }
 
 extern "C" int psb_leapfrog_f64(const PsbTable* d_tables, int ntab, const double* d_tabdata,
                                 int64_t n_tabdata, PsbWire* d_wires, int nw,
-                                const int32_t* d_order, double* d_y1, double* d_y2,
-                                int64_t n_state, int nkmax, int screened, const double* d_field,
-                                int64_t field_stride, int64_t n_field, int nsteps, double dt,
-                                double* d_P, int64_t n_P, int p_stride, int p_cap,
-                                const PsbModel* model, void* stream) {
+                                const int32_t* d_order, int n_order, double* d_y1, double* d_y2,
+                                int64_t n_state, int nkmax, int tab_flags,
+                                const double* d_field, int64_t field_stride, int64_t n_field,
+                                int nsteps, double dt, double* d_P, int64_t n_P, int p_stride,
+                                int p_cap, const PsbModel* model, void* stream) {
   int rc = common_checks(d_tables, ntab, d_tabdata, d_wires, nw, d_y2, model, nkmax);
   if (rc) return rc;
   if (!d_y1 || !d_field) return set_error(PSB_ERR_INVALID, "d_y1 or d_field is null");
-  if (nsteps < 0) return set_error(PSB_ERR_INVALID, "nsteps < 0");
+  if (nsteps < 0 || (d_order && n_order < 0))
+    return set_error(PSB_ERR_INVALID, "nsteps or n_order < 0");
   if (nsteps == 0) return PSB_OK;
   Batch bt{};
   bt.tables = d_tables;
@@ -662,5 +679,5 @@ extern "C" int psb_leapfrog_f64(const PsbTable* d_tables, int ntab, const double
   bt.p_stride = p_stride;
   bt.p_cap = p_cap;
   bt.hbar = model->hbar;
-  return launch_sbe_f64(bt, kLeapfrog, nullptr, nkmax, screened != 0, (cudaStream_t)stream);
+  return launch_sbe_f64(bt, kLeapfrog, n_order, nkmax, tab_flags, (cudaStream_t)stream);
 }

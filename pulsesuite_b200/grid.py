@@ -174,6 +174,10 @@ def pack_tables(grids, blocks, screened=False, excitons=True):
             flags |= abi.PSB_TAB_EXCITONS
         if screened:
             flags |= abi.PSB_TAB_SCREENED
+        v = np.asarray(b).reshape(abi.TAB_BLOCKS, g.nk)
+        if np.array_equal(v[abi.TAB_VEH], v[abi.TAB_VEE]) and np.array_equal(
+                v[abi.TAB_VEH], v[abi.TAB_VHH]):
+            flags |= abi.PSB_TAB_SHARED_V
         tables[i]["flags"] = flags
         tables[i]["off"] = off
         tables[i]["L"] = g.L
