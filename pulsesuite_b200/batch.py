@@ -19,9 +19,16 @@ from . import _lib, abi, coulomb, device
 
 
 class WireBatch:
+    """``form`` selects the step kernel: "plain" (FP64 throughout,
+    psb_rk4_f64) or "split" (bf16 hi+lo tensor-core exchange with FP32
+    right-hand side and FP64 stage combination, psb_rk4_split)."""
+
     def __init__(self, grids, wires, screened=False, excitons=True, p_cap=0, tables=None,
-                 tabdata=None):
+                 tabdata=None, form="plain"):
         device.require_cuda()
+        if form not in ("plain", "split"):
+            raise ValueError("form must be 'plain' or 'split'")
+        self.form = form
         self.grids = list(grids)
         self.screened = bool(screened)
         if tables is None:
@@ -65,12 +72,67 @@ class WireBatch:
             if (tf & abi.PSB_TAB_SHARED_V).all():
                 flags |= abi.PSB_TAB_SHARED_V
             self.classes.append((torch.as_tensor(sel, device="cuda"), int(nks[sel].max()), flags))
+        if form == "split":
+            self._setup_split()
         self.tab_flags = 0
         if (self.h_tables["flags"] & abi.PSB_TAB_SCREENED).any():
             self.tab_flags |= abi.PSB_TAB_SCREENED
         if (self.h_tables["flags"] & abi.PSB_TAB_SHARED_V).all():
             self.tab_flags |= abi.PSB_TAB_SHARED_V
         self.model = abi.model_array(hbar)
+
+    def _setup_split(self):
+        """T tiles per grid, wire groups (one CTA each) and the workspace."""
+        need = abi.PSB_TAB_EXCITONS | abi.PSB_TAB_SHARED_V
+        f = self.h_tables["flags"]
+        if ((f & need) != need).any() or (f & abi.PSB_TAB_SCREENED).any():
+            raise _lib.PsbError("split form needs unscreened tables with Veh == Vee == Vhh")
+        lib = _lib.load()
+        nt = len(self.h_tables)
+        stab = np.zeros(nt, dtype=abi.SPLIT_TABLE_DTYPE)
+        sizes = [int(lib.psb_split_tile_bytes(int(n))) for n in self.h_tables["nk"]]
+        offs = np.zeros(nt, dtype=np.int64)
+        tot = 0
+        for i, sz in enumerate(sizes):
+            offs[i] = tot
+            tot += (sz + 255) // 256 * 256
+        self.tiles = torch.zeros(max(tot, 256), dtype=torch.uint8, device="cuda")
+        for i in range(nt):
+            nk = int(self.h_tables["nk"][i])
+            V = self.tabdata[int(self.h_tables["off"][i]):int(self.h_tables["off"][i]) + nk]
+            vscale = float(V[1:].abs().max().item()) if nk > 1 else 1.0
+            vscale = vscale if vscale > 0 else 1.0
+            stab[i]["tile_off"] = offs[i]
+            stab[i]["vscale"] = vscale
+            stab[i]["kpad"] = (nk + 63) // 64 * 64
+            stab[i]["mtiles"] = (nk + 127) // 128
+            _lib.call("psb_split_prepare", device.ptr(V), nk, vscale,
+                      device.ptr(self.tiles[offs[i]:]), self.tiles.numel() - int(offs[i]),
+                      device.stream_ptr())
+        self.h_stab = stab
+        self.d_stab = device.to_device(stab)
+        # groups: same table, up to 16 wires (8 above nk 512), largest grids first
+        self.split_launches = []
+        for wg in (16, 8):
+            groups = []
+            for t in np.argsort(-self.h_tables["nk"], kind="stable"):
+                nk = int(self.h_tables["nk"][t])
+                if (wg == 16) != (nk <= 512):
+                    continue
+                ws = np.nonzero(self.h_wires["table"] == t)[0]
+                for i in range(0, len(ws), wg):
+                    g = np.zeros(1, dtype=abi.SPLIT_GROUP_DTYPE)
+                    g["table"] = t
+                    g["nw"] = len(ws[i:i + wg])
+                    g["wire"][0, :g["nw"][0]] = ws[i:i + wg]
+                    g["wire"][0, g["nw"][0]:] = -1
+                    groups.append(g)
+            if groups:
+                ga = np.concatenate(groups)
+                nkmax = int(self.h_tables["nk"][ga["table"]].max())
+                self.split_launches.append((wg, device.to_device(ga), len(ga), nkmax))
+        self.ws = torch.zeros(int(lib.psb_split_ws_bytes(self.n_state)), dtype=torch.uint8,
+                              device="cuda")
 
     # -- state --------------------------------------------------------------
     def set_state(self, y, y1=None):
@@ -104,6 +166,8 @@ class WireBatch:
     @property
     def launches_per_call(self):
         """Kernel launches one rk4/leapfrog call issues (one per size class)."""
+        if self.form == "split":
+            return len(self.split_launches)
         return len(self.classes)
 
     def rhs(self, stream=None):
@@ -114,6 +178,15 @@ class WireBatch:
         return dy
 
     def rk4(self, nsteps, dt, p_stride=1, stream=None):
+        if self.form == "split":
+            for wg, groups, ng, nkmax in self.split_launches:
+                _lib.call("psb_rk4_split", *self._common(), device.ptr(self.d_stab),
+                          device.ptr(self.tiles), self.tiles.numel(), device.ptr(groups), ng,
+                          wg, nkmax, device.ptr(self.y), self.n_state, device.ptr(self.ws),
+                          self.ws.numel(), int(nsteps), float(dt), device.ptr(self.P),
+                          self.P.shape[0], int(p_stride), self.p_cap, abi.as_ptr(self.model),
+                          device.stream_ptr(stream))
+            return
         for order, nkmax, flags in self.classes:
             _lib.call("psb_rk4_f64", *self._common(), device.ptr(order), order.numel(),
                       device.ptr(self.y), self.n_state, nkmax, flags, int(nsteps), float(dt),
