@@ -42,6 +42,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c1", choices=["c1", "c2", "c3"])
     ap.add_argument("--chunk", type=int, default=100, help="time steps per bench step")
+    ap.add_argument("--form", default="plain", choices=["plain", "split"],
+                    help="plain FP64 kernel or split bf16x3 tensor-core kernel")
     ap.add_argument("--nwires", type=int, default=0, help="override the workload's wire count")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -165,6 +167,16 @@ def fp64_peak_tflops(torch, _lib, device):
     return best
 
 
+def measured_bf16_peak():
+    """Dense bf16 peak of this pool's B200s (driver-measured cuBLAS burst)."""
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            v = float(json.load(f)["bf16_tflops"])
+        return v, "MEASURED_PEAKS.json bf16_tflops (cuBLAS burst), of measured"
+    except (OSError, KeyError, ValueError):
+        return 1590.0, "fallback 1.59 PFLOP/s (no MEASURED_PEAKS.json)"
+
+
 def run_ours(a):
     import torch
     import torch.distributed as dist
@@ -183,7 +195,7 @@ def run_ours(a):
 
     wl = make_workload(a.workload, rank, a.nwires)
     S = a.chunk
-    b = WireBatch(wl.grids, wl.wires, screened=wl.screened, p_cap=S)
+    b = WireBatch(wl.grids, wl.wires, screened=wl.screened, p_cap=S, form=a.form)
     stream = torch.cuda.current_stream()
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
     units = wl.units_per_step * S
@@ -243,12 +255,22 @@ def run_ours(a):
     h2d = y_host.numel() * 8
     d2h = (P_out.numel() + y_out.numel()) * 8
 
-    peak = fp64_peak_tflops(torch, _lib, device)
     avg_launch_ms = total_ms / a.steps
+    if a.form == "plain":
+        peak = fp64_peak_tflops(torch, _lib, device)
+        peak_source = "measured in this run: psb_probe_fp64_fma (FMA loop)"
+        bound = "fp64"
+    else:
+        # the split algorithm's tensor-core work: 3 bf16 products x 4 columns
+        # x Nk MACs per element and stage (unpadded grid)
+        flops_launch = float(np.sum(wl.nks.astype(np.float64) ** 2)) * 96.0 * S
+        peak, peak_source = measured_bf16_peak()
+        bound = "tensor"
     achieved = flops_launch / (avg_launch_ms * 1e-3) / 1e12
 
     line = {
-        "metric": "SBE wire*k*steps/s (plain FP64 RK4)",
+        "metric": ("SBE wire*k*steps/s (plain FP64 RK4)" if a.form == "plain" else
+                   "SBE wire*k*steps/s (split bf16x3 tensor-core RK4)"),
         "value": value,
         "unit": "wire*k*steps/s",
         "n_gpus": world,
@@ -258,17 +280,16 @@ def run_ours(a):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64",
+        "dtype": "f64" if a.form == "plain" else "bf16x3+f32acc+f64",
         "data": "synthetic (seeded configuration draws)",
         "config": {"workload": wl.name, "wires_per_gpu": len(wl.wires),
                    "wire_k_per_time_step": wl.units_per_step, "time_steps_per_bench_step": S,
-                   "form": "plain f64", "l2": "256 MiB write between timed steps",
+                   "form": a.form, "l2": "256 MiB write between timed steps",
                    "parallelism": f"wires sharded, {world} independent GPU(s)"},
         "e2e": {"value": units * a.steps * world / (e2e_ms * 1e-3), "unit": "wire*k*steps/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak, "traffic": None,
-                     "peak_source": "measured in this run: psb_probe_fp64_fma (FMA loop)",
+        "roofline": {"bound": bound, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": None, "peak_source": peak_source,
                      "flops_per_launch": flops_launch},
         "gpu_launches": a.steps * b.launches_per_call,
         "clocks": clk.summary(),

@@ -229,18 +229,11 @@ int psb_f64_smem_bytes(int nk, int tab_flags);
  * grid, the exchange sums of all wires are one contraction
  *   D[k][(w,v)] = sum_k' T[k][k'] X[k'][(w,v)],  T[k][k'] = V(|k-k'|)/vscale,
  * computed on the tensor cores as bf16 hi+lo split products (Th Xh + Th Xl +
- * Tl Xh) accumulated in FP32; the right-hand side is evaluated in FP32 and
- * the RK4 stages are combined in FP64 (densities and P(t) sums in FP64).
- * The state keeps the FP64 layout of the plain form with p rounded to FP32.
+ * Tl Xh) accumulated in FP32, with vscale the power of two at or above
+ * max V.  The O(Nk) right-hand side, the RK4 stage combination, the state and
+ * the P(t) sums stay FP64 (FP64 layout of the plain form).
  * Requires PSB_TAB_EXCITONS | PSB_TAB_SHARED_V tables without screening.
  */
-typedef struct PsbSplitTable {
-  int64_t tile_off;  /* byte offset of this grid's T tiles in d_tiles (16-aligned)  */
-  double vscale;     /* exchange = vscale * D                                       */
-  int32_t kpad;      /* nk rounded up to a multiple of 64                           */
-  int32_t mtiles;    /* ceil(nk / 128)                                              */
-} PsbSplitTable;
-
 #define PSB_SPLIT_WMAX 16
 /* One CTA's work: 1..wgroup wires of one table (same k grid). */
 typedef struct PsbSplitGroup {
@@ -249,35 +242,27 @@ typedef struct PsbSplitGroup {
   int32_t wire[PSB_SPLIT_WMAX];
 } PsbSplitGroup;
 
-/* Bytes of T tiles of a grid of nk points (psb_split_prepare output). */
-int64_t psb_split_tile_bytes(int nk);
 /* Workspace bytes psb_rk4_split needs for n_state elements. */
 int64_t psb_split_ws_bytes(int64_t n_state);
-/* Dynamic shared memory (bytes) of one CTA for a grid of nk, wgroup 8 or 16. */
+/* Dynamic shared memory (bytes) of one CTA for a grid of nk, wgroup 4/8/16. */
 int psb_split_smem_bytes(int nk, int wgroup);
-/*
- * Build the T tiles of one grid from its V(q) block (d_V = tabdata + off,
- * q = 0..nk-1; vscale > 0, normally max V).  No counterpart in the reference
- * (it is this form's operand preparation of CalcH's exchange matrix,
- * SBEs.py:829-834).
- */
-int psb_split_prepare(const double* d_V, int nk, double vscale, void* d_tiles,
-                      int64_t n_tiles_bytes, void* stream);
+/* Largest nk a group of wgroup wires supports (shared and tensor memory). */
+int psb_split_max_nk(int wgroup);
 /*
  * nsteps RK4 steps of every group (one CTA each), same contract as
  * psb_rk4_f64 (state, t, steps, status, P(t) records) for the wires of
- * d_groups[0..ngroups).  wgroup (8 or 16) is the group capacity compiled
- * for; nkmax the largest grid among the groups (wgroup 16: nkmax <= 512).
+ * d_groups[0..ngroups).  wgroup (4, 8 or 16) is the group capacity compiled
+ * for; nkmax the largest grid among the groups (<= psb_split_max_nk(wgroup)).
  * d_ws: caller-allocated workspace of psb_split_ws_bytes(n_state) bytes,
- * 32-byte aligned.  Replaces, like psb_rk4_f64, CalcH + dpdt/dCdt/dDdt
- * (SBEs.py:669-935, 1850-2636) integrated by rk4_dpc (integrator.py:143-167).
+ * 32-byte aligned (stage state and RK accumulator per element).  Replaces,
+ * like psb_rk4_f64, CalcH + dpdt/dCdt/dDdt (SBEs.py:669-935, 1850-2636)
+ * integrated by rk4_dpc (libpulsesuite/integrator.py:143-167).
  */
 int psb_rk4_split(const PsbTable* d_tables, int ntab, const double* d_tabdata, int64_t n_tabdata,
-                  PsbWire* d_wires, int nw, const PsbSplitTable* d_stab, const void* d_tiles,
-                  int64_t n_tiles_bytes, const PsbSplitGroup* d_groups, int ngroups, int wgroup,
-                  int nkmax, double* d_y, int64_t n_state, void* d_ws, int64_t n_ws_bytes,
-                  int nsteps, double dt, double* d_P, int64_t n_P, int p_stride, int p_cap,
-                  const PsbModel* model, void* stream);
+                  PsbWire* d_wires, int nw, const PsbSplitGroup* d_groups, int ngroups,
+                  int wgroup, int nkmax, double* d_y, int64_t n_state, void* d_ws,
+                  int64_t n_ws_bytes, int nsteps, double dt, double* d_P, int64_t n_P,
+                  int p_stride, int p_cap, const PsbModel* model, void* stream);
 
 /* ---- measurement --------------------------------------------------------- */
 /*

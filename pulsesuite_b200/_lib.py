@@ -31,12 +31,11 @@ _SIGNATURES = {
                           i64, i32, f64, vp, i64, i32, i32, vp, vp], i32),
     "psb_f64_smem_bytes": ([i32, i32], i32),
     "psb_probe_fp64_fma": ([i32, i32, vp, vp, vp], i32),
-    "psb_split_tile_bytes": ([i32], i64),
     "psb_split_ws_bytes": ([i64], i64),
     "psb_split_smem_bytes": ([i32, i32], i32),
-    "psb_split_prepare": ([vp, i32, f64, vp, i64, vp], i32),
-    "psb_rk4_split": ([vp, i32, vp, i64, vp, i32, vp, vp, i64, vp, i32, i32, i32, vp, i64, vp, i64,
-                       i32, f64, vp, i64, i32, i32, vp, vp], i32),
+    "psb_split_max_nk": ([i32], i32),
+    "psb_rk4_split": ([vp, i32, vp, i64, vp, i32, vp, i32, i32, i32, vp, i64, vp, i64, i32, f64,
+                       vp, i64, i32, i32, vp, vp], i32),
 }
 
 

@@ -58,15 +58,12 @@ WIRE_DTYPE = np.dtype(
 MODEL_DTYPE = np.dtype([("hbar", "<f8"), ("flags", "<i4"), ("reserved", "<i4")], align=True)
 
 PSB_SPLIT_WMAX = 16
-SPLIT_TABLE_DTYPE = np.dtype(
-    [("tile_off", "<i8"), ("vscale", "<f8"), ("kpad", "<i4"), ("mtiles", "<i4")], align=True)
 SPLIT_GROUP_DTYPE = np.dtype(
     [("table", "<i4"), ("nw", "<i4"), ("wire", "<i4", (PSB_SPLIT_WMAX,))], align=True)
 
 assert TABLE_DTYPE.itemsize == 32
 assert WIRE_DTYPE.itemsize == 136
 assert MODEL_DTYPE.itemsize == 16
-assert SPLIT_TABLE_DTYPE.itemsize == 24
 assert SPLIT_GROUP_DTYPE.itemsize == 72
 
 

@@ -82,55 +82,50 @@ class WireBatch:
         self.model = abi.model_array(hbar)
 
     def _setup_split(self):
-        """T tiles per grid, wire groups (one CTA each) and the workspace."""
+        """Wire groups (one CTA each) and the workspace of the split form.
+
+        A group holds up to W in {4, 8, 16} wires of one grid.  The exchange
+        work of a group per step is ~W Nk^2, so W is chosen per grid to give
+        roughly two waves of equal CTAs over the SMs (small W for large
+        grids, W = 16 once a grid has enough wires), which balances uneven
+        batches; the three W classes run concurrently on side streams."""
         need = abi.PSB_TAB_EXCITONS | abi.PSB_TAB_SHARED_V
         f = self.h_tables["flags"]
         if ((f & need) != need).any() or (f & abi.PSB_TAB_SCREENED).any():
             raise _lib.PsbError("split form needs unscreened tables with Veh == Vee == Vhh")
         lib = _lib.load()
-        nt = len(self.h_tables)
-        stab = np.zeros(nt, dtype=abi.SPLIT_TABLE_DTYPE)
-        sizes = [int(lib.psb_split_tile_bytes(int(n))) for n in self.h_tables["nk"]]
-        offs = np.zeros(nt, dtype=np.int64)
-        tot = 0
-        for i, sz in enumerate(sizes):
-            offs[i] = tot
-            tot += (sz + 255) // 256 * 256
-        self.tiles = torch.zeros(max(tot, 256), dtype=torch.uint8, device="cuda")
-        for i in range(nt):
-            nk = int(self.h_tables["nk"][i])
-            V = self.tabdata[int(self.h_tables["off"][i]):int(self.h_tables["off"][i]) + nk]
-            vscale = float(V[1:].abs().max().item()) if nk > 1 else 1.0
-            vscale = vscale if vscale > 0 else 1.0
-            stab[i]["tile_off"] = offs[i]
-            stab[i]["vscale"] = vscale
-            stab[i]["kpad"] = (nk + 63) // 64 * 64
-            stab[i]["mtiles"] = (nk + 127) // 128
-            _lib.call("psb_split_prepare", device.ptr(V), nk, vscale,
-                      device.ptr(self.tiles[offs[i]:]), self.tiles.numel() - int(offs[i]),
-                      device.stream_ptr())
-        self.h_stab = stab
-        self.d_stab = device.to_device(stab)
-        # groups: same table, up to 16 wires (8 above nk 512), largest grids first
+        maxnk = {wg: int(lib.psb_split_max_nk(wg)) for wg in (4, 8, 16)}
+        nks = self.h_tables["nk"].astype(np.int64)
+        counts = np.bincount(self.h_wires["table"], minlength=len(nks))
+        sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+        target = float(np.sum(counts * nks.astype(np.float64) ** 2)) / (2.0 * sms)
+        classes = {4: [], 8: [], 16: []}
+        for t in np.argsort(-nks, kind="stable"):
+            nk = int(nks[t])
+            if counts[t] == 0:
+                continue
+            wg = 4
+            for cand in (16, 8):
+                if nk <= maxnk[cand] and cand * nk * nk <= max(target, 4 * nk * nk):
+                    wg = cand
+                    break
+            if nk > maxnk[wg]:
+                raise _lib.PsbError(f"split form: nk {nk} exceeds the supported maximum")
+            ws = np.nonzero(self.h_wires["table"] == t)[0]
+            for i in range(0, len(ws), wg):
+                g = np.zeros(1, dtype=abi.SPLIT_GROUP_DTYPE)
+                g["table"] = t
+                g["nw"] = len(ws[i:i + wg])
+                g["wire"][0, :] = -1
+                g["wire"][0, :g["nw"][0]] = ws[i:i + wg]
+                classes[wg].append(g)
         self.split_launches = []
-        for wg in (16, 8):
-            groups = []
-            for t in np.argsort(-self.h_tables["nk"], kind="stable"):
-                nk = int(self.h_tables["nk"][t])
-                if (wg == 16) != (nk <= 512):
-                    continue
-                ws = np.nonzero(self.h_wires["table"] == t)[0]
-                for i in range(0, len(ws), wg):
-                    g = np.zeros(1, dtype=abi.SPLIT_GROUP_DTYPE)
-                    g["table"] = t
-                    g["nw"] = len(ws[i:i + wg])
-                    g["wire"][0, :g["nw"][0]] = ws[i:i + wg]
-                    g["wire"][0, g["nw"][0]:] = -1
-                    groups.append(g)
-            if groups:
-                ga = np.concatenate(groups)
-                nkmax = int(self.h_tables["nk"][ga["table"]].max())
+        for wg in (16, 8, 4):
+            if classes[wg]:
+                ga = np.concatenate(classes[wg])
+                nkmax = int(nks[ga["table"]].max())
                 self.split_launches.append((wg, device.to_device(ga), len(ga), nkmax))
+        self.side_streams = [torch.cuda.Stream() for _ in self.split_launches[1:]]
         self.ws = torch.zeros(int(lib.psb_split_ws_bytes(self.n_state)), dtype=torch.uint8,
                               device="cuda")
 
@@ -179,13 +174,23 @@ class WireBatch:
 
     def rk4(self, nsteps, dt, p_stride=1, stream=None):
         if self.form == "split":
-            for wg, groups, ng, nkmax in self.split_launches:
-                _lib.call("psb_rk4_split", *self._common(), device.ptr(self.d_stab),
-                          device.ptr(self.tiles), self.tiles.numel(), device.ptr(groups), ng,
-                          wg, nkmax, device.ptr(self.y), self.n_state, device.ptr(self.ws),
-                          self.ws.numel(), int(nsteps), float(dt), device.ptr(self.P),
-                          self.P.shape[0], int(p_stride), self.p_cap, abi.as_ptr(self.model),
-                          device.stream_ptr(stream))
+            main = stream if stream is not None else torch.cuda.current_stream()
+            streams = [main] + self.side_streams
+            if len(streams) > 1:
+                fork = torch.cuda.Event()
+                fork.record(main)
+                for s in streams[1:]:
+                    s.wait_event(fork)
+            for (wg, groups, ng, nkmax), s in zip(self.split_launches, streams):
+                _lib.call("psb_rk4_split", *self._common(), device.ptr(groups), ng, wg, nkmax,
+                          device.ptr(self.y), self.n_state, device.ptr(self.ws), self.ws.numel(),
+                          int(nsteps), float(dt), device.ptr(self.P), self.P.shape[0],
+                          int(p_stride), self.p_cap, abi.as_ptr(self.model),
+                          device.stream_ptr(s))
+            for s in streams[1:]:
+                join = torch.cuda.Event()
+                join.record(s)
+                main.wait_event(join)
             return
         for order, nkmax, flags in self.classes:
             _lib.call("psb_rk4_f64", *self._common(), device.ptr(order), order.numel(),

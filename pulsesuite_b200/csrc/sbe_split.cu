@@ -6,22 +6,26 @@
 //     D[k][(w,v)] = sum_k' T[k][k'] X[k'][(w,v)],   T[k][k'] = V(|k-k'|)/vscale
 // with X the stage state (v: p_re, p_im, ne, nh).  T and X are split into
 // bf16 hi + lo parts and D = Th Xh + Th Xl + Tl Xh is accumulated in FP32 in
-// tensor memory (the lo*lo term is below FP32 resolution of the sum).
+// tensor memory (Tl Xl is below the FP32 resolution of the sum).
 //
-// One CTA owns a group of W wires for all `nsteps` RK4 steps:
+// One CTA owns a group of W (4, 8 or 16) wires for all `nsteps` RK4 steps:
 //   * X (bf16 hi and lo, the MMA B operand, N = 4W columns, wire-major) lives
 //     in shared memory for the whole call;
-//   * the T tiles (MMA A operand, 128 k rows x 64 k' per tile, built once per
-//     grid by psb_split_prepare and L2-resident) stream through a two-slot
-//     ring filled with cp.async.bulk by a producer warp;
-//   * one thread of the MMA warp issues tcgen05.mma (M = 128, N = 4W, K = 16)
-//     into one TMEM accumulator block per 128-row tile of k;
-//   * eight epilogue warps read the accumulators (tcgen05.ld), evaluate the
-//     diagonal SBE right-hand side in FP32, combine the RK4 stages in FP64
-//     (stage order of libpulsesuite/integrator.py:143-157), and write the next
-//     stage's X back into shared memory.
+//   * T is Toeplitz, so it is never stored as a matrix: each 128 x 64 tile
+//     of the MMA A operand is generated straight into tensor memory from a
+//     table of bf16 pairs (Tv(d), Tv(d-1)) in shared memory -- one 32-bit
+//     lookup per TMEM cell -- double buffered, and the MMA reads A from TMEM;
+//   * one thread issues tcgen05.mma (M = 128, N = 4W, K = 16) into one TMEM
+//     accumulator block per 128-row tile of k;
+//   * eight warps generate the T tiles during the MMA phase and, once the
+//     accumulators are complete, evaluate the diagonal SBE right-hand side,
+//     combine the RK4 stages (stage order of libpulsesuite/integrator.py:
+//     143-157) and write the next stage's X back into shared memory.
+// The right-hand side and the stage state are FP64 (O(Nk) work per wire);
+// only the O(Nk^2) exchange contraction runs in split bf16.
 // Every mbarrier wait is bounded; on a timeout the CTA records
-// PSB_ERR_TIMEOUT in its wires' status, drains, frees TMEM and returns.
+// PSB_ERR_TIMEOUT in its wires' status, waits for its MMAs, frees TMEM and
+// returns.
 #include <cuda_bf16.h>
 #include <math.h>
 
@@ -31,14 +35,15 @@ namespace psb {
 namespace split {
 
 constexpr int kEpiWarps = 8;
-constexpr int kProducerWarp = 8;
-constexpr int kMmaWarp = 9;
-constexpr int kThreadsS = 32 * 10;
-constexpr int kNSlot = 2;
-constexpr int kTileRows = 128;  // M of one MMA / rows of a T tile
-constexpr int kTileK = 64;      // k' per T tile
-constexpr int kLimbBytes = kTileRows * kTileK * 2;  // 16 KiB per bf16 limb
+constexpr int kMmaWarp = 8;
+constexpr int kThreadsS = 32 * 9;
+constexpr int kTileRows = 128;  // M of one MMA
+constexpr int kTileK = 64;      // k' per generated A tile
+constexpr int kACols = kTileK / 2;  // TMEM columns of one bf16 limb of an A tile
 constexpr uint32_t kSpinLimit = 1u << 26;
+// dynamic shared memory per CTA (the 227 KiB limit less the static reduction
+// buffer and its alignment padding)
+constexpr uint32_t kMaxDynSmem = 226 * 1024;
 
 // ---------------------------------------------------------------------------
 // PTX helpers.
@@ -50,10 +55,8 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
                : "memory");
 }
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-               "r"(bytes)
-               : "memory");
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   uint32_t ok;
@@ -66,7 +69,8 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait; false when the limit ran out or another role aborted.
+// Bounded wait; false when the limit ran out (which also sets abort) or
+// another role aborted.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort) {
   for (uint32_t i = 0; i < kSpinLimit; ++i) {
     if (mbar_try_wait(bar, parity)) return true;
@@ -75,23 +79,16 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volati
   *abort = 1;
   return false;
 }
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes,
-                                         uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
-          "r"(smem_u32(dst)),
-      "l"(src), "r"(bytes), "r"(smem_u32(bar))
-      : "memory");
-}
-__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
-                                          uint32_t idesc, uint32_t accum) {
+// D[tmem] (+)= A[tmem] * B[smem desc]
+__device__ __forceinline__ void umma_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t bdesc,
+                                        uint32_t idesc, uint32_t accum) {
   uint32_t m0 = 0, m1 = 0, m2 = 0, m3 = 0;
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(
           d_tmem),
-      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum), "r"(m0), "r"(m1), "r"(m2), "r"(m3));
+      "r"(a_tmem), "l"(bdesc), "r"(idesc), "r"(accum), "r"(m0), "r"(m1), "r"(m2), "r"(m3));
 }
 __device__ __forceinline__ void umma_commit(uint64_t* bar) {
   asm volatile(
@@ -111,18 +108,25 @@ __device__ __forceinline__ void fence_async_smem() {
 __device__ __forceinline__ void named_sync(int id, int nthreads) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
-  uint32_t r[16];
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float* v) {
+  uint32_t r[8];
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15])
+        "=r"(r[7])
       : "r"(taddr));
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+  for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t* r) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
+      "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(taddr),
+      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]),
+      "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]),
+      "r"(r[15])
+      : "memory");
 }
 
 // Shared-memory matrix descriptor, no swizzle (canonical interleaved layout
@@ -133,18 +137,13 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
          ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 
-// Instruction descriptor of kind::f16: D f32, A and B bf16, A K-major,
-// B MN-major, M = 128, N = n.
+// Instruction descriptor of kind::f16: D f32, A and B bf16, A K-major
+// (required for A in TMEM), B MN-major, M = 128, N = n.
 __host__ __device__ constexpr uint32_t idesc_bf16(int n) {
   return (1u << 4) | (1u << 7) | (1u << 10) | (1u << 16) | ((uint32_t)(n >> 3) << 17) |
          ((uint32_t)(kTileRows >> 4) << 24);
 }
 
-// Byte offset of element (row r, k c) in a 128 x 64 T tile (K-major):
-// K-groups of 8 at 2048 B, row groups of 8 at 128 B, rows at 16 B.
-__host__ __device__ __forceinline__ uint32_t tile_off(int r, int c) {
-  return (uint32_t)((c >> 3) * 2048 + (r >> 3) * 128 + (r & 7) * 16 + (c & 7) * 2);
-}
 // Byte offset of element (k, col) in the X operand (MN-major, N columns
 // contiguous inside a core matrix): column groups at sbo, k groups at 128 B.
 __device__ __forceinline__ uint32_t x_off(int k, int col, uint32_t sbo) {
@@ -153,6 +152,13 @@ __device__ __forceinline__ uint32_t x_off(int k, int col, uint32_t sbo) {
 
 __host__ __device__ inline int kpad_of(int nk) { return (nk + kTileK - 1) / kTileK * kTileK; }
 __host__ __device__ inline int mtiles_of(int nk) { return (nk + kTileRows - 1) / kTileRows; }
+// TMEM columns: accumulators (mtiles x N) then two A buffers (hi + lo limbs).
+__host__ __device__ inline int tmem_cols(int nk, int n) {
+  int need = mtiles_of(nk) * n + 4 * kACols;
+  int c = 32;
+  while (c < need) c <<= 1;
+  return c;
+}
 
 struct Args {
   const PsbTable* tables;
@@ -161,14 +167,11 @@ struct Args {
   int64_t n_tabdata;
   PsbWire* wires;
   int nw;
-  const PsbSplitTable* stab;
-  const uint8_t* tiles;
-  int64_t n_tiles;
   const PsbSplitGroup* groups;
   int ngroups;
   double* y;
   int64_t n_state;
-  float4* ws_ys;
+  double4* ws_ys;
   double4* ws_acc;
   int nsteps;
   double dt;
@@ -182,18 +185,22 @@ struct Args {
 template <int W>
 struct Layout {
   static constexpr int N = 4 * W;
-  uint32_t x_hi, x_lo, ring, bars, misc, total;
-  __host__ __device__ Layout(int kpad) {
-    uint32_t xb = (uint32_t)kpad * N * 2;
+  uint32_t x_hi, x_lo, tab, bars, misc, total;
+  int ntab_words;
+  __host__ __device__ Layout(int nk) {
+    const int kpad = kpad_of(nk), nM = mtiles_of(nk);
+    const uint32_t xb = (uint32_t)kpad * N * 2;
     x_hi = 0;
     x_lo = x_hi + xb;
-    ring = x_lo + xb;
-    bars = ring + kNSlot * 2 * kLimbBytes;
-    misc = bars + 8 * (2 * kNSlot + 2);  // full[], empty[], dready, final
-    // misc: tmem base (16 B), abort (16 B), M re/im float2[W], wire params
-    // (gap, gamma, mscale, pscale: float4[W]), t double[W], off int64[W],
-    // P partials double[2][4][W]
-    total = misc + 32 + 8 * W + 16 * W + 8 * W + 8 * W + 64 * W;
+    tab = x_lo + xb;
+    ntab_words = kTileRows * nM + kpad;
+    bars = tab + 2 * 4 * (uint32_t)ntab_words;  // hi and lo pair tables
+    bars = (bars + 15) & ~15u;
+    misc = bars + 8 * 8;  // afull[2], afree[2], dready, final
+    // misc: tmem base (16 B), abort + snapshots (16 B), M re/im double2[W],
+    // wire params (gap, gamma, mscale, pscale: double4[W]), t double[W],
+    // off int64[W], P partials double[2][4][W]
+    total = misc + 32 + 128 * W;
   }
 };
 
@@ -201,8 +208,9 @@ struct Layout {
 // The kernel.
 // ---------------------------------------------------------------------------
 template <int W>
-__global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
+__global__ void __launch_bounds__(kThreadsS, W <= 8 ? 2 : 1) split_rk4_kernel(Args a) {
   constexpr int N = 4 * W;
+  constexpr int WH = W / 2;  // wires per epilogue warp
   extern __shared__ __align__(1024) uint8_t smem[];
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
@@ -211,19 +219,14 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   // ---- validate the group (uniform across the CTA) -------------------------
   bool ok = grp.table >= 0 && grp.table < a.ntab && grp.nw >= 1 && grp.nw <= W;
   PsbTable tb{};
-  PsbSplitTable st{};
   if (ok) {
     tb = a.tables[grp.table];
-    st = a.stab[grp.table];
-    ok = tb.nk >= 2 && tb.nk <= PSB_MAX_NK && st.kpad == kpad_of(tb.nk) &&
-         (st.tile_off & 15) == 0 && st.kpad * N * 4 <= 128 * 1024 &&
-         st.mtiles == mtiles_of(tb.nk) && st.mtiles * N <= 512 && st.tile_off >= 0 &&
-         st.tile_off + (int64_t)st.mtiles * (st.kpad / kTileK) * 2 * kLimbBytes <= a.n_tiles &&
+    ok = tb.nk >= 2 && tb.nk <= PSB_MAX_NK && mtiles_of(tb.nk) * N + 4 * kACols <= 512 &&
          tb.off >= 0 && tb.off + 9 * (int64_t)tb.nk <= a.n_tabdata &&
          (tb.flags & PSB_TAB_EXCITONS) && (tb.flags & PSB_TAB_SHARED_V) &&
          !(tb.flags & PSB_TAB_SCREENED);
     for (int i = 0; ok && i < grp.nw; ++i) {
-      int wi = grp.wire[i];
+      const int wi = grp.wire[i];
       ok = wi >= 0 && wi < a.nw && a.wires[wi].table == grp.table && a.wires[wi].off >= 0 &&
            a.wires[wi].off + tb.nk <= a.n_state;
     }
@@ -233,35 +236,46 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
       a.wires[grp.wire[tid]].status = PSB_ERR_INVALID;
     return;
   }
-  const int nk = tb.nk, kpad = st.kpad, nM = st.mtiles, nK = kpad / kTileK;
-  const Layout<W> L(kpad);
+  const int nk = tb.nk, kpad = kpad_of(nk), nM = mtiles_of(nk), nK = kpad / kTileK;
+  const Layout<W> L(nk);
   uint8_t* xh = smem + L.x_hi;
   uint8_t* xl = smem + L.x_lo;
-  uint8_t* ring = smem + L.ring;
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.bars);
-  uint64_t* empty = full + kNSlot;
-  uint64_t* dready = empty + kNSlot;
+  uint32_t* tab_hi = reinterpret_cast<uint32_t*>(smem + L.tab);
+  uint32_t* tab_lo = tab_hi + L.ntab_words;
+  uint64_t* afull = reinterpret_cast<uint64_t*>(smem + L.bars);
+  uint64_t* afree = afull + 2;
+  uint64_t* dready = afree + 2;
   uint64_t* final_bar = dready + 1;  // teardown: all MMAs of this CTA done
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + L.misc);
   volatile int* abort = reinterpret_cast<volatile int*>(smem + L.misc + 16);
   // abort as seen at each stage's end barrier (written by one participant
   // before the barrier, read by all after it, so every role breaks together)
   volatile int* snap = reinterpret_cast<volatile int*>(smem + L.misc + 20);
-  float2* Msh = reinterpret_cast<float2*>(smem + L.misc + 32);
-  float4* wpar = reinterpret_cast<float4*>(smem + L.misc + 32 + 8 * W);
-  double* wt = reinterpret_cast<double*>(smem + L.misc + 32 + 24 * W);
-  int64_t* woff = reinterpret_cast<int64_t*>(smem + L.misc + 32 + 32 * W);
-  double* ppart = reinterpret_cast<double*>(smem + L.misc + 32 + 40 * W);
+  double2* Msh = reinterpret_cast<double2*>(smem + L.misc + 32);
+  double4* wpar = reinterpret_cast<double4*>(smem + L.misc + 32 + 16 * W);
+  double* wt = reinterpret_cast<double*>(smem + L.misc + 32 + 48 * W);
+  int64_t* woff = reinterpret_cast<int64_t*>(smem + L.misc + 32 + 56 * W);
+  double* ppart = reinterpret_cast<double*>(smem + L.misc + 32 + 64 * W);
   const uint32_t xsbo = (uint32_t)(kpad / 8) * 128;
+  const double* blk = a.tabdata + tb.off;
+  const double* Ee = blk + 3 * nk;
+  const double* Eh = blk + 4 * nk;
 
   // ---- set-up ---------------------------------------------------------------
+  // vscale: the power of two at or above max V, so T = V/vscale is exact.
+  __shared__ double vmax_w[kThreadsS / 32];
+  double vm = 0.0;
+  for (int qq = 1 + tid; qq < nk; qq += kThreadsS) vm = fmax(vm, fabs(blk[qq]));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) vm = fmax(vm, __shfl_xor_sync(0xffffffffu, vm, o));
+  if (lane == 0) vmax_w[warp] = vm;
   for (uint32_t i = tid * 16; i < 2 * (uint32_t)kpad * N * 2; i += kThreadsS * 16)
     *reinterpret_cast<uint4*>(smem + i) = make_uint4(0, 0, 0, 0);
   if (tid == 0) {
-    for (int s = 0; s < kNSlot; ++s) {
-      mbar_init(&full[s], 1);
-      mbar_init(&empty[s], 1);
-    }
+    mbar_init(&afull[0], kEpiWarps);
+    mbar_init(&afull[1], kEpiWarps);
+    mbar_init(&afree[0], 1);
+    mbar_init(&afree[1], 1);
     mbar_init(dready, 1);
     mbar_init(final_bar, 1);
     *abort = 0;
@@ -272,17 +286,16 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   if (tid < W) {
     if (tid < grp.nw) {
       const PsbWire& w = a.wires[grp.wire[tid]];
-      wpar[tid] = make_float4((float)w.gap, (float)w.gamma, (float)w.mscale, (float)w.pscale);
+      wpar[tid] = make_double4(w.gap, w.gamma, w.mscale, w.pscale);
       wt[tid] = w.t;
       woff[tid] = w.off;
     } else {
-      wpar[tid] = make_float4(0.f, 0.f, 0.f, 0.f);
+      wpar[tid] = make_double4(0.0, 0.0, 0.0, 0.0);
       wt[tid] = 0.0;
       woff[tid] = -1;
     }
   }
-  int ncols = 32;
-  while (ncols < nM * N) ncols <<= 1;
+  const int ncols = tmem_cols(nk, N);
   if (warp == kMmaWarp) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(tmem_slot)),
@@ -293,18 +306,35 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
-
-  const double* blk = a.tabdata + tb.off;
-  const double* Ee = blk + 3 * nk;
-  const double* Eh = blk + 4 * nk;
-  const float vscale = (float)st.vscale;
-  const float inv_hbar = (float)(1.0 / a.hbar);
-  const double h = a.dt;
+  double vmax = 0.0;
+#pragma unroll
+  for (int i = 0; i < kThreadsS / 32; ++i) vmax = fmax(vmax, vmax_w[i]);
+  int ex = 0;
+  frexp(vmax > 0.0 ? vmax : 1.0, &ex);
+  const double vscale = ldexp(1.0, ex);
+  const double inv_vscale = ldexp(1.0, -ex);
+  // Pair tables: word(d) = (Tv(d), Tv(d-1)) for d in [2 - kpad, 128 nM - 1],
+  // Tv(d) = bf16 limb of V(|d|)/vscale (0 at d = 0 and outside the grid).
+  const int dlo = 2 - kpad;
+  auto tv = [&](int d, __nv_bfloat16& hi, __nv_bfloat16& lo) {
+    const int ad = d < 0 ? -d : d;
+    const float v = (ad > 0 && ad < nk) ? (float)(blk[ad] * inv_vscale) : 0.f;
+    hi = __float2bfloat16_rn(v);
+    lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+  };
+  for (int i = tid; i < L.ntab_words; i += kThreadsS) {
+    const int d = dlo + i;
+    __nv_bfloat16 h0, l0, h1, l1;
+    tv(d, h0, l0);
+    tv(d - 1, h1, l1);
+    tab_hi[i] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+    tab_lo[i] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
+  }
 
   // ---- epilogue-role helpers --------------------------------------------------
-  const int q = warp & 3;                // TMEM lane quarter
-  const int hh = warp >> 2;              // wire half
-  const int w0 = hh * (W / 2);           // first wire of this warp
+  const int q = warp & 3;          // TMEM lane quarter
+  const int hh = (warp >> 2) & 1;  // wire half / A column half
+  const int w0 = hh * WH;          // first wire of this warp
   auto store_x = [&](int k, int w, const float v[4]) {
     __nv_bfloat16 hi[4], lo[4];
 #pragma unroll
@@ -312,7 +342,7 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
       hi[c] = __float2bfloat16_rn(v[c]);
       lo[c] = __float2bfloat16_rn(v[c] - __bfloat162float(hi[c]));
     }
-    uint32_t o = x_off(k, 4 * w, xsbo);
+    const uint32_t o = x_off(k, 4 * w, xsbo);
     uint2 ph, pl;
     ph.x = (uint32_t)__bfloat16_as_ushort(hi[0]) | ((uint32_t)__bfloat16_as_ushort(hi[1]) << 16);
     ph.y = (uint32_t)__bfloat16_as_ushort(hi[2]) | ((uint32_t)__bfloat16_as_ushort(hi[3]) << 16);
@@ -322,18 +352,18 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
     *reinterpret_cast<uint2*>(xl + o) = pl;
   };
 
-  // Stage-0 input: X = split(y), ys = y (fp32), for this thread's elements.
+  // Stage-0 input: X = split(y), ys = y, for this thread's elements.
   if (warp < kEpiWarps) {
     for (int mi = 0; mi < nM; ++mi) {
       const int k = mi * kTileRows + 32 * q + lane;
       if (k >= nk) continue;
-      for (int j = 0; j < W / 2; ++j) {
+      for (int j = 0; j < WH; ++j) {
         const int w = w0 + j;
         if (w >= grp.nw) break;
         const int64_t e = woff[w] + k;
         const double4 yv = reinterpret_cast<const double4*>(a.y)[e];
-        float v[4] = {(float)yv.x, (float)yv.y, (float)yv.z, (float)yv.w};
-        a.ws_ys[e] = make_float4(v[0], v[1], v[2], v[3]);
+        const float v[4] = {(float)yv.x, (float)yv.y, (float)yv.z, (float)yv.w};
+        a.ws_ys[e] = yv;
         store_x(k, w, v);
       }
     }
@@ -342,61 +372,35 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   __syncthreads();
 
   const uint32_t idesc = idesc_bf16(N);
-  const int total_iters = a.nsteps * 4;  // stages
+  const int total_stages = a.nsteps * 4;
+  const uint32_t acol0 = (uint32_t)(nM * N);  // first A-buffer column
+  const double h = a.dt;
+  const double hbar = a.hbar;
 
-  if (warp == kProducerWarp) {
-    // ---- producer: stream the T tiles of every stage through the ring -------
-    if (lane == 0) {
-      const uint8_t* tiles = a.tiles + st.tile_off;
-      uint32_t it = 0;
-      for (int s = 0; s < total_iters && !*abort; ++s) {
-        for (int mi = 0; mi < nM && !*abort; ++mi) {
-          for (int kj = 0; kj < nK; ++kj, ++it) {
-            const int slot = it % kNSlot;
-            const uint32_t round = it / kNSlot;
-            if (round > 0 && !mbar_wait(&empty[slot], (round - 1) & 1, abort)) break;
-            uint8_t* dst = ring + slot * 2 * kLimbBytes;
-            const uint8_t* src = tiles + ((size_t)(mi * nK + kj) * 2) * kLimbBytes;
-            mbar_arrive_expect_tx(&full[slot], 2 * kLimbBytes);
-            bulk_g2s(dst, src, kLimbBytes, &full[slot]);
-            bulk_g2s(dst + kLimbBytes, src + kLimbBytes, kLimbBytes, &full[slot]);
-          }
-        }
-      }
-      // Drain: wait (bounded) until the consumer released every slot we
-      // filled, so no bulk copy is in flight when the CTA exits.
-      for (uint32_t j = (it > kNSlot ? it - kNSlot : 0); j < it; ++j) {
-        const int slot = j % kNSlot;
-        for (uint32_t i = 0; i < kSpinLimit; ++i)
-          if (mbar_try_wait(&full[slot], (j / kNSlot) & 1)) break;
-      }
-    }
-  } else if (warp == kMmaWarp) {
+  if (warp == kMmaWarp) {
     // ---- MMA issuer -----------------------------------------------------------
     uint32_t it = 0;
-    for (int s = 0; s < total_iters; ++s) {
+    for (int s = 0; s < total_stages; ++s) {
       if (lane == 0 && !*abort) {
         tc_fence_after();
         for (int mi = 0; mi < nM; ++mi) {
           const uint32_t dcol = tmem + (uint32_t)(mi * N);
           for (int kj = 0; kj < nK; ++kj, ++it) {
-            const int slot = it % kNSlot;
-            if (!mbar_wait(&full[slot], (it / kNSlot) & 1, abort)) break;
+            const int b = it & 1;
+            if (!mbar_wait(&afull[b], (it >> 1) & 1, abort)) break;
             tc_fence_after();
-            const uint32_t ah = smem_u32(ring + slot * 2 * kLimbBytes);
-            const uint32_t al = ah + kLimbBytes;
+            const uint32_t ah = tmem + acol0 + (uint32_t)(b * 2 * kACols);
+            const uint32_t al = ah + kACols;
 #pragma unroll
             for (int ks = 0; ks < kTileK / 16; ++ks) {
               const int k0 = kj * kTileK + ks * 16;
-              const uint64_t dah = smem_desc(ah + ks * 4096, 2048, 128);
-              const uint64_t dal = smem_desc(al + ks * 4096, 2048, 128);
               const uint64_t dbh = smem_desc(smem_u32(xh) + (k0 >> 3) * 128, 128, xsbo);
               const uint64_t dbl = smem_desc(smem_u32(xl) + (k0 >> 3) * 128, 128, xsbo);
-              umma_bf16(dcol, dah, dbh, idesc, (kj | ks) != 0);
-              umma_bf16(dcol, dah, dbl, idesc, 1);
-              umma_bf16(dcol, dal, dbh, idesc, 1);
+              umma_ts(dcol, ah + ks * 8, dbh, idesc, (kj | ks) != 0);
+              umma_ts(dcol, ah + ks * 8, dbl, idesc, 1);
+              umma_ts(dcol, al + ks * 8, dbh, idesc, 1);
             }
-            umma_commit(&empty[slot]);  // slot reusable once these MMAs finish
+            umma_commit(&afree[b]);  // buffer reusable once these MMAs finish
           }
           if (*abort) break;
         }
@@ -408,11 +412,11 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
       if (snap[s & 1]) break;
     }
   } else {
-    // ---- epilogue warps ---------------------------------------------------------
-    for (int s = 0; s < total_iters; ++s) {
+    // ---- generator / epilogue warps -----------------------------------------------
+    uint32_t it = 0;
+    for (int s = 0; s < total_stages; ++s) {
       const int stg = s & 3;
-      // drive of this stage for the group's wires (fp32 is enough: M enters
-      // the RHS as an additive fp32 term)
+      // drive of this stage for the group's wires
       if (warp == 0 && lane < grp.nw) {
         const PsbWire& w = a.wires[grp.wire[lane]];
         const double t = wt[lane] + (stg == 0 ? 0.0 : (stg == 3 ? h : h / 2.0));
@@ -425,96 +429,115 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
           er += env * cs;
           ei += env * sn;
         }
-        Msh[lane] = make_float2((float)(-w.mscale * er), (float)(-w.mscale * ei));
+        Msh[lane] = make_double2(-w.mscale * er, -w.mscale * ei);
+      }
+      // Generate this stage's A tiles into the two TMEM buffers, in the order
+      // the MMA thread consumes them.  Row r = 32q + lane of tile (mi, kj) is
+      // Tv(d0 - c), c = 0..63, d0 = 128 mi + r - 64 kj; TMEM column j of a limb
+      // holds c = 2j, 2j+1, i.e. word(d0 - 2j).  This warp writes columns
+      // 16 hh .. 16 hh + 15 of both limbs.
+      for (int mi = 0; mi < nM && !*abort; ++mi) {
+        for (int kj = 0; kj < nK; ++kj, ++it) {
+          const int b = it & 1;
+          const uint32_t round = it >> 1;
+          if (round > 0 && !mbar_wait(&afree[b], (round - 1) & 1, abort)) break;
+          const int d0 = mi * kTileRows + 32 * q + lane - kj * kTileK;
+          const int base = d0 - 32 * hh - dlo;  // table index of word(d0 - 2*(16 hh))
+          uint32_t rh[16], rl[16];
+#pragma unroll
+          for (int jj = 0; jj < 16; ++jj) {
+            rh[jj] = tab_hi[base - 2 * jj];
+            rl[jj] = tab_lo[base - 2 * jj];
+          }
+          const uint32_t ta = tmem + ((uint32_t)(32 * q) << 16) + acol0 +
+                              (uint32_t)(b * 2 * kACols + 16 * hh);
+          tmem_st16(ta, rh);
+          tmem_st16(ta + kACols, rl);
+          asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&afull[b]);
+        }
       }
       named_sync(2, 32 * kEpiWarps);
       const bool got = mbar_wait(dready, s & 1, abort);
       tc_fence_after();
       if (got) {
-        double pr[W / 2], pim[W / 2];
+        double pr[WH], pim[WH];
 #pragma unroll
-        for (int j = 0; j < W / 2; ++j) pr[j] = pim[j] = 0.0;
+        for (int j = 0; j < WH; ++j) pr[j] = pim[j] = 0.0;
         for (int mi = 0; mi < nM; ++mi) {
           const int k = mi * kTileRows + 32 * q + lane;
-          float d[2 * W];
+          float d[4 * WH];
 #pragma unroll
-          for (int c = 0; c < 2 * W; c += 16)
-            tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(mi * N + 2 * W * hh + c),
-                      d + c);
+          for (int c = 0; c < 4 * WH; c += 8)
+            tmem_ld8(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(mi * N + 4 * WH * hh + c),
+                     d + c);
           if (k >= nk) continue;
-          const float ee = (float)Ee[k], eh = (float)Eh[k];
+          const double ee = Ee[k], eh = Eh[k];
 #pragma unroll
-          for (int j = 0; j < W / 2; ++j) {
+          for (int j = 0; j < WH; ++j) {
             const int w = w0 + j;
             if (w >= grp.nw) break;
             const int64_t e = woff[w] + k;
-            const float4 par = wpar[w];
-            const float2 M = Msh[w];
-            const float4 ys = a.ws_ys[e];
-            // exchange sums (SBEs.py:896-921) and the diagonal RHS
-            // (SBEs.py:1962-1975, 2325-2337, 2623-2636) in fp32
-            const float omr = M.x + vscale * d[4 * j + 0];
-            const float omi = M.y + vscale * d[4 * j + 1];
-            const float se = (ee + par.x) - vscale * d[4 * j + 2];
-            const float sh = eh - vscale * d[4 * j + 3];
-            const float sum = se + sh;
-            const float nn = ys.z + ys.w - 1.0f;
-            const float xr = sum * ys.x - omr * nn;
-            const float xi = sum * ys.y - omi * nn;
-            const float hg = par.y;  // gamma
-            float f[4];
-            f[0] = xi * inv_hbar - hg * ys.x;
-            f[1] = -xr * inv_hbar - hg * ys.y;
-            const float u = omi * ys.x - omr * ys.y;
-            f[2] = 2.0f * u * inv_hbar;
+            const double4 par = wpar[w];
+            const double2 M = Msh[w];
+            const double4 ys = a.ws_ys[e];
+            // exchange sums (SBEs.py:896-921) from the tensor cores, the
+            // diagonal RHS (SBEs.py:1962-1975, 2325-2337, 2623-2636) in fp64
+            const double omr = M.x + vscale * (double)d[4 * j + 0];
+            const double omi = M.y + vscale * (double)d[4 * j + 1];
+            const double se = (ee + par.x) - vscale * (double)d[4 * j + 2];
+            const double sh = eh - vscale * (double)d[4 * j + 3];
+            const double sum = se + sh;
+            const double nn = ys.z + ys.w - 1.0;
+            const double xr = sum * ys.x - omr * nn;
+            const double xi = sum * ys.y - omi * nn;
+            const double hg = par.y;  // gamma
+            double f[4];
+            f[0] = xi / hbar - hg * ys.x;
+            f[1] = -xr / hbar - hg * ys.y;
+            const double u = omi * ys.x - omr * ys.y;
+            f[2] = 2.0 * u / hbar;
             f[3] = f[2];
             // RK4 stage combination in fp64 (integrator.py:143-157):
             // acc = k1 + 2 k2 + 2 k3, y += h/6 (acc + k4)
-            double4 yv = reinterpret_cast<const double4*>(a.y)[e];
+            const double4 yv = reinterpret_cast<const double4*>(a.y)[e];
+            const double yy[4] = {yv.x, yv.y, yv.z, yv.w};
             double4 acc;
             double nxt[4];
-            const double yy[4] = {yv.x, yv.y, yv.z, yv.w};
             if (stg == 0) {
               acc = make_double4(f[0], f[1], f[2], f[3]);
 #pragma unroll
-              for (int c = 0; c < 4; ++c) nxt[c] = yy[c] + (h / 2.0) * (double)f[c];
+              for (int c = 0; c < 4; ++c) nxt[c] = yy[c] + (h / 2.0) * f[c];
             } else if (stg == 3) {
               acc = a.ws_acc[e];
               const double ac[4] = {acc.x, acc.y, acc.z, acc.w};
 #pragma unroll
-              for (int c = 0; c < 4; ++c) nxt[c] = yy[c] + (h / 6.0) * (ac[c] + (double)f[c]);
-              // state stored with p rounded to fp32 (the split form's
-              // working precision), densities in fp64
-              yv = make_double4((double)(float)nxt[0], (double)(float)nxt[1], nxt[2], nxt[3]);
-              reinterpret_cast<double4*>(a.y)[e] = yv;
-              pr[j] += yv.x;
-              pim[j] += yv.y;
+              for (int c = 0; c < 4; ++c) nxt[c] = yy[c] + (h / 6.0) * (ac[c] + f[c]);
+              reinterpret_cast<double4*>(a.y)[e] = make_double4(nxt[0], nxt[1], nxt[2], nxt[3]);
+              pr[j] += nxt[0];
+              pim[j] += nxt[1];
             } else {
               acc = a.ws_acc[e];
-              acc.x += 2.0 * (double)f[0];
-              acc.y += 2.0 * (double)f[1];
-              acc.z += 2.0 * (double)f[2];
-              acc.w += 2.0 * (double)f[3];
+              acc.x += 2.0 * f[0];
+              acc.y += 2.0 * f[1];
+              acc.z += 2.0 * f[2];
+              acc.w += 2.0 * f[3];
               const double c2 = stg == 1 ? h / 2.0 : h;
 #pragma unroll
-              for (int c = 0; c < 4; ++c) nxt[c] = yy[c] + c2 * (double)f[c];
+              for (int c = 0; c < 4; ++c) nxt[c] = yy[c] + c2 * f[c];
             }
             if (stg != 3) a.ws_acc[e] = acc;
-            float v[4] = {(float)nxt[0], (float)nxt[1], (float)nxt[2], (float)nxt[3]};
-            if (stg == 3) {
-              v[0] = (float)yv.x;
-              v[1] = (float)yv.y;
-              v[2] = (float)yv.z;
-              v[3] = (float)yv.w;
-            }
-            a.ws_ys[e] = make_float4(v[0], v[1], v[2], v[3]);
+            const float v[4] = {(float)nxt[0], (float)nxt[1], (float)nxt[2], (float)nxt[3]};
+            a.ws_ys[e] = make_double4(nxt[0], nxt[1], nxt[2], nxt[3]);
             store_x(k, w, v);
           }
         }
         if (stg == 3) {
           // P(t) = pscale * sum_k p_k, reduced in a fixed order
 #pragma unroll
-          for (int j = 0; j < W / 2; ++j) {
+          for (int j = 0; j < WH; ++j) {
             double sr = pr[j], si = pim[j];
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
@@ -544,8 +567,8 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
               sr += ppart[(0 * 4 + qq) * W + w];
               si += ppart[(1 * 4 + qq) * W + w];
             }
-            a.P[2 * (wd.p_off + r)] = (double)wpar[w].w * sr;
-            a.P[2 * (wd.p_off + r) + 1] = (double)wpar[w].w * si;
+            a.P[2 * (wd.p_off + r)] = wpar[w].w * sr;
+            a.P[2 * (wd.p_off + r) + 1] = wpar[w].w * si;
           }
         }
       }
@@ -586,41 +609,21 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   }
 }
 
-// T tiles of one grid: tile (mi, kj) holds rows k = 128 mi + r and columns
-// k' = 64 kj + c of T[k][k'] = V(|k - k'|)/vscale (0 on the diagonal, the
-// excluded q = 0 term, and outside the grid), hi limb then lo limb.
-__global__ void prepare_tiles_kernel(const double* __restrict__ V, int nk, double vscale,
-                                     uint8_t* __restrict__ tiles) {
-  const int kpad = kpad_of(nk), nK = kpad / kTileK, nM = mtiles_of(nk);
-  const int64_t total = (int64_t)nM * nK * kTileRows * kTileK;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const int c = (int)(i % kTileK);
-    const int r = (int)((i / kTileK) % kTileRows);
-    const int64_t t = i / ((int64_t)kTileK * kTileRows);
-    const int kj = (int)(t % nK), mi = (int)(t / nK);
-    const int k = mi * kTileRows + r, kp = kj * kTileK + c;
-    float v = 0.f;
-    if (k < nk && kp < nk && k != kp) v = (float)(V[k > kp ? k - kp : kp - k] / vscale);
-    const __nv_bfloat16 hi = __float2bfloat16_rn(v);
-    const __nv_bfloat16 lo = __float2bfloat16_rn(v - __bfloat162float(hi));
-    uint8_t* tb = tiles + (size_t)(mi * nK + kj) * 2 * kLimbBytes;
-    *reinterpret_cast<__nv_bfloat16*>(tb + tile_off(r, c)) = hi;
-    *reinterpret_cast<__nv_bfloat16*>(tb + kLimbBytes + tile_off(r, c)) = lo;
-  }
-}
-
 template <int W>
-int launch(const Args& a, int kpad_max, cudaStream_t s) {
-  const Layout<W> L(kpad_max);
-  if (L.total > 227 * 1024)
-    return set_error(PSB_ERR_SIZE, "split form: %u bytes of shared memory for kpad %d, W %d",
-                     L.total, kpad_max, W);
+int launch(const Args& a, int nkmax, cudaStream_t s) {
+  uint32_t smem = 0;
+  for (int nk = 2; nk <= nkmax; ++nk) {
+    const uint32_t t = Layout<W>(nk).total;
+    if (t > smem) smem = t;
+  }
+  if (smem > kMaxDynSmem || tmem_cols(nkmax, 4 * W) > 512)
+    return set_error(PSB_ERR_SIZE, "split form: nk %d does not fit a group of %d wires", nkmax,
+                     W);
   cudaError_t e = cudaFuncSetAttribute(split_rk4_kernel<W>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess)
     return set_error(PSB_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
-  split_rk4_kernel<W><<<a.ngroups, kThreadsS, L.total, s>>>(a);
+  split_rk4_kernel<W><<<a.ngroups, kThreadsS, smem, s>>>(a);
   return check_cuda("split_rk4_kernel");
 }
 
@@ -629,52 +632,44 @@ int launch(const Args& a, int kpad_max, cudaStream_t s) {
 
 using namespace psb;
 
-extern "C" int64_t psb_split_tile_bytes(int nk) {
-  if (nk < 2 || nk > PSB_MAX_NK) return set_error(PSB_ERR_SIZE, "nk %d out of range", nk);
-  return (int64_t)split::mtiles_of(nk) * (split::kpad_of(nk) / split::kTileK) * 2 *
-         split::kLimbBytes;
-}
-
 extern "C" int64_t psb_split_ws_bytes(int64_t n_state) {
   if (n_state < 0) return set_error(PSB_ERR_INVALID, "n_state < 0");
-  return 48 * n_state + 32;
+  return 64 * n_state + 32;
 }
 
 extern "C" int psb_split_smem_bytes(int nk, int wgroup) {
   if (nk < 2 || nk > PSB_MAX_NK) return set_error(PSB_ERR_SIZE, "nk %d out of range", nk);
-  const int kp = split::kpad_of(nk);
-  if (wgroup == 16) return (int)split::Layout<16>(kp).total;
-  if (wgroup == 8) return (int)split::Layout<8>(kp).total;
-  return set_error(PSB_ERR_INVALID, "wgroup must be 8 or 16");
+  if (wgroup == 16) return (int)split::Layout<16>(nk).total;
+  if (wgroup == 8) return (int)split::Layout<8>(nk).total;
+  if (wgroup == 4) return (int)split::Layout<4>(nk).total;
+  return set_error(PSB_ERR_INVALID, "wgroup must be 4, 8 or 16");
 }
 
-extern "C" int psb_split_prepare(const double* d_V, int nk, double vscale, void* d_tiles,
-                                 int64_t n_tiles_bytes, void* stream) {
-  if (!d_V || !d_tiles || !(vscale > 0.0))
-    return set_error(PSB_ERR_INVALID, "psb_split_prepare: bad arguments");
-  if (nk < 2 || nk > PSB_MAX_NK) return set_error(PSB_ERR_SIZE, "nk %d out of range", nk);
-  if (((uintptr_t)d_tiles & 15) != 0)
-    return set_error(PSB_ERR_INVALID, "psb_split_prepare: tiles must be 16-byte aligned");
-  if (n_tiles_bytes < psb_split_tile_bytes(nk))
-    return set_error(PSB_ERR_SIZE, "psb_split_prepare: tile buffer too small");
-  split::prepare_tiles_kernel<<<148 * 4, 256, 0, (cudaStream_t)stream>>>(d_V, nk, vscale,
-                                                                          (uint8_t*)d_tiles);
-  return check_cuda("psb_split_prepare");
+extern "C" int psb_split_max_nk(int wgroup) {
+  if (wgroup != 4 && wgroup != 8 && wgroup != 16)
+    return set_error(PSB_ERR_INVALID, "wgroup must be 4, 8 or 16");
+  int best = 0;
+  for (int nk = 2; nk <= PSB_MAX_NK; ++nk) {
+    const uint32_t sm = wgroup == 16 ? split::Layout<16>(nk).total
+                                     : (wgroup == 8 ? split::Layout<8>(nk).total
+                                                    : split::Layout<4>(nk).total);
+    if (sm <= split::kMaxDynSmem && split::tmem_cols(nk, 4 * wgroup) <= 512) best = nk;
+  }
+  return best;
 }
 
 extern "C" int psb_rk4_split(const PsbTable* d_tables, int ntab, const double* d_tabdata,
                              int64_t n_tabdata, PsbWire* d_wires, int nw,
-                             const PsbSplitTable* d_stab, const void* d_tiles,
-                             int64_t n_tiles_bytes, const PsbSplitGroup* d_groups, int ngroups,
-                             int wgroup, int nkmax, double* d_y, int64_t n_state, void* d_ws,
-                             int64_t n_ws_bytes, int nsteps, double dt, double* d_P, int64_t n_P,
-                             int p_stride, int p_cap, const PsbModel* model, void* stream) {
-  if (!d_tables || !d_tabdata || !d_wires || !d_stab || !d_tiles || !d_groups || !d_y ||
-      !d_ws || !model || ntab <= 0 || nw < 0 || ngroups < 0)
+                             const PsbSplitGroup* d_groups, int ngroups, int wgroup, int nkmax,
+                             double* d_y, int64_t n_state, void* d_ws, int64_t n_ws_bytes,
+                             int nsteps, double dt, double* d_P, int64_t n_P, int p_stride,
+                             int p_cap, const PsbModel* model, void* stream) {
+  if (!d_tables || !d_tabdata || !d_wires || !d_groups || !d_y || !d_ws || !model || ntab <= 0 ||
+      nw < 0 || ngroups < 0)
     return set_error(PSB_ERR_INVALID, "psb_rk4_split: null pointer or bad count");
-  if (wgroup != 8 && wgroup != 16)
-    return set_error(PSB_ERR_INVALID, "psb_rk4_split: wgroup must be 8 or 16");
-  if (nkmax < 2 || nkmax > PSB_MAX_NK || (wgroup == 16 && nkmax > 512))
+  if (wgroup != 4 && wgroup != 8 && wgroup != 16)
+    return set_error(PSB_ERR_INVALID, "psb_rk4_split: wgroup must be 4, 8 or 16");
+  if (nkmax < 2 || nkmax > psb_split_max_nk(wgroup))
     return set_error(PSB_ERR_SIZE, "psb_rk4_split: nkmax %d too large for wgroup %d", nkmax,
                      wgroup);
   if (n_ws_bytes < psb_split_ws_bytes(n_state))
@@ -691,15 +686,12 @@ extern "C" int psb_rk4_split(const PsbTable* d_tables, int ntab, const double* d
   a.n_tabdata = n_tabdata;
   a.wires = d_wires;
   a.nw = nw;
-  a.stab = d_stab;
-  a.tiles = (const uint8_t*)d_tiles;
-  a.n_tiles = n_tiles_bytes;
   a.groups = d_groups;
   a.ngroups = ngroups;
   a.y = d_y;
   a.n_state = n_state;
-  a.ws_ys = (float4*)d_ws;
-  a.ws_acc = (double4*)((uint8_t*)d_ws + ((16 * n_state + 31) & ~(int64_t)31));
+  a.ws_ys = (double4*)d_ws;
+  a.ws_acc = (double4*)((uint8_t*)d_ws + 32 * n_state);
   a.nsteps = nsteps;
   a.dt = dt;
   a.P = d_P;
@@ -707,7 +699,7 @@ extern "C" int psb_rk4_split(const PsbTable* d_tables, int ntab, const double* d
   a.p_stride = p_stride;
   a.p_cap = p_cap;
   a.hbar = model->hbar;
-  const int kp = split::kpad_of(nkmax);
-  return wgroup == 16 ? split::launch<16>(a, kp, (cudaStream_t)stream)
-                      : split::launch<8>(a, kp, (cudaStream_t)stream);
+  if (wgroup == 16) return split::launch<16>(a, nkmax, (cudaStream_t)stream);
+  if (wgroup == 8) return split::launch<8>(a, nkmax, (cudaStream_t)stream);
+  return split::launch<4>(a, nkmax, (cudaStream_t)stream);
 }
