@@ -43,7 +43,9 @@ def parse():
     ap.add_argument("--workload", default="c1", choices=["c1", "c2", "c3"])
     ap.add_argument("--chunk", type=int, default=100, help="time steps per bench step")
     ap.add_argument("--form", default="plain", choices=["plain", "split"],
-                    help="plain FP64 kernel or split bf16x3 tensor-core kernel")
+                    help="plain FP64 kernel or split hi+lo tensor-core kernel")
+    ap.add_argument("--limb", default="bf16", choices=["bf16", "fp16"],
+                    help="16-bit limb format of the split form")
     ap.add_argument("--nwires", type=int, default=0, help="override the workload's wire count")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -195,7 +197,8 @@ def run_ours(a):
 
     wl = make_workload(a.workload, rank, a.nwires)
     S = a.chunk
-    b = WireBatch(wl.grids, wl.wires, screened=wl.screened, p_cap=S, form=a.form)
+    b = WireBatch(wl.grids, wl.wires, screened=wl.screened, p_cap=S, form=a.form,
+                  limb=a.limb)
     stream = torch.cuda.current_stream()
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
     units = wl.units_per_step * S
@@ -270,7 +273,7 @@ def run_ours(a):
 
     line = {
         "metric": ("SBE wire*k*steps/s (plain FP64 RK4)" if a.form == "plain" else
-                   "SBE wire*k*steps/s (split bf16x3 tensor-core RK4)"),
+                   f"SBE wire*k*steps/s (split {a.limb}x3 tensor-core RK4)"),
         "value": value,
         "unit": "wire*k*steps/s",
         "n_gpus": world,
@@ -280,7 +283,7 @@ def run_ours(a):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64" if a.form == "plain" else "bf16x3+f32acc+f64",
+        "dtype": "f64" if a.form == "plain" else f"{a.limb}x3+f32acc+f64",
         "data": "synthetic (seeded configuration draws)",
         "config": {"workload": wl.name, "wires_per_gpu": len(wl.wires),
                    "wire_k_per_time_step": wl.units_per_step, "time_steps_per_bench_step": S,

@@ -228,13 +228,17 @@ int psb_f64_smem_bytes(int nk, int tab_flags);
  * The batched form of the same RK4 step: per group of wires sharing one k
  * grid, the exchange sums of all wires are one contraction
  *   D[k][(w,v)] = sum_k' T[k][k'] X[k'][(w,v)],  T[k][k'] = V(|k-k'|)/vscale,
- * computed on the tensor cores as bf16 hi+lo split products (Th Xh + Th Xl +
- * Tl Xh) accumulated in FP32, with vscale the power of two at or above
- * max V.  The O(Nk) right-hand side, the RK4 stage combination, the state and
+ * computed on the tensor cores as hi+lo split products of 16-bit limbs
+ * (Th Xh + Th Xl + Tl Xh; bf16 or fp16 limbs) accumulated in FP32, with
+ * vscale the power of two at or above max V.  The O(Nk) right-hand side, the RK4 stage combination, the state and
  * the P(t) sums stay FP64 (FP64 layout of the plain form).
  * Requires PSB_TAB_EXCITONS | PSB_TAB_SHARED_V tables without screening.
  */
 #define PSB_SPLIT_WMAX 16
+/* 16-bit limb format of the split: bf16 (hi+lo ~ 16 significant bits) or
+ * fp16 (hi+lo ~ 22 significant bits; same tensor-core rate). */
+#define PSB_LIMB_BF16 0
+#define PSB_LIMB_FP16 1
 /* One CTA's work: 1..wgroup wires of one table (same k grid). */
 typedef struct PsbSplitGroup {
   int32_t table;
@@ -260,7 +264,7 @@ int psb_split_max_nk(int wgroup);
  */
 int psb_rk4_split(const PsbTable* d_tables, int ntab, const double* d_tabdata, int64_t n_tabdata,
                   PsbWire* d_wires, int nw, const PsbSplitGroup* d_groups, int ngroups,
-                  int wgroup, int nkmax, double* d_y, int64_t n_state, void* d_ws,
+                  int wgroup, int nkmax, int limb, double* d_y, int64_t n_state, void* d_ws,
                   int64_t n_ws_bytes, int nsteps, double dt, double* d_P, int64_t n_P,
                   int p_stride, int p_cap, const PsbModel* model, void* stream);
 

@@ -24,11 +24,14 @@ class WireBatch:
     right-hand side and FP64 stage combination, psb_rk4_split)."""
 
     def __init__(self, grids, wires, screened=False, excitons=True, p_cap=0, tables=None,
-                 tabdata=None, form="plain"):
+                 tabdata=None, form="plain", limb="bf16"):
         device.require_cuda()
         if form not in ("plain", "split"):
             raise ValueError("form must be 'plain' or 'split'")
+        if limb not in ("bf16", "fp16"):
+            raise ValueError("limb must be 'bf16' or 'fp16'")
         self.form = form
+        self.limb = abi.PSB_LIMB_FP16 if limb == "fp16" else abi.PSB_LIMB_BF16
         self.grids = list(grids)
         self.screened = bool(screened)
         if tables is None:
@@ -183,7 +186,7 @@ class WireBatch:
                     s.wait_event(fork)
             for (wg, groups, ng, nkmax), s in zip(self.split_launches, streams):
                 _lib.call("psb_rk4_split", *self._common(), device.ptr(groups), ng, wg, nkmax,
-                          device.ptr(self.y), self.n_state, device.ptr(self.ws), self.ws.numel(),
+                          self.limb, device.ptr(self.y), self.n_state, device.ptr(self.ws), self.ws.numel(),
                           int(nsteps), float(dt), device.ptr(self.P), self.P.shape[0],
                           int(p_stride), self.p_cap, abi.as_ptr(self.model),
                           device.stream_ptr(s))

@@ -27,6 +27,7 @@
 // PSB_ERR_TIMEOUT in its wires' status, waits for its MMAs, frees TMEM and
 // returns.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <math.h>
 
 #include "psb_common.cuh"
@@ -129,6 +130,28 @@ __device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t* r) {
       : "memory");
 }
 
+// One 16-bit limb of the split: bf16 (8 significant bits) or fp16 (11
+// significant bits; values are O(1) after the vscale normalisation).
+template <bool F16>
+__device__ __forceinline__ uint16_t limb_bits(float v, float& back) {
+  if (F16) {
+    const __half hv = __float2half_rn(v);
+    back = __half2float(hv);
+    return __half_as_ushort(hv);
+  }
+  const __nv_bfloat16 bv = __float2bfloat16_rn(v);
+  back = __bfloat162float(bv);
+  return __bfloat16_as_ushort(bv);
+}
+// hi and lo limbs of v (v ~ hi + lo)
+template <bool F16>
+__device__ __forceinline__ void split2(float v, uint16_t& hi, uint16_t& lo) {
+  float b;
+  hi = limb_bits<F16>(v, b);
+  float b2;
+  lo = limb_bits<F16>(v - b, b2);
+}
+
 // Shared-memory matrix descriptor, no swizzle (canonical interleaved layout
 // of 8 x 16-byte core matrices): start address, leading-dimension (K) and
 // stride-dimension (M/N) byte offsets, descriptor version 1.
@@ -137,11 +160,12 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
          ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 
-// Instruction descriptor of kind::f16: D f32, A and B bf16, A K-major
-// (required for A in TMEM), B MN-major, M = 128, N = n.
-__host__ __device__ constexpr uint32_t idesc_bf16(int n) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | (1u << 16) | ((uint32_t)(n >> 3) << 17) |
-         ((uint32_t)(kTileRows >> 4) << 24);
+// Instruction descriptor of kind::f16: D f32, A and B bf16 (format 1) or
+// fp16 (format 0), A K-major (required for A in TMEM), B MN-major, M = 128,
+// N = n.
+__host__ __device__ constexpr uint32_t idesc_f16(int n, bool f16) {
+  return (1u << 4) | ((f16 ? 0u : 1u) << 7) | ((f16 ? 0u : 1u) << 10) | (1u << 16) |
+         ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kTileRows >> 4) << 24);
 }
 
 // Byte offset of element (k, col) in the X operand (MN-major, N columns
@@ -207,7 +231,7 @@ struct Layout {
 // ---------------------------------------------------------------------------
 // The kernel.
 // ---------------------------------------------------------------------------
-template <int W>
+template <int W, bool F16>
 __global__ void __launch_bounds__(kThreadsS, W <= 8 ? 2 : 1) split_rk4_kernel(Args a) {
   constexpr int N = 4 * W;
   constexpr int WH = W / 2;  // wires per epilogue warp
@@ -316,19 +340,18 @@ __global__ void __launch_bounds__(kThreadsS, W <= 8 ? 2 : 1) split_rk4_kernel(Ar
   // Pair tables: word(d) = (Tv(d), Tv(d-1)) for d in [2 - kpad, 128 nM - 1],
   // Tv(d) = bf16 limb of V(|d|)/vscale (0 at d = 0 and outside the grid).
   const int dlo = 2 - kpad;
-  auto tv = [&](int d, __nv_bfloat16& hi, __nv_bfloat16& lo) {
+  auto tv = [&](int d, uint16_t& hi, uint16_t& lo) {
     const int ad = d < 0 ? -d : d;
     const float v = (ad > 0 && ad < nk) ? (float)(blk[ad] * inv_vscale) : 0.f;
-    hi = __float2bfloat16_rn(v);
-    lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+    split2<F16>(v, hi, lo);
   };
   for (int i = tid; i < L.ntab_words; i += kThreadsS) {
     const int d = dlo + i;
-    __nv_bfloat16 h0, l0, h1, l1;
+    uint16_t h0, l0, h1, l1;
     tv(d, h0, l0);
     tv(d - 1, h1, l1);
-    tab_hi[i] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
-    tab_lo[i] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
+    tab_hi[i] = (uint32_t)h0 | ((uint32_t)h1 << 16);
+    tab_lo[i] = (uint32_t)l0 | ((uint32_t)l1 << 16);
   }
 
   // ---- epilogue-role helpers --------------------------------------------------
@@ -336,18 +359,15 @@ __global__ void __launch_bounds__(kThreadsS, W <= 8 ? 2 : 1) split_rk4_kernel(Ar
   const int hh = (warp >> 2) & 1;  // wire half / A column half
   const int w0 = hh * WH;          // first wire of this warp
   auto store_x = [&](int k, int w, const float v[4]) {
-    __nv_bfloat16 hi[4], lo[4];
+    uint16_t hi[4], lo[4];
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      hi[c] = __float2bfloat16_rn(v[c]);
-      lo[c] = __float2bfloat16_rn(v[c] - __bfloat162float(hi[c]));
-    }
+    for (int c = 0; c < 4; ++c) split2<F16>(v[c], hi[c], lo[c]);
     const uint32_t o = x_off(k, 4 * w, xsbo);
     uint2 ph, pl;
-    ph.x = (uint32_t)__bfloat16_as_ushort(hi[0]) | ((uint32_t)__bfloat16_as_ushort(hi[1]) << 16);
-    ph.y = (uint32_t)__bfloat16_as_ushort(hi[2]) | ((uint32_t)__bfloat16_as_ushort(hi[3]) << 16);
-    pl.x = (uint32_t)__bfloat16_as_ushort(lo[0]) | ((uint32_t)__bfloat16_as_ushort(lo[1]) << 16);
-    pl.y = (uint32_t)__bfloat16_as_ushort(lo[2]) | ((uint32_t)__bfloat16_as_ushort(lo[3]) << 16);
+    ph.x = (uint32_t)hi[0] | ((uint32_t)hi[1] << 16);
+    ph.y = (uint32_t)hi[2] | ((uint32_t)hi[3] << 16);
+    pl.x = (uint32_t)lo[0] | ((uint32_t)lo[1] << 16);
+    pl.y = (uint32_t)lo[2] | ((uint32_t)lo[3] << 16);
     *reinterpret_cast<uint2*>(xh + o) = ph;
     *reinterpret_cast<uint2*>(xl + o) = pl;
   };
@@ -371,7 +391,7 @@ __global__ void __launch_bounds__(kThreadsS, W <= 8 ? 2 : 1) split_rk4_kernel(Ar
   }
   __syncthreads();
 
-  const uint32_t idesc = idesc_bf16(N);
+  const uint32_t idesc = idesc_f16(N, F16);
   const int total_stages = a.nsteps * 4;
   const uint32_t acol0 = (uint32_t)(nM * N);  // first A-buffer column
   const double h = a.dt;
@@ -609,7 +629,7 @@ __global__ void __launch_bounds__(kThreadsS, W <= 8 ? 2 : 1) split_rk4_kernel(Ar
   }
 }
 
-template <int W>
+template <int W, bool F16>
 int launch(const Args& a, int nkmax, cudaStream_t s) {
   uint32_t smem = 0;
   for (int nk = 2; nk <= nkmax; ++nk) {
@@ -619,11 +639,11 @@ int launch(const Args& a, int nkmax, cudaStream_t s) {
   if (smem > kMaxDynSmem || tmem_cols(nkmax, 4 * W) > 512)
     return set_error(PSB_ERR_SIZE, "split form: nk %d does not fit a group of %d wires", nkmax,
                      W);
-  cudaError_t e = cudaFuncSetAttribute(split_rk4_kernel<W>,
+  cudaError_t e = cudaFuncSetAttribute(split_rk4_kernel<W, F16>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess)
     return set_error(PSB_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
-  split_rk4_kernel<W><<<a.ngroups, kThreadsS, smem, s>>>(a);
+  split_rk4_kernel<W, F16><<<a.ngroups, kThreadsS, smem, s>>>(a);
   return check_cuda("split_rk4_kernel");
 }
 
@@ -661,7 +681,8 @@ extern "C" int psb_split_max_nk(int wgroup) {
 extern "C" int psb_rk4_split(const PsbTable* d_tables, int ntab, const double* d_tabdata,
                              int64_t n_tabdata, PsbWire* d_wires, int nw,
                              const PsbSplitGroup* d_groups, int ngroups, int wgroup, int nkmax,
-                             double* d_y, int64_t n_state, void* d_ws, int64_t n_ws_bytes,
+                             int limb, double* d_y, int64_t n_state, void* d_ws,
+                             int64_t n_ws_bytes,
                              int nsteps, double dt, double* d_P, int64_t n_P, int p_stride,
                              int p_cap, const PsbModel* model, void* stream) {
   if (!d_tables || !d_tabdata || !d_wires || !d_groups || !d_y || !d_ws || !model || ntab <= 0 ||
@@ -669,6 +690,8 @@ extern "C" int psb_rk4_split(const PsbTable* d_tables, int ntab, const double* d
     return set_error(PSB_ERR_INVALID, "psb_rk4_split: null pointer or bad count");
   if (wgroup != 4 && wgroup != 8 && wgroup != 16)
     return set_error(PSB_ERR_INVALID, "psb_rk4_split: wgroup must be 4, 8 or 16");
+  if (limb != PSB_LIMB_BF16 && limb != PSB_LIMB_FP16)
+    return set_error(PSB_ERR_INVALID, "psb_rk4_split: limb must be PSB_LIMB_BF16 or _FP16");
   if (nkmax < 2 || nkmax > psb_split_max_nk(wgroup))
     return set_error(PSB_ERR_SIZE, "psb_rk4_split: nkmax %d too large for wgroup %d", nkmax,
                      wgroup);
@@ -699,7 +722,13 @@ extern "C" int psb_rk4_split(const PsbTable* d_tables, int ntab, const double* d
   a.p_stride = p_stride;
   a.p_cap = p_cap;
   a.hbar = model->hbar;
-  if (wgroup == 16) return split::launch<16>(a, nkmax, (cudaStream_t)stream);
-  if (wgroup == 8) return split::launch<8>(a, nkmax, (cudaStream_t)stream);
-  return split::launch<4>(a, nkmax, (cudaStream_t)stream);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (limb == PSB_LIMB_FP16) {
+    if (wgroup == 16) return split::launch<16, true>(a, nkmax, st);
+    if (wgroup == 8) return split::launch<8, true>(a, nkmax, st);
+    return split::launch<4, true>(a, nkmax, st);
+  }
+  if (wgroup == 16) return split::launch<16, false>(a, nkmax, st);
+  if (wgroup == 8) return split::launch<8, false>(a, nkmax, st);
+  return split::launch<4, false>(a, nkmax, st);
 }

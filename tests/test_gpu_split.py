@@ -37,26 +37,28 @@ def test_split_small_single_wire(cuda):
     assert relerr(y[:, 2], yo[:, 2]) < TOL_STATE
 
 
-def test_split_uneven_batch_vs_oracle(cuda):
+@pytest.mark.parametrize("limb", ["bf16", "fp16"])
+def test_split_uneven_batch_vs_oracle(cuda, limb):
     nks = [64, 512, 96, 128, 320, 64, 256, 480, 160, 1024, 64, 512, 128, 96, 1024, 256,
            64, 64, 64, 64, 64, 64, 64, 64, 64, 64, 64, 64, 64, 64, 64, 64, 64]
     grids, w = uneven_case(nks, seed=21, nsteps=300)
     n, dt = 300, 1e-15
-    b = WireBatch(grids, w, p_cap=n, form="split")
+    b = WireBatch(grids, w, p_cap=n, form="split", limb=limb)
     b.rk4(n, dt)
     st = b.wires()
     assert (st["status"] == 0).all(), st["status"]
     y = b.state()
     yo, Po, _ = oracle_run(grids, w, n, dt)
-    worst = 0.0
+    allerrs = []
     for i in range(len(nks)):
         s = b.wire_slice(i)
-        errs = [relerr(b.records(i), Po[i]),
-                relerr(y[s, 0] + 1j * y[s, 1], yo[s, 0] + 1j * yo[s, 1]),
-                relerr(y[s, 2], yo[s, 2]), relerr(y[s, 3], yo[s, 3])]
-        worst = max(worst, max(errs[1:]))
-        assert errs[0] < TOL and max(errs[1:]) < TOL_STATE, (i, nks[i], errs)
-    print("worst split state error", worst)
+        allerrs.append([relerr(b.records(i), Po[i]),
+                        relerr(y[s, 0] + 1j * y[s, 1], yo[s, 0] + 1j * yo[s, 1]),
+                        relerr(y[s, 2], yo[s, 2]), relerr(y[s, 3], yo[s, 3])])
+    e = np.array(allerrs)
+    print(f"split {limb}: max P err {e[:, 0].max():.2e}, max state err {e[:, 1:].max():.2e}")
+    tol_p, tol_s = (TOL, TOL_STATE) if limb == "fp16" else (3 * TOL, 3 * TOL_STATE)
+    assert e[:, 0].max() < tol_p and e[:, 1:].max() < tol_s, e
 
 
 def test_split_full_config0_vs_reference(cuda):
