@@ -5,8 +5,10 @@
 // 896-921) are, for W wires sharing one k grid, one dense contraction
 //     D[k][(w,v)] = sum_k' T[k][k'] X[k'][(w,v)],   T[k][k'] = V(|k-k'|)/vscale
 // with X the stage state (v: p_re, p_im, ne, nh).  T and X are split into
-// bf16 hi + lo parts and D = Th Xh + Th Xl + Tl Xh is accumulated in FP32 in
-// tensor memory (Tl Xl is below the FP32 resolution of the sum).
+// bf16 hi + lo parts and D = Th Xh + (Th Xl + Tl Xh) is accumulated in FP32
+// in tensor memory, the main product and the two corrections in separate
+// accumulators that the epilogue adds in FP64 (Tl Xl is below the FP32
+// resolution of the sum).
 //
 // One CTA owns a group of W (4, 8 or 16) wires for all `nsteps` RK4 steps:
 //   * X (bf16 hi and lo, the MMA B operand, N = 4W columns, wire-major) lives
@@ -109,16 +111,17 @@ __device__ __forceinline__ void fence_async_smem() {
 __device__ __forceinline__ void named_sync(int id, int nthreads) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
-__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float* v) {
-  uint32_t r[8];
+// 8 consecutive TMEM columns of this thread's lane (no wait: pair with
+// tmem_ld_wait before the registers are used)
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t* r) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
         "=r"(r[7])
       : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_ld_wait() {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
 }
 __device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t* r) {
   asm volatile(
@@ -176,9 +179,15 @@ __device__ __forceinline__ uint32_t x_off(int k, int col, uint32_t sbo) {
 
 __host__ __device__ inline int kpad_of(int nk) { return (nk + kTileK - 1) / kTileK * kTileK; }
 __host__ __device__ inline int mtiles_of(int nk) { return (nk + kTileRows - 1) / kTileRows; }
-// TMEM columns: accumulators (mtiles x N) then two A buffers (hi + lo limbs).
+// TMEM columns: main accumulators Th*Xh (mtiles x N), correction
+// accumulators Th*Xl + Tl*Xh (mtiles x N), then two A buffers (hi + lo).
+// Keeping the small corrections out of the main accumulator stops every
+// FP32 accumulate from dropping their low-order bits.
+__host__ __device__ inline int tmem_need(int nk, int n) {
+  return 2 * mtiles_of(nk) * n + 4 * kACols;
+}
 __host__ __device__ inline int tmem_cols(int nk, int n) {
-  int need = mtiles_of(nk) * n + 4 * kACols;
+  int need = tmem_need(nk, n);
   int c = 32;
   while (c < need) c <<= 1;
   return c;
@@ -232,7 +241,7 @@ struct Layout {
 // The kernel.
 // ---------------------------------------------------------------------------
 template <int W, bool F16>
-__global__ void __launch_bounds__(kThreadsS, W <= 8 ? 2 : 1) split_rk4_kernel(Args a) {
+__global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   constexpr int N = 4 * W;
   constexpr int WH = W / 2;  // wires per epilogue warp
   extern __shared__ __align__(1024) uint8_t smem[];
@@ -245,7 +254,7 @@ __global__ void __launch_bounds__(kThreadsS, W <= 8 ? 2 : 1) split_rk4_kernel(Ar
   PsbTable tb{};
   if (ok) {
     tb = a.tables[grp.table];
-    ok = tb.nk >= 2 && tb.nk <= PSB_MAX_NK && mtiles_of(tb.nk) * N + 4 * kACols <= 512 &&
+    ok = tb.nk >= 2 && tb.nk <= PSB_MAX_NK && tmem_need(tb.nk, N) <= 512 &&
          tb.off >= 0 && tb.off + 9 * (int64_t)tb.nk <= a.n_tabdata &&
          (tb.flags & PSB_TAB_EXCITONS) && (tb.flags & PSB_TAB_SHARED_V) &&
          !(tb.flags & PSB_TAB_SCREENED);
@@ -393,7 +402,8 @@ __global__ void __launch_bounds__(kThreadsS, W <= 8 ? 2 : 1) split_rk4_kernel(Ar
 
   const uint32_t idesc = idesc_f16(N, F16);
   const int total_stages = a.nsteps * 4;
-  const uint32_t acol0 = (uint32_t)(nM * N);  // first A-buffer column
+  const uint32_t ccol0 = (uint32_t)(nM * N);      // first correction-accumulator column
+  const uint32_t acol0 = (uint32_t)(2 * nM * N);  // first A-buffer column
   const double h = a.dt;
   const double hbar = a.hbar;
 
@@ -405,6 +415,7 @@ __global__ void __launch_bounds__(kThreadsS, W <= 8 ? 2 : 1) split_rk4_kernel(Ar
         tc_fence_after();
         for (int mi = 0; mi < nM; ++mi) {
           const uint32_t dcol = tmem + (uint32_t)(mi * N);
+          const uint32_t ccol = tmem + ccol0 + (uint32_t)(mi * N);
           for (int kj = 0; kj < nK; ++kj, ++it) {
             const int b = it & 1;
             if (!mbar_wait(&afull[b], (it >> 1) & 1, abort)) break;
@@ -417,8 +428,8 @@ __global__ void __launch_bounds__(kThreadsS, W <= 8 ? 2 : 1) split_rk4_kernel(Ar
               const uint64_t dbh = smem_desc(smem_u32(xh) + (k0 >> 3) * 128, 128, xsbo);
               const uint64_t dbl = smem_desc(smem_u32(xl) + (k0 >> 3) * 128, 128, xsbo);
               umma_ts(dcol, ah + ks * 8, dbh, idesc, (kj | ks) != 0);
-              umma_ts(dcol, ah + ks * 8, dbl, idesc, 1);
-              umma_ts(dcol, al + ks * 8, dbh, idesc, 1);
+              umma_ts(ccol, ah + ks * 8, dbl, idesc, (kj | ks) != 0);
+              umma_ts(ccol, al + ks * 8, dbh, idesc, 1);
             }
             umma_commit(&afree[b]);  // buffer reusable once these MMAs finish
           }
@@ -488,27 +499,47 @@ __global__ void __launch_bounds__(kThreadsS, W <= 8 ? 2 : 1) split_rk4_kernel(Ar
         for (int j = 0; j < WH; ++j) pr[j] = pim[j] = 0.0;
         for (int mi = 0; mi < nM; ++mi) {
           const int k = mi * kTileRows + 32 * q + lane;
-          float d[4 * WH];
-#pragma unroll
-          for (int c = 0; c < 4 * WH; c += 8)
-            tmem_ld8(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(mi * N + 4 * WH * hh + c),
-                     d + c);
+          const uint32_t lrow = tmem + ((uint32_t)(32 * q) << 16);
+          const double ee = k < nk ? Ee[k] : 0.0, eh = k < nk ? Eh[k] : 0.0;
+          // wires in pairs: one 8-column TMEM load per accumulator, and the
+          // pair's element state loaded together for memory parallelism
+#pragma unroll 1
+          for (int jp = 0; jp < WH; jp += 2) {
+          uint32_t d1[8], d2[8];
+          tmem_ld8(lrow + (uint32_t)(mi * N + 4 * (w0 + jp)), d1);
+          tmem_ld8(lrow + ccol0 + (uint32_t)(mi * N + 4 * (w0 + jp)), d2);
+          tmem_ld_wait();
           if (k >= nk) continue;
-          const double ee = Ee[k], eh = Eh[k];
+          double4 ysv[2], yvv[2], accv[2];
 #pragma unroll
-          for (int j = 0; j < WH; ++j) {
+          for (int u = 0; u < 2; ++u) {
+            if (w0 + jp + u < grp.nw) {
+              const int64_t e = woff[w0 + jp + u] + k;
+              ysv[u] = a.ws_ys[e];
+              yvv[u] = reinterpret_cast<const double4*>(a.y)[e];
+              if (stg != 0) accv[u] = a.ws_acc[e];
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < 2; ++u) {
+            const int j = jp + u;
             const int w = w0 + j;
             if (w >= grp.nw) break;
             const int64_t e = woff[w] + k;
             const double4 par = wpar[w];
             const double2 M = Msh[w];
-            const double4 ys = a.ws_ys[e];
+            const double4 ys = ysv[u];
+            double ex[4];
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+              ex[c] = vscale * ((double)__uint_as_float(d1[4 * u + c]) +
+                                (double)__uint_as_float(d2[4 * u + c]));
             // exchange sums (SBEs.py:896-921) from the tensor cores, the
             // diagonal RHS (SBEs.py:1962-1975, 2325-2337, 2623-2636) in fp64
-            const double omr = M.x + vscale * (double)d[4 * j + 0];
-            const double omi = M.y + vscale * (double)d[4 * j + 1];
-            const double se = (ee + par.x) - vscale * (double)d[4 * j + 2];
-            const double sh = eh - vscale * (double)d[4 * j + 3];
+            const double omr = M.x + ex[0];
+            const double omi = M.y + ex[1];
+            const double se = (ee + par.x) - ex[2];
+            const double sh = eh - ex[3];
             const double sum = se + sh;
             const double nn = ys.z + ys.w - 1.0;
             const double xr = sum * ys.x - omr * nn;
@@ -517,12 +548,12 @@ __global__ void __launch_bounds__(kThreadsS, W <= 8 ? 2 : 1) split_rk4_kernel(Ar
             double f[4];
             f[0] = xi / hbar - hg * ys.x;
             f[1] = -xr / hbar - hg * ys.y;
-            const double u = omi * ys.x - omr * ys.y;
-            f[2] = 2.0 * u / hbar;
+            const double uu = omi * ys.x - omr * ys.y;
+            f[2] = 2.0 * uu / hbar;
             f[3] = f[2];
             // RK4 stage combination in fp64 (integrator.py:143-157):
             // acc = k1 + 2 k2 + 2 k3, y += h/6 (acc + k4)
-            const double4 yv = reinterpret_cast<const double4*>(a.y)[e];
+            const double4 yv = yvv[u];
             const double yy[4] = {yv.x, yv.y, yv.z, yv.w};
             double4 acc;
             double nxt[4];
@@ -531,7 +562,7 @@ __global__ void __launch_bounds__(kThreadsS, W <= 8 ? 2 : 1) split_rk4_kernel(Ar
 #pragma unroll
               for (int c = 0; c < 4; ++c) nxt[c] = yy[c] + (h / 2.0) * f[c];
             } else if (stg == 3) {
-              acc = a.ws_acc[e];
+              acc = accv[u];
               const double ac[4] = {acc.x, acc.y, acc.z, acc.w};
 #pragma unroll
               for (int c = 0; c < 4; ++c) nxt[c] = yy[c] + (h / 6.0) * (ac[c] + f[c]);
@@ -539,7 +570,7 @@ __global__ void __launch_bounds__(kThreadsS, W <= 8 ? 2 : 1) split_rk4_kernel(Ar
               pr[j] += nxt[0];
               pim[j] += nxt[1];
             } else {
-              acc = a.ws_acc[e];
+              acc = accv[u];
               acc.x += 2.0 * f[0];
               acc.y += 2.0 * f[1];
               acc.z += 2.0 * f[2];
@@ -552,6 +583,7 @@ __global__ void __launch_bounds__(kThreadsS, W <= 8 ? 2 : 1) split_rk4_kernel(Ar
             const float v[4] = {(float)nxt[0], (float)nxt[1], (float)nxt[2], (float)nxt[3]};
             a.ws_ys[e] = make_double4(nxt[0], nxt[1], nxt[2], nxt[3]);
             store_x(k, w, v);
+          }
           }
         }
         if (stg == 3) {
@@ -636,7 +668,7 @@ int launch(const Args& a, int nkmax, cudaStream_t s) {
     const uint32_t t = Layout<W>(nk).total;
     if (t > smem) smem = t;
   }
-  if (smem > kMaxDynSmem || tmem_cols(nkmax, 4 * W) > 512)
+  if (smem > kMaxDynSmem || tmem_need(nkmax, 4 * W) > 512)
     return set_error(PSB_ERR_SIZE, "split form: nk %d does not fit a group of %d wires", nkmax,
                      W);
   cudaError_t e = cudaFuncSetAttribute(split_rk4_kernel<W, F16>,
@@ -673,7 +705,7 @@ extern "C" int psb_split_max_nk(int wgroup) {
     const uint32_t sm = wgroup == 16 ? split::Layout<16>(nk).total
                                      : (wgroup == 8 ? split::Layout<8>(nk).total
                                                     : split::Layout<4>(nk).total);
-    if (sm <= split::kMaxDynSmem && split::tmem_cols(nk, 4 * wgroup) <= 512) best = nk;
+    if (sm <= split::kMaxDynSmem && split::tmem_need(nk, 4 * wgroup) <= 512) best = nk;
   }
   return best;
 }
