@@ -44,7 +44,7 @@ def parse():
     ap.add_argument("--chunk", type=int, default=100, help="time steps per bench step")
     ap.add_argument("--form", default="plain", choices=["plain", "split"],
                     help="plain FP64 kernel or split hi+lo tensor-core kernel")
-    ap.add_argument("--limb", default="bf16", choices=["bf16", "fp16"],
+    ap.add_argument("--limb", default="fp16", choices=["bf16", "fp16"],
                     help="16-bit limb format of the split form")
     ap.add_argument("--nwires", type=int, default=0, help="override the workload's wire count")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)

@@ -229,9 +229,13 @@ int psb_f64_smem_bytes(int nk, int tab_flags);
  * grid, the exchange sums of all wires are one contraction
  *   D[k][(w,v)] = sum_k' T[k][k'] X[k'][(w,v)],  T[k][k'] = V(|k-k'|)/vscale,
  * computed on the tensor cores as hi+lo split products of 16-bit limbs
- * (Th Xh + Th Xl + Tl Xh; bf16 or fp16 limbs) accumulated in FP32, with
- * vscale the power of two at or above max V.  The O(Nk) right-hand side, the RK4 stage combination, the state and
- * the P(t) sums stay FP64 (FP64 layout of the plain form).
+ * (Th Xh + Th Xl + Tl Xh; bf16 or fp16 limbs), with vscale the power of two
+ * at or above max V.  Every 64-wide slice of k' is accumulated in a fresh
+ * tensor-memory block and drained at once, so the tensor cores' FP32
+ * accumulation never runs over more than four K = 16 steps.  The O(Nk)
+ * right-hand side and the stage point / RK accumulator are FP32, the state
+ * y and the P(t) sums FP64 (FP64 layout of the plain form).  Target
+ * accuracy: normwise relative error <= 1e-6 in P(t) against the FP64 form.
  * Requires PSB_TAB_EXCITONS | PSB_TAB_SHARED_V tables without screening.
  */
 #define PSB_SPLIT_WMAX 16
@@ -239,7 +243,8 @@ int psb_f64_smem_bytes(int nk, int tab_flags);
  * fp16 (hi+lo ~ 22 significant bits; same tensor-core rate). */
 #define PSB_LIMB_BF16 0
 #define PSB_LIMB_FP16 1
-/* One CTA's work: 1..wgroup wires of one table (same k grid). */
+/* One CTA's work: 1..wgroup wires of one table (same k grid); wire slots
+ * past nw are ignored. */
 typedef struct PsbSplitGroup {
   int32_t table;
   int32_t nw;
@@ -248,17 +253,22 @@ typedef struct PsbSplitGroup {
 
 /* Workspace bytes psb_rk4_split needs for n_state elements. */
 int64_t psb_split_ws_bytes(int64_t n_state);
-/* Dynamic shared memory (bytes) of one CTA for a grid of nk, wgroup 4/8/16. */
+/* Dynamic shared memory (bytes) of one CTA for a grid of nk, wgroup 4 or 8
+ * (the layout psb_rk4_split picks for nkmax = nk). */
 int psb_split_smem_bytes(int nk, int wgroup);
-/* Largest nk a group of wgroup wires supports (shared and tensor memory). */
+/* Largest nk a group of wgroup (4 or 8) wires supports. */
 int psb_split_max_nk(int wgroup);
+/* Largest nk for which the stage state of a group stays resident in shared
+ * memory for the whole call (faster; larger grids keep it in the workspace). */
+int psb_split_max_nk_resident(int wgroup);
 /*
  * nsteps RK4 steps of every group (one CTA each), same contract as
  * psb_rk4_f64 (state, t, steps, status, P(t) records) for the wires of
- * d_groups[0..ngroups).  wgroup (4, 8 or 16) is the group capacity compiled
+ * d_groups[0..ngroups).  wgroup (4 or 8) is the group capacity compiled
  * for; nkmax the largest grid among the groups (<= psb_split_max_nk(wgroup)).
  * d_ws: caller-allocated workspace of psb_split_ws_bytes(n_state) bytes,
- * 32-byte aligned (stage state and RK accumulator per element).  Replaces,
+ * 32-byte aligned (stage state and RK accumulator per element).  On
+ * PSB_ERR_TIMEOUT the state of the group's wires is unspecified.  Replaces,
  * like psb_rk4_f64, CalcH + dpdt/dCdt/dDdt (SBEs.py:669-935, 1850-2636)
  * integrated by rk4_dpc (libpulsesuite/integrator.py:143-167).
  */

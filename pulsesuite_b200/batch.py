@@ -24,7 +24,7 @@ class WireBatch:
     right-hand side and FP64 stage combination, psb_rk4_split)."""
 
     def __init__(self, grids, wires, screened=False, excitons=True, p_cap=0, tables=None,
-                 tabdata=None, form="plain", limb="bf16"):
+                 tabdata=None, form="plain", limb="fp16"):
         device.require_cuda()
         if form not in ("plain", "split"):
             raise ValueError("form must be 'plain' or 'split'")
@@ -87,33 +87,35 @@ class WireBatch:
     def _setup_split(self):
         """Wire groups (one CTA each) and the workspace of the split form.
 
-        A group holds up to W in {4, 8, 16} wires of one grid.  The exchange
-        work of a group per step is ~W Nk^2, so W is chosen per grid to give
-        roughly two waves of equal CTAs over the SMs (small W for large
-        grids, W = 16 once a grid has enough wires), which balances uneven
-        batches; the three W classes run concurrently on side streams."""
+        A group holds up to W in {4, 8} wires of one grid.  The exchange work
+        of a group per step is ~W Nk^2, so W is chosen per grid to give
+        roughly two waves of equal CTAs over the SMs (W = 4 for large grids,
+        W = 8 once a grid has enough wires).  Groups are launched in classes
+        of (W, state resident in shared memory or not) so that a large grid
+        does not push the small ones out of the resident layout; the classes
+        run concurrently on side streams."""
         need = abi.PSB_TAB_EXCITONS | abi.PSB_TAB_SHARED_V
         f = self.h_tables["flags"]
         if ((f & need) != need).any() or (f & abi.PSB_TAB_SCREENED).any():
             raise _lib.PsbError("split form needs unscreened tables with Veh == Vee == Vhh")
         lib = _lib.load()
-        maxnk = {wg: int(lib.psb_split_max_nk(wg)) for wg in (4, 8, 16)}
+        maxnk = {wg: int(lib.psb_split_max_nk(wg)) for wg in (4, 8)}
+        resnk = {wg: int(lib.psb_split_max_nk_resident(wg)) for wg in (4, 8)}
         nks = self.h_tables["nk"].astype(np.int64)
         counts = np.bincount(self.h_wires["table"], minlength=len(nks))
         sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
         target = float(np.sum(counts * nks.astype(np.float64) ** 2)) / (2.0 * sms)
-        classes = {4: [], 8: [], 16: []}
+        classes = {}
         for t in np.argsort(-nks, kind="stable"):
             nk = int(nks[t])
             if counts[t] == 0:
                 continue
             wg = 4
-            for cand in (16, 8):
-                if nk <= maxnk[cand] and cand * nk * nk <= max(target, 4 * nk * nk):
-                    wg = cand
-                    break
+            if nk <= resnk[8] and 8 * nk * nk <= max(target, 4 * nk * nk):
+                wg = 8
             if nk > maxnk[wg]:
                 raise _lib.PsbError(f"split form: nk {nk} exceeds the supported maximum")
+            key = (wg, nk <= resnk[wg])
             ws = np.nonzero(self.h_wires["table"] == t)[0]
             for i in range(0, len(ws), wg):
                 g = np.zeros(1, dtype=abi.SPLIT_GROUP_DTYPE)
@@ -121,13 +123,12 @@ class WireBatch:
                 g["nw"] = len(ws[i:i + wg])
                 g["wire"][0, :] = -1
                 g["wire"][0, :g["nw"][0]] = ws[i:i + wg]
-                classes[wg].append(g)
+                classes.setdefault(key, []).append(g)
         self.split_launches = []
-        for wg in (16, 8, 4):
-            if classes[wg]:
-                ga = np.concatenate(classes[wg])
-                nkmax = int(nks[ga["table"]].max())
-                self.split_launches.append((wg, device.to_device(ga), len(ga), nkmax))
+        for key in sorted(classes, key=lambda kk: (-kk[0], not kk[1])):
+            ga = np.concatenate(classes[key])
+            nkmax = int(nks[ga["table"]].max())
+            self.split_launches.append((key[0], device.to_device(ga), len(ga), nkmax))
         self.side_streams = [torch.cuda.Stream() for _ in self.split_launches[1:]]
         self.ws = torch.zeros(int(lib.psb_split_ws_bytes(self.n_state)), dtype=torch.uint8,
                               device="cuda")

@@ -4,27 +4,50 @@
 // The exchange sums of every right-hand side (pulsesuite/PSTD3D/SBEs.py:
 // 896-921) are, for W wires sharing one k grid, one dense contraction
 //     D[k][(w,v)] = sum_k' T[k][k'] X[k'][(w,v)],   T[k][k'] = V(|k-k'|)/vscale
-// with X the stage state (v: p_re, p_im, ne, nh).  T and X are split into
-// bf16 hi + lo parts and D = Th Xh + (Th Xl + Tl Xh) is accumulated in FP32
-// in tensor memory, the main product and the two corrections in separate
-// accumulators that the epilogue adds in FP64 (Tl Xl is below the FP32
-// resolution of the sum).
+// with X the stage point (v: p_re, p_im, ne, nh).  T and X are split into
+// 16-bit hi + lo limbs and D = Th Xh + (Th Xl + Tl Xh) is formed on the
+// tensor cores (Tl Xl is below the resolution of the sum).
 //
-// One CTA owns a group of W (4, 8 or 16) wires for all `nsteps` RK4 steps:
-//   * X (bf16 hi and lo, the MMA B operand, N = 4W columns, wire-major) lives
-//     in shared memory for the whole call;
-//   * T is Toeplitz, so it is never stored as a matrix: each 128 x 64 tile
-//     of the MMA A operand is generated straight into tensor memory from a
-//     table of bf16 pairs (Tv(d), Tv(d-1)) in shared memory -- one 32-bit
-//     lookup per TMEM cell -- double buffered, and the MMA reads A from TMEM;
-//   * one thread issues tcgen05.mma (M = 128, N = 4W, K = 16) into one TMEM
-//     accumulator block per 128-row tile of k;
-//   * eight warps generate the T tiles during the MMA phase and, once the
-//     accumulators are complete, evaluate the diagonal SBE right-hand side,
-//     combine the RK4 stages (stage order of libpulsesuite/integrator.py:
-//     143-157) and write the next stage's X back into shared memory.
-// The right-hand side and the stage state are FP64 (O(Nk) work per wire);
-// only the O(Nk^2) exchange contraction runs in split bf16.
+// Accuracy.  The tensor cores' FP32 accumulation aligns every product of a
+// K = 16 step to the largest term, accumulator included, and drops the bits
+// below: the error of one step grows with the accumulator, and it is biased.
+// Accumulated over all of k' (K up to 1024) that bias reached ~3e-6 in P(t).
+// So every 64-wide slice of k' goes into a fresh tensor-memory block (main
+// product and corrections apart, each at most four K = 16 steps deep) and is
+// drained at once; the slices are summed with round-to-nearest on the CUDA
+// cores.  What remains is the representation of T and X: T enters every
+// step unchanged, so its rounding acts as a small static change of the
+// Coulomb matrix and shifts the phase of p linearly in time.  bf16 limbs
+// (hi + lo: 16 bits) leave ~1e-6 in P(t) on small grids; fp16 limbs (22
+// bits, the default) reach ~1e-7 once T is scaled by 2^14 and every X column
+// by the power of two that puts its largest value in [2^14, 2^15), so that
+// no lo limb falls into the fp16 subnormals.  The right-hand side is FP64
+// (the band energies set the phase of p and must not be rounded), the stage
+// point and the RK accumulator FP32 and the state y FP64.
+//
+// One CTA owns a group of W (4 or 8) wires for all `nsteps` RK4 steps,
+// 128-row tiles of k at a time:
+//   * X (the MMA B operand, N = 4W columns, wire-major) lives in shared
+//     memory, double buffered: stage s reads X[s & 1], its epilogue writes
+//     X[(s + 1) & 1], so the epilogue of a k tile overlaps the MMAs of the
+//     next tile;
+//   * T is Toeplitz and never stored as a matrix: each 128 x 64 tile of the
+//     A operand is generated straight into tensor memory by four generator
+//     warps from a table of limb pairs (Tv(d), Tv(d-1)) in shared memory --
+//     one 32-bit lookup per TMEM cell.  A tile depends only on 2 mi - kj
+//     (mi the row tile, kj the k' slice); when all distinct tiles fit in
+//     tensor memory (nk <= 256) they are generated once per call, else they
+//     stream through a double buffer;
+//   * one thread issues tcgen05.mma (M = 128, N = 4W, K = 16), three
+//     products per K step, into a double-buffered pair of slice blocks;
+//   * eight drain/epilogue warps sum the slices of a row tile and then
+//     evaluate the diagonal SBE right-hand side and the RK4 stage
+//     combination (stage order of libpulsesuite/integrator.py:143-157);
+//     at the end of a stage they write the next X from the stage points
+//     with the column scales of that stage;
+//   * the per-element state (y FP64, stage point and accumulator FP32) stays
+//     in shared memory for the whole call when it fits (psb_split_max_nk_
+//     resident), else in the caller's workspace.
 // Every mbarrier wait is bounded; on a timeout the CTA records
 // PSB_ERR_TIMEOUT in its wires' status, waits for its MMAs, frees TMEM and
 // returns.
@@ -37,15 +60,18 @@
 namespace psb {
 namespace split {
 
-constexpr int kEpiWarps = 8;
-constexpr int kMmaWarp = 8;
-constexpr int kThreadsS = 32 * 9;
+constexpr int kEpiWarps = 8;    // warps 0..7: drain + epilogue
+constexpr int kGenWarp0 = 8;    // warps 8..11: A-tile generators
+constexpr int kGenWarps = 4;
+constexpr int kMmaWarp = 12;    // warp 12: TMEM owner + MMA issuer
+constexpr int kThreadsS = 32 * 13;
 constexpr int kTileRows = 128;  // M of one MMA
-constexpr int kTileK = 64;      // k' per generated A tile
-constexpr int kACols = kTileK / 2;  // TMEM columns of one bf16 limb of an A tile
+constexpr int kTileK = 64;      // k' per A tile and per drained slice
+constexpr int kACols = kTileK / 2;  // TMEM columns of one 16-bit limb of an A tile
+constexpr int kTmemCols = 512;
 constexpr uint32_t kSpinLimit = 1u << 26;
-// dynamic shared memory per CTA (the 227 KiB limit less the static reduction
-// buffer and its alignment padding)
+// dynamic shared memory per CTA (the 227 KiB limit less the static
+// shared memory and alignment padding)
 constexpr uint32_t kMaxDynSmem = 226 * 1024;
 
 // ---------------------------------------------------------------------------
@@ -179,15 +205,19 @@ __device__ __forceinline__ uint32_t x_off(int k, int col, uint32_t sbo) {
 
 __host__ __device__ inline int kpad_of(int nk) { return (nk + kTileK - 1) / kTileK * kTileK; }
 __host__ __device__ inline int mtiles_of(int nk) { return (nk + kTileRows - 1) / kTileRows; }
-// TMEM columns: main accumulators Th*Xh (mtiles x N), correction
-// accumulators Th*Xl + Tl*Xh (mtiles x N), then two A buffers (hi + lo).
-// Keeping the small corrections out of the main accumulator stops every
-// FP32 accumulate from dropping their low-order bits.
-__host__ __device__ inline int tmem_need(int nk, int n) {
-  return 2 * mtiles_of(nk) * n + 4 * kACols;
+// Distinct A tiles of a grid: one per value of 2 mi - kj.
+__host__ __device__ inline int ntiles_of(int nk) {
+  return kpad_of(nk) / kTileK + 2 * (mtiles_of(nk) - 1);
+}
+// TMEM columns: two slice blocks of main product + corrections (4 N), then
+// the A slots (hi + lo limbs, 2 kACols each): all distinct tiles when they
+// fit (persistent), else a double buffer.
+__host__ __device__ inline bool persistent_tiles(int nk, int n) {
+  return 4 * n + 2 * kACols * ntiles_of(nk) <= kTmemCols;
 }
 __host__ __device__ inline int tmem_cols(int nk, int n) {
-  int need = tmem_need(nk, n);
+  const int slots = persistent_tiles(nk, n) ? ntiles_of(nk) : 2;
+  const int need = 4 * n + 2 * kACols * slots;
   int c = 32;
   while (c < need) c <<= 1;
   return c;
@@ -204,8 +234,8 @@ struct Args {
   int ngroups;
   double* y;
   int64_t n_state;
-  double4* ws_ys;
-  double4* ws_acc;
+  float4* ws_ys;   // stage point per element (workspace layout)
+  float4* ws_acc;  // RK accumulator per element (workspace layout)
   int nsteps;
   double dt;
   double* P;
@@ -213,37 +243,40 @@ struct Args {
   int p_stride;
   int p_cap;
   double hbar;
+  uint32_t smem_bytes;  // dynamic shared memory of the launch
 };
 
-template <int W>
+// Shared-memory layout of one CTA.  RES: the element state (y double4,
+// stage point float4, accumulator float4 per (wire, k)) is resident here.
+template <int W, bool RES>
 struct Layout {
   static constexpr int N = 4 * W;
-  uint32_t x_hi, x_lo, tab, bars, misc, total;
+  uint32_t xbuf, st, tab, bars, misc, total;
   int ntab_words;
   __host__ __device__ Layout(int nk) {
     const int kpad = kpad_of(nk), nM = mtiles_of(nk);
-    const uint32_t xb = (uint32_t)kpad * N * 2;
-    x_hi = 0;
-    x_lo = x_hi + xb;
-    tab = x_lo + xb;
+    xbuf = 2u * (uint32_t)kpad * N * 2;  // one stage buffer: hi + lo limbs
+    st = 2 * xbuf;
+    tab = st + (RES ? 64u * W * (uint32_t)kpad : 0u);
     ntab_words = kTileRows * nM + kpad;
     bars = tab + 2 * 4 * (uint32_t)ntab_words;  // hi and lo pair tables
     bars = (bars + 15) & ~15u;
-    misc = bars + 8 * 8;  // afull[2], afree[2], dready, final
+    misc = bars + 8 * 12;  // afull[2], afree[2], dfull[2], dfree[2], final
     // misc: tmem base (16 B), abort + snapshots (16 B), M re/im double2[W],
     // wire params (gap, gamma, mscale, pscale: double4[W]), t double[W],
-    // off int64[W], P partials double[2][4][W]
-    total = misc + 32 + 128 * W;
+    // off int64[W], P partials double[2][4][W], X column decode factors
+    // double[2][N], column maxima float[4][N]
+    total = misc + 32 + 256 * W;
   }
 };
 
 // ---------------------------------------------------------------------------
 // The kernel.
 // ---------------------------------------------------------------------------
-template <int W, bool F16>
+template <int W, bool F16, bool RES>
 __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   constexpr int N = 4 * W;
-  constexpr int WH = W / 2;  // wires per epilogue warp
+  constexpr int WH = W / 2;  // wires per drain/epilogue warp
   extern __shared__ __align__(1024) uint8_t smem[];
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
@@ -254,10 +287,10 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   PsbTable tb{};
   if (ok) {
     tb = a.tables[grp.table];
-    ok = tb.nk >= 2 && tb.nk <= PSB_MAX_NK && tmem_need(tb.nk, N) <= 512 &&
-         tb.off >= 0 && tb.off + 9 * (int64_t)tb.nk <= a.n_tabdata &&
-         (tb.flags & PSB_TAB_EXCITONS) && (tb.flags & PSB_TAB_SHARED_V) &&
-         !(tb.flags & PSB_TAB_SCREENED);
+    ok = tb.nk >= 2 && tb.nk <= PSB_MAX_NK && tb.off >= 0 &&
+         tb.off + 9 * (int64_t)tb.nk <= a.n_tabdata && (tb.flags & PSB_TAB_EXCITONS) &&
+         (tb.flags & PSB_TAB_SHARED_V) && !(tb.flags & PSB_TAB_SCREENED) &&
+         Layout<W, RES>(tb.nk).total <= a.smem_bytes;
     for (int i = 0; ok && i < grp.nw; ++i) {
       const int wi = grp.wire[i];
       ok = wi >= 0 && wi < a.nw && a.wires[wi].table == grp.table && a.wires[wi].off >= 0 &&
@@ -270,15 +303,20 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
     return;
   }
   const int nk = tb.nk, kpad = kpad_of(nk), nM = mtiles_of(nk), nK = kpad / kTileK;
-  const Layout<W> L(nk);
-  uint8_t* xh = smem + L.x_hi;
-  uint8_t* xl = smem + L.x_lo;
+  const Layout<W, RES> L(nk);
+  const bool persist = persistent_tiles(nk, N);
+  const int ntile = ntiles_of(nk);
+  uint8_t* xbase = smem;  // X[b]: hi at xbase + b xbuf, lo at + xbuf/2
+  double4* s_y = reinterpret_cast<double4*>(smem + L.st);
+  float4* s_ys = reinterpret_cast<float4*>(smem + L.st + 32u * W * kpad);
+  float4* s_acc = reinterpret_cast<float4*>(smem + L.st + 48u * W * kpad);
   uint32_t* tab_hi = reinterpret_cast<uint32_t*>(smem + L.tab);
   uint32_t* tab_lo = tab_hi + L.ntab_words;
   uint64_t* afull = reinterpret_cast<uint64_t*>(smem + L.bars);
   uint64_t* afree = afull + 2;
-  uint64_t* dready = afree + 2;
-  uint64_t* final_bar = dready + 1;  // teardown: all MMAs of this CTA done
+  uint64_t* dfull = afree + 2;
+  uint64_t* dfree = dfull + 2;
+  uint64_t* final_bar = dfree + 2;  // teardown: all MMAs of this CTA done
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + L.misc);
   volatile int* abort = reinterpret_cast<volatile int*>(smem + L.misc + 16);
   // abort as seen at each stage's end barrier (written by one participant
@@ -289,7 +327,10 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   double* wt = reinterpret_cast<double*>(smem + L.misc + 32 + 48 * W);
   int64_t* woff = reinterpret_cast<int64_t*>(smem + L.misc + 32 + 56 * W);
   double* ppart = reinterpret_cast<double*>(smem + L.misc + 32 + 64 * W);
+  double* xfac = reinterpret_cast<double*>(smem + L.misc + 32 + 128 * W);
+  float* colmax = reinterpret_cast<float*>(smem + L.misc + 32 + 192 * W);
   const uint32_t xsbo = (uint32_t)(kpad / 8) * 128;
+  const uint32_t xlimb = L.xbuf / 2;
   const double* blk = a.tabdata + tb.off;
   const double* Ee = blk + 3 * nk;
   const double* Eh = blk + 4 * nk;
@@ -302,14 +343,15 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) vm = fmax(vm, __shfl_xor_sync(0xffffffffu, vm, o));
   if (lane == 0) vmax_w[warp] = vm;
-  for (uint32_t i = tid * 16; i < 2 * (uint32_t)kpad * N * 2; i += kThreadsS * 16)
-    *reinterpret_cast<uint4*>(smem + i) = make_uint4(0, 0, 0, 0);
+  for (uint32_t i = tid * 16; i < 2 * L.xbuf; i += kThreadsS * 16)
+    *reinterpret_cast<uint4*>(xbase + i) = make_uint4(0, 0, 0, 0);
   if (tid == 0) {
-    mbar_init(&afull[0], kEpiWarps);
-    mbar_init(&afull[1], kEpiWarps);
-    mbar_init(&afree[0], 1);
-    mbar_init(&afree[1], 1);
-    mbar_init(dready, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&afull[b], kGenWarps);
+      mbar_init(&afree[b], 1);
+      mbar_init(&dfull[b], 1);
+      mbar_init(&dfree[b], kEpiWarps);
+    }
     mbar_init(final_bar, 1);
     *abort = 0;
     snap[0] = 0;
@@ -339,112 +381,233 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
+  // TMEM column map: slice blocks Dm[b] at 2N b, Dc[b] at 2N b + N; A slot i
+  // at acol0 + 2 kACols i (hi limb, then lo limb).
+  const uint32_t acol0 = (uint32_t)(4 * N);
   double vmax = 0.0;
 #pragma unroll
   for (int i = 0; i < kThreadsS / 32; ++i) vmax = fmax(vmax, vmax_w[i]);
   int ex = 0;
   frexp(vmax > 0.0 ? vmax : 1.0, &ex);
-  const double vscale = ldexp(1.0, ex);
-  const double inv_vscale = ldexp(1.0, -ex);
+  // fp16 limbs: T scaled by 2^14 so that its lo limbs stay normal numbers
+  const int tsh = F16 ? 14 : 0;
+  const double vscale = ldexp(1.0, ex - tsh);  // V = vscale * T
+  const double inv_vscale = ldexp(1.0, tsh - ex);
   // Pair tables: word(d) = (Tv(d), Tv(d-1)) for d in [2 - kpad, 128 nM - 1],
-  // Tv(d) = bf16 limb of V(|d|)/vscale (0 at d = 0 and outside the grid).
+  // Tv(d) = limb of V(|d|)/vscale (0 at d = 0 and outside the grid).
   const int dlo = 2 - kpad;
-  auto tv = [&](int d, uint16_t& hi, uint16_t& lo) {
-    const int ad = d < 0 ? -d : d;
-    const float v = (ad > 0 && ad < nk) ? (float)(blk[ad] * inv_vscale) : 0.f;
-    split2<F16>(v, hi, lo);
-  };
   for (int i = tid; i < L.ntab_words; i += kThreadsS) {
     const int d = dlo + i;
-    uint16_t h0, l0, h1, l1;
-    tv(d, h0, l0);
-    tv(d - 1, h1, l1);
-    tab_hi[i] = (uint32_t)h0 | ((uint32_t)h1 << 16);
-    tab_lo[i] = (uint32_t)l0 | ((uint32_t)l1 << 16);
+    uint16_t h[2], l[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int dd = d - u;
+      const int ad = dd < 0 ? -dd : dd;
+      const float v = (ad > 0 && ad < nk) ? (float)(blk[ad] * inv_vscale) : 0.f;
+      split2<F16>(v, h[u], l[u]);
+    }
+    tab_hi[i] = (uint32_t)h[0] | ((uint32_t)h[1] << 16);
+    tab_lo[i] = (uint32_t)l[0] | ((uint32_t)l[1] << 16);
   }
 
-  // ---- epilogue-role helpers --------------------------------------------------
-  const int q = warp & 3;          // TMEM lane quarter
-  const int hh = (warp >> 2) & 1;  // wire half / A column half
-  const int w0 = hh * WH;          // first wire of this warp
-  auto store_x = [&](int k, int w, const float v[4]) {
-    uint16_t hi[4], lo[4];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) split2<F16>(v[c], hi[c], lo[c]);
-    const uint32_t o = x_off(k, 4 * w, xsbo);
-    uint2 ph, pl;
-    ph.x = (uint32_t)hi[0] | ((uint32_t)hi[1] << 16);
-    ph.y = (uint32_t)hi[2] | ((uint32_t)hi[3] << 16);
-    pl.x = (uint32_t)lo[0] | ((uint32_t)lo[1] << 16);
-    pl.y = (uint32_t)lo[2] | ((uint32_t)lo[3] << 16);
-    *reinterpret_cast<uint2*>(xh + o) = ph;
-    *reinterpret_cast<uint2*>(xl + o) = pl;
+  // ---- element ownership of the drain/epilogue warps -----------------------------
+  // warp (q, hh): rows 128 mi + 32 q + lane (q = TMEM lane quarter), wires
+  // w0 .. w0 + WH - 1.
+  const int q = warp & 3;
+  const int hh = (warp >> 2) & 1;
+  const int w0 = hh * WH;
+  double4* g_y = reinterpret_cast<double4*>(a.y);
+  auto ys_ptr = [&](int w, int k) -> float4* {
+    return RES ? s_ys + (w * kpad + k) : a.ws_ys + (woff[w] + k);
   };
-
-  // Stage-0 input: X = split(y), ys = y, for this thread's elements.
-  if (warp < kEpiWarps) {
+  // Largest |value| of each of this warp's X columns (fp16 limbs only),
+  // published per lane quarter q.
+  auto publish_colmax = [&](float* cm) {
+#pragma unroll
+    for (int c = 0; c < 4 * WH; ++c) {
+      float m = cm[c];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+      if (lane == 0) colmax[q * N + 4 * w0 + c] = m;
+    }
+  };
+  // X[b] = split(stage point * column scale) for this thread's elements.
+  // fp16: the column scale is the power of two that puts the column's
+  // largest value in [2^14, 2^15) (lo limbs stay normal, nothing
+  // overflows); xfac[b] = vscale / scale decodes the exchange sums.
+  auto x_pass = [&](int b) {
+    float sc[4 * WH];
+#pragma unroll
+    for (int c = 0; c < 4 * WH; ++c) {
+      int sexp = 0;
+      if (F16) {
+        const int col = 4 * w0 + c;
+        const float m = fmaxf(fmaxf(colmax[col], colmax[N + col]),
+                              fmaxf(colmax[2 * N + col], colmax[3 * N + col]));
+        if (m > 0.f && isfinite(m)) {
+          int e2;
+          frexpf(m, &e2);  // m < 2^e2
+          sexp = min(max(15 - e2, -100), 100);
+        }
+      }
+      sc[c] = ldexpf(1.f, sexp);
+      if (q == 0 && lane == c) xfac[b * N + 4 * w0 + c] = ldexp(vscale, -sexp);
+    }
+    uint8_t* xh = xbase + b * L.xbuf;
     for (int mi = 0; mi < nM; ++mi) {
       const int k = mi * kTileRows + 32 * q + lane;
       if (k >= nk) continue;
+#pragma unroll
       for (int j = 0; j < WH; ++j) {
         const int w = w0 + j;
         if (w >= grp.nw) break;
-        const int64_t e = woff[w] + k;
-        const double4 yv = reinterpret_cast<const double4*>(a.y)[e];
-        const float v[4] = {(float)yv.x, (float)yv.y, (float)yv.z, (float)yv.w};
-        a.ws_ys[e] = yv;
-        store_x(k, w, v);
+        const float4 v = *ys_ptr(w, k);
+        uint16_t hi[4], lo[4];
+        split2<F16>(v.x * sc[4 * j + 0], hi[0], lo[0]);
+        split2<F16>(v.y * sc[4 * j + 1], hi[1], lo[1]);
+        split2<F16>(v.z * sc[4 * j + 2], hi[2], lo[2]);
+        split2<F16>(v.w * sc[4 * j + 3], hi[3], lo[3]);
+        const uint32_t o = x_off(k, 4 * w, xsbo);
+        uint2 ph, pl;
+        ph.x = (uint32_t)hi[0] | ((uint32_t)hi[1] << 16);
+        ph.y = (uint32_t)hi[2] | ((uint32_t)hi[3] << 16);
+        pl.x = (uint32_t)lo[0] | ((uint32_t)lo[1] << 16);
+        pl.y = (uint32_t)lo[2] | ((uint32_t)lo[3] << 16);
+        *reinterpret_cast<uint2*>(xh + o) = ph;
+        *reinterpret_cast<uint2*>(xh + xlimb + o) = pl;
       }
     }
     fence_async_smem();
+  };
+  auto track = [&](float* cm, int j, float4 v) {
+    if (F16) {
+      cm[4 * j + 0] = fmaxf(cm[4 * j + 0], fabsf(v.x));
+      cm[4 * j + 1] = fmaxf(cm[4 * j + 1], fabsf(v.y));
+      cm[4 * j + 2] = fmaxf(cm[4 * j + 2], fabsf(v.z));
+      cm[4 * j + 3] = fmaxf(cm[4 * j + 3], fabsf(v.w));
+    }
+  };
+
+  // Stage-0 input: X[0] = split(y), stage point = y.
+  if (warp < kEpiWarps) {
+    float cm0[4 * WH];
+#pragma unroll
+    for (int c = 0; c < 4 * WH; ++c) cm0[c] = 0.f;
+    for (int mi = 0; mi < nM; ++mi) {
+      const int k = mi * kTileRows + 32 * q + lane;
+      if (k >= nk) continue;
+#pragma unroll
+      for (int j = 0; j < WH; ++j) {
+        const int w = w0 + j;
+        if (w >= grp.nw) break;
+        const double4 yv = g_y[woff[w] + k];
+        const float4 yf = make_float4((float)yv.x, (float)yv.y, (float)yv.z, (float)yv.w);
+        if (RES) s_y[w * kpad + k] = yv;
+        *ys_ptr(w, k) = yf;
+        track(cm0, j, yf);
+      }
+    }
+    publish_colmax(cm0);
+    named_sync(2, 32 * kEpiWarps);
+    x_pass(0);
   }
   __syncthreads();
 
   const uint32_t idesc = idesc_f16(N, F16);
   const int total_stages = a.nsteps * 4;
-  const uint32_t ccol0 = (uint32_t)(nM * N);      // first correction-accumulator column
-  const uint32_t acol0 = (uint32_t)(2 * nM * N);  // first A-buffer column
   const double h = a.dt;
-  const double hbar = a.hbar;
+  const double inv_hbar = 1.0 / a.hbar;
 
   if (warp == kMmaWarp) {
     // ---- MMA issuer -----------------------------------------------------------
     uint32_t it = 0;
     for (int s = 0; s < total_stages; ++s) {
       if (lane == 0 && !*abort) {
+        if (s == 0 && persist) mbar_wait(&afull[0], 0, abort);
         tc_fence_after();
-        for (int mi = 0; mi < nM; ++mi) {
-          const uint32_t dcol = tmem + (uint32_t)(mi * N);
-          const uint32_t ccol = tmem + ccol0 + (uint32_t)(mi * N);
+        const uint32_t xh = smem_u32(xbase + (s & 1) * L.xbuf);
+        const uint32_t xl = xh + xlimb;
+        for (int mi = 0; mi < nM && !*abort; ++mi) {
           for (int kj = 0; kj < nK; ++kj, ++it) {
             const int b = it & 1;
-            if (!mbar_wait(&afull[b], (it >> 1) & 1, abort)) break;
+            if (!persist && !mbar_wait(&afull[b], (it >> 1) & 1, abort)) break;
+            if (it >= 2 && !mbar_wait(&dfree[b], ((it >> 1) - 1) & 1, abort)) break;
             tc_fence_after();
-            const uint32_t ah = tmem + acol0 + (uint32_t)(b * 2 * kACols);
+            const int slot = persist ? 2 * mi - kj + nK - 1 : b;
+            const uint32_t ah = tmem + acol0 + (uint32_t)(slot * 2 * kACols);
             const uint32_t al = ah + kACols;
+            const uint32_t dm = tmem + (uint32_t)(2 * N * b);
+            const uint32_t dc = dm + (uint32_t)N;
 #pragma unroll
             for (int ks = 0; ks < kTileK / 16; ++ks) {
               const int k0 = kj * kTileK + ks * 16;
-              const uint64_t dbh = smem_desc(smem_u32(xh) + (k0 >> 3) * 128, 128, xsbo);
-              const uint64_t dbl = smem_desc(smem_u32(xl) + (k0 >> 3) * 128, 128, xsbo);
-              umma_ts(dcol, ah + ks * 8, dbh, idesc, (kj | ks) != 0);
-              umma_ts(ccol, ah + ks * 8, dbl, idesc, (kj | ks) != 0);
-              umma_ts(ccol, al + ks * 8, dbh, idesc, 1);
+              const uint64_t dbh = smem_desc(xh + (k0 >> 3) * 128, 128, xsbo);
+              const uint64_t dbl = smem_desc(xl + (k0 >> 3) * 128, 128, xsbo);
+              umma_ts(dm, ah + ks * 8, dbh, idesc, ks != 0);
+              umma_ts(dc, ah + ks * 8, dbl, idesc, ks != 0);
+              umma_ts(dc, al + ks * 8, dbh, idesc, 1);
             }
-            umma_commit(&afree[b]);  // buffer reusable once these MMAs finish
+            if (!persist) umma_commit(&afree[b]);  // A slot reusable once these finish
+            umma_commit(&dfull[b]);                // the slice is ready to drain
           }
-          if (*abort) break;
         }
-        umma_commit(dready);
       }
       __syncwarp();
       // wait for the epilogue to publish the next stage's X
       named_sync(1, 32 * (kEpiWarps + 1));
       if (snap[s & 1]) break;
     }
+  } else if (warp >= kGenWarp0) {
+    // ---- A-tile generators ------------------------------------------------------
+    // Row r = 32 gq + lane of the tile for 2 mi - kj = dl is Tv(d0 - c),
+    // c = 0..63, d0 = 64 dl + r; TMEM column j of a limb holds c = 2j, 2j+1,
+    // i.e. word(d0 - 2j).
+    const int gq = warp - kGenWarp0;
+    auto gen_tile = [&](int dl, int slot) {
+      const int base = 64 * dl + 32 * gq + lane - dlo;
+      const uint32_t ta = tmem + ((uint32_t)(32 * gq) << 16) + acol0 +
+                          (uint32_t)(slot * 2 * kACols);
+#pragma unroll
+      for (int half = 0; half < 2; ++half) {
+        uint32_t rh[16], rl[16];
+#pragma unroll
+        for (int jj = 0; jj < 16; ++jj) {
+          rh[jj] = tab_hi[base - 2 * (16 * half + jj)];
+          rl[jj] = tab_lo[base - 2 * (16 * half + jj)];
+        }
+        tmem_st16(ta + 16 * half, rh);
+        tmem_st16(ta + kACols + 16 * half, rl);
+      }
+    };
+    if (persist) {
+      for (int sl = 0; sl < ntile; ++sl) gen_tile(sl - (nK - 1), sl);
+      asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&afull[0]);
+    } else {
+      uint32_t it = 0;
+      for (int s = 0; s < total_stages && !*abort; ++s) {
+        for (int mi = 0; mi < nM && !*abort; ++mi) {
+          for (int kj = 0; kj < nK; ++kj, ++it) {
+            const int b = it & 1;
+            bool got = it < 2 || mbar_wait(&afree[b], ((it >> 1) - 1) & 1, abort);
+            got = __all_sync(0xffffffffu, got);
+            if (!got) break;
+            tc_fence_after();
+            gen_tile(2 * mi - kj, b);
+            asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&afull[b]);
+          }
+        }
+      }
+    }
   } else {
-    // ---- generator / epilogue warps -----------------------------------------------
+    // ---- drain / epilogue warps -----------------------------------------------------
     uint32_t it = 0;
+    const uint32_t lrow = tmem + ((uint32_t)(32 * q) << 16);
     for (int s = 0; s < total_stages; ++s) {
       const int stg = s & 3;
       // drive of this stage for the group's wires
@@ -462,150 +625,125 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
         }
         Msh[lane] = make_double2(-w.mscale * er, -w.mscale * ei);
       }
-      // Generate this stage's A tiles into the two TMEM buffers, in the order
-      // the MMA thread consumes them.  Row r = 32q + lane of tile (mi, kj) is
-      // Tv(d0 - c), c = 0..63, d0 = 128 mi + r - 64 kj; TMEM column j of a limb
-      // holds c = 2j, 2j+1, i.e. word(d0 - 2j).  This warp writes columns
-      // 16 hh .. 16 hh + 15 of both limbs.
-      for (int mi = 0; mi < nM && !*abort; ++mi) {
+      named_sync(2, 32 * kEpiWarps);
+      double pr[WH], pim[WH];
+#pragma unroll
+      for (int j = 0; j < WH; ++j) pr[j] = pim[j] = 0.0;
+      float cm[4 * WH];
+#pragma unroll
+      for (int c = 0; c < 4 * WH; ++c) cm[c] = 0.f;
+      const double* fx = xfac + (s & 1) * N;
+      for (int mi = 0; mi < nM; ++mi) {
+        const int k = mi * kTileRows + 32 * q + lane;
+        // exchange sums of this row for this warp's wires: slice blocks
+        // summed with round-to-nearest
+        float exs[4 * WH];
+#pragma unroll
+        for (int c = 0; c < 4 * WH; ++c) exs[c] = 0.f;
         for (int kj = 0; kj < nK; ++kj, ++it) {
           const int b = it & 1;
-          const uint32_t round = it >> 1;
-          if (round > 0 && !mbar_wait(&afree[b], (round - 1) & 1, abort)) break;
-          const int d0 = mi * kTileRows + 32 * q + lane - kj * kTileK;
-          const int base = d0 - 32 * hh - dlo;  // table index of word(d0 - 2*(16 hh))
-          uint32_t rh[16], rl[16];
+          bool got = mbar_wait(&dfull[b], (it >> 1) & 1, abort);
+          got = __all_sync(0xffffffffu, got);
+          if (!got) break;
+          tc_fence_after();
+          const uint32_t dm = lrow + (uint32_t)(2 * N * b + 4 * w0);
+          uint32_t rm[4 * WH], rc[4 * WH];
 #pragma unroll
-          for (int jj = 0; jj < 16; ++jj) {
-            rh[jj] = tab_hi[base - 2 * jj];
-            rl[jj] = tab_lo[base - 2 * jj];
+          for (int c = 0; c < 4 * WH; c += 8) {
+            tmem_ld8(dm + c, rm + c);
+            tmem_ld8(dm + N + c, rc + c);
           }
-          const uint32_t ta = tmem + ((uint32_t)(32 * q) << 16) + acol0 +
-                              (uint32_t)(b * 2 * kACols + 16 * hh);
-          tmem_st16(ta, rh);
-          tmem_st16(ta + kACols, rl);
-          asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+          tmem_ld_wait();
           tc_fence_before();
           __syncwarp();
-          if (lane == 0) mbar_arrive(&afull[b]);
+          if (lane == 0) mbar_arrive(&dfree[b]);
+#pragma unroll
+          for (int c = 0; c < 4 * WH; ++c)
+            exs[c] += __uint_as_float(rm[c]) + __uint_as_float(rc[c]);
+        }
+        if (*abort || k >= nk) continue;
+        // ---- epilogue of this k tile ----
+        const double ee = Ee[k], eh = Eh[k];
+#pragma unroll
+        for (int j = 0; j < WH; ++j) {
+          const int w = w0 + j;
+          if (w >= grp.nw) break;
+          const int64_t eg = woff[w] + k;
+          const int es = w * kpad + k;
+          double4* yp = RES ? s_y + es : g_y + eg;
+          float4* ysp = ys_ptr(w, k);
+          float4* accp = RES ? s_acc + es : a.ws_acc + eg;
+          const double4 par = wpar[w];
+          const double2 M = Msh[w];
+          const float4 ysf = *ysp;
+          const double ys[4] = {ysf.x, ysf.y, ysf.z, ysf.w};
+          // exchange sums (SBEs.py:896-921) from the tensor cores, the
+          // diagonal RHS (SBEs.py:1962-1975, 2325-2337, 2623-2636) in fp64
+          const double omr = M.x + fx[4 * w + 0] * (double)exs[4 * j + 0];
+          const double omi = M.y + fx[4 * w + 1] * (double)exs[4 * j + 1];
+          const double se = (ee + par.x) - fx[4 * w + 2] * (double)exs[4 * j + 2];
+          const double sh = eh - fx[4 * w + 3] * (double)exs[4 * j + 3];
+          const double sum = se + sh;
+          const double nn = ys[2] + ys[3] - 1.0;
+          const double xr = sum * ys[0] - omr * nn;
+          const double xi = sum * ys[1] - omi * nn;
+          const double hg = par.y;  // gamma
+          double f[4];
+          f[0] = xi * inv_hbar - hg * ys[0];
+          f[1] = -xr * inv_hbar - hg * ys[1];
+          f[2] = 2.0 * (omi * ys[0] - omr * ys[1]) * inv_hbar;
+          f[3] = f[2];
+          // RK4 stage combination (integrator.py:143-157): acc = k1 + 2 k2
+          // + 2 k3 (FP32 store), y += h/6 (acc + k4) in FP64
+          const double4 yv = *yp;
+          const double yy[4] = {yv.x, yv.y, yv.z, yv.w};
+          double nxt[4];
+          if (stg == 0) {
+            *accp = make_float4((float)f[0], (float)f[1], (float)f[2], (float)f[3]);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) nxt[c] = yy[c] + (h / 2.0) * f[c];
+          } else if (stg == 3) {
+            const float4 af = *accp;
+            const double ac[4] = {af.x, af.y, af.z, af.w};
+#pragma unroll
+            for (int c = 0; c < 4; ++c) nxt[c] = yy[c] + (h / 6.0) * (ac[c] + f[c]);
+            *yp = make_double4(nxt[0], nxt[1], nxt[2], nxt[3]);
+            pr[j] += nxt[0];
+            pim[j] += nxt[1];
+          } else {
+            const float4 af = *accp;
+            *accp = make_float4((float)((double)af.x + 2.0 * f[0]), (float)((double)af.y + 2.0 * f[1]),
+                                (float)((double)af.z + 2.0 * f[2]), (float)((double)af.w + 2.0 * f[3]));
+            const double c2 = stg == 1 ? h / 2.0 : h;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) nxt[c] = yy[c] + c2 * f[c];
+          }
+          const float4 nf = make_float4((float)nxt[0], (float)nxt[1], (float)nxt[2], (float)nxt[3]);
+          *ysp = nf;
+          track(cm, j, nf);
         }
       }
-      named_sync(2, 32 * kEpiWarps);
-      const bool got = mbar_wait(dready, s & 1, abort);
-      tc_fence_after();
-      if (got) {
-        double pr[WH], pim[WH];
+      if (stg == 3) {
+        // P(t) = pscale * sum_k p_k, reduced in a fixed order
 #pragma unroll
-        for (int j = 0; j < WH; ++j) pr[j] = pim[j] = 0.0;
-        for (int mi = 0; mi < nM; ++mi) {
-          const int k = mi * kTileRows + 32 * q + lane;
-          const uint32_t lrow = tmem + ((uint32_t)(32 * q) << 16);
-          const double ee = k < nk ? Ee[k] : 0.0, eh = k < nk ? Eh[k] : 0.0;
-          // wires in pairs: one 8-column TMEM load per accumulator, and the
-          // pair's element state loaded together for memory parallelism
-#pragma unroll 1
-          for (int jp = 0; jp < WH; jp += 2) {
-          uint32_t d1[8], d2[8];
-          tmem_ld8(lrow + (uint32_t)(mi * N + 4 * (w0 + jp)), d1);
-          tmem_ld8(lrow + ccol0 + (uint32_t)(mi * N + 4 * (w0 + jp)), d2);
-          tmem_ld_wait();
-          if (k >= nk) continue;
-          double4 ysv[2], yvv[2], accv[2];
+        for (int j = 0; j < WH; ++j) {
+          double sr = pr[j], si = pim[j];
 #pragma unroll
-          for (int u = 0; u < 2; ++u) {
-            if (w0 + jp + u < grp.nw) {
-              const int64_t e = woff[w0 + jp + u] + k;
-              ysv[u] = a.ws_ys[e];
-              yvv[u] = reinterpret_cast<const double4*>(a.y)[e];
-              if (stg != 0) accv[u] = a.ws_acc[e];
-            }
+          for (int o = 16; o > 0; o >>= 1) {
+            sr += __shfl_xor_sync(0xffffffffu, sr, o);
+            si += __shfl_xor_sync(0xffffffffu, si, o);
           }
-#pragma unroll
-          for (int u = 0; u < 2; ++u) {
-            const int j = jp + u;
-            const int w = w0 + j;
-            if (w >= grp.nw) break;
-            const int64_t e = woff[w] + k;
-            const double4 par = wpar[w];
-            const double2 M = Msh[w];
-            const double4 ys = ysv[u];
-            double ex[4];
-#pragma unroll
-            for (int c = 0; c < 4; ++c)
-              ex[c] = vscale * ((double)__uint_as_float(d1[4 * u + c]) +
-                                (double)__uint_as_float(d2[4 * u + c]));
-            // exchange sums (SBEs.py:896-921) from the tensor cores, the
-            // diagonal RHS (SBEs.py:1962-1975, 2325-2337, 2623-2636) in fp64
-            const double omr = M.x + ex[0];
-            const double omi = M.y + ex[1];
-            const double se = (ee + par.x) - ex[2];
-            const double sh = eh - ex[3];
-            const double sum = se + sh;
-            const double nn = ys.z + ys.w - 1.0;
-            const double xr = sum * ys.x - omr * nn;
-            const double xi = sum * ys.y - omi * nn;
-            const double hg = par.y;  // gamma
-            double f[4];
-            f[0] = xi / hbar - hg * ys.x;
-            f[1] = -xr / hbar - hg * ys.y;
-            const double uu = omi * ys.x - omr * ys.y;
-            f[2] = 2.0 * uu / hbar;
-            f[3] = f[2];
-            // RK4 stage combination in fp64 (integrator.py:143-157):
-            // acc = k1 + 2 k2 + 2 k3, y += h/6 (acc + k4)
-            const double4 yv = yvv[u];
-            const double yy[4] = {yv.x, yv.y, yv.z, yv.w};
-            double4 acc;
-            double nxt[4];
-            if (stg == 0) {
-              acc = make_double4(f[0], f[1], f[2], f[3]);
-#pragma unroll
-              for (int c = 0; c < 4; ++c) nxt[c] = yy[c] + (h / 2.0) * f[c];
-            } else if (stg == 3) {
-              acc = accv[u];
-              const double ac[4] = {acc.x, acc.y, acc.z, acc.w};
-#pragma unroll
-              for (int c = 0; c < 4; ++c) nxt[c] = yy[c] + (h / 6.0) * (ac[c] + f[c]);
-              reinterpret_cast<double4*>(a.y)[e] = make_double4(nxt[0], nxt[1], nxt[2], nxt[3]);
-              pr[j] += nxt[0];
-              pim[j] += nxt[1];
-            } else {
-              acc = accv[u];
-              acc.x += 2.0 * f[0];
-              acc.y += 2.0 * f[1];
-              acc.z += 2.0 * f[2];
-              acc.w += 2.0 * f[3];
-              const double c2 = stg == 1 ? h / 2.0 : h;
-#pragma unroll
-              for (int c = 0; c < 4; ++c) nxt[c] = yy[c] + c2 * f[c];
-            }
-            if (stg != 3) a.ws_acc[e] = acc;
-            const float v[4] = {(float)nxt[0], (float)nxt[1], (float)nxt[2], (float)nxt[3]};
-            a.ws_ys[e] = make_double4(nxt[0], nxt[1], nxt[2], nxt[3]);
-            store_x(k, w, v);
-          }
-          }
-        }
-        if (stg == 3) {
-          // P(t) = pscale * sum_k p_k, reduced in a fixed order
-#pragma unroll
-          for (int j = 0; j < WH; ++j) {
-            double sr = pr[j], si = pim[j];
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-              sr += __shfl_xor_sync(0xffffffffu, sr, o);
-              si += __shfl_xor_sync(0xffffffffu, si, o);
-            }
-            if (lane == 0) {
-              ppart[(0 * 4 + q) * W + w0 + j] = sr;
-              ppart[(1 * 4 + q) * W + w0 + j] = si;
-            }
+          if (lane == 0) {
+            ppart[(0 * 4 + q) * W + w0 + j] = sr;
+            ppart[(1 * 4 + q) * W + w0 + j] = si;
           }
         }
       }
-      fence_async_smem();
-      tc_fence_before();
+      if (F16) publish_colmax(cm);
       named_sync(2, 32 * kEpiWarps);
+      // next stage's X from the stage points (after every column maximum
+      // is in)
+      if (!*abort) x_pass((s + 1) & 1);
       if (stg == 3 && warp == 0 && lane < grp.nw) {
         const int w = lane;
         const int step = s >> 2;
@@ -627,6 +765,18 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
       if (warp == 0 && lane == 0) snap[s & 1] = *abort;
       named_sync(1, 32 * (kEpiWarps + 1));
       if (snap[s & 1]) break;
+    }
+    // resident state back to the caller's y
+    if (RES && !*abort) {
+      for (int mi = 0; mi < nM; ++mi) {
+        const int k = mi * kTileRows + 32 * q + lane;
+        if (k >= nk) continue;
+        for (int j = 0; j < WH; ++j) {
+          const int w = w0 + j;
+          if (w >= grp.nw) break;
+          g_y[woff[w] + k] = s_y[w * kpad + k];
+        }
+      }
     }
   }
 
@@ -653,7 +803,7 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
       wp->steps += a.nsteps;
       bool bad = false;
       for (int k = 0; k < nk; ++k) {
-        const double4 yv = reinterpret_cast<const double4*>(a.y)[woff[tid] + k];
+        const double4 yv = g_y[woff[tid] + k];
         bad |= !(isfinite(yv.x) && isfinite(yv.y) && isfinite(yv.z) && isfinite(yv.w));
       }
       if (bad && wp->status == PSB_OK) wp->status = PSB_ERR_NONFINITE;
@@ -661,22 +811,33 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   }
 }
 
-template <int W, bool F16>
-int launch(const Args& a, int nkmax, cudaStream_t s) {
-  uint32_t smem = 0;
-  for (int nk = 2; nk <= nkmax; ++nk) {
-    const uint32_t t = Layout<W>(nk).total;
-    if (t > smem) smem = t;
-  }
-  if (smem > kMaxDynSmem || tmem_need(nkmax, 4 * W) > 512)
+template <int W, bool RES>
+int max_nk() {
+  int best = 0;
+  for (int nk = 2; nk <= PSB_MAX_NK; ++nk)
+    if (Layout<W, RES>(nk).total <= kMaxDynSmem) best = nk;
+  return best;
+}
+
+template <int W, bool F16, bool RES>
+int launch_res(Args a, int nkmax, cudaStream_t s) {
+  const uint32_t smem = Layout<W, RES>(nkmax).total;  // monotone in nk
+  if (smem > kMaxDynSmem)
     return set_error(PSB_ERR_SIZE, "split form: nk %d does not fit a group of %d wires", nkmax,
                      W);
-  cudaError_t e = cudaFuncSetAttribute(split_rk4_kernel<W, F16>,
+  cudaError_t e = cudaFuncSetAttribute(split_rk4_kernel<W, F16, RES>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess)
     return set_error(PSB_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
-  split_rk4_kernel<W, F16><<<a.ngroups, kThreadsS, smem, s>>>(a);
+  a.smem_bytes = smem;
+  split_rk4_kernel<W, F16, RES><<<a.ngroups, kThreadsS, smem, s>>>(a);
   return check_cuda("split_rk4_kernel");
+}
+
+template <int W, bool F16>
+int launch(const Args& a, int nkmax, cudaStream_t s) {
+  if (nkmax <= max_nk<W, true>()) return launch_res<W, F16, true>(a, nkmax, s);
+  return launch_res<W, F16, false>(a, nkmax, s);
 }
 
 }  // namespace split
@@ -689,39 +850,41 @@ extern "C" int64_t psb_split_ws_bytes(int64_t n_state) {
   return 64 * n_state + 32;
 }
 
-extern "C" int psb_split_smem_bytes(int nk, int wgroup) {
-  if (nk < 2 || nk > PSB_MAX_NK) return set_error(PSB_ERR_SIZE, "nk %d out of range", nk);
-  if (wgroup == 16) return (int)split::Layout<16>(nk).total;
-  if (wgroup == 8) return (int)split::Layout<8>(nk).total;
-  if (wgroup == 4) return (int)split::Layout<4>(nk).total;
-  return set_error(PSB_ERR_INVALID, "wgroup must be 4, 8 or 16");
+extern "C" int psb_split_max_nk(int wgroup) {
+  if (wgroup == 8) return split::max_nk<8, false>();
+  if (wgroup == 4) return split::max_nk<4, false>();
+  return set_error(PSB_ERR_INVALID, "wgroup must be 4 or 8");
 }
 
-extern "C" int psb_split_max_nk(int wgroup) {
-  if (wgroup != 4 && wgroup != 8 && wgroup != 16)
-    return set_error(PSB_ERR_INVALID, "wgroup must be 4, 8 or 16");
-  int best = 0;
-  for (int nk = 2; nk <= PSB_MAX_NK; ++nk) {
-    const uint32_t sm = wgroup == 16 ? split::Layout<16>(nk).total
-                                     : (wgroup == 8 ? split::Layout<8>(nk).total
-                                                    : split::Layout<4>(nk).total);
-    if (sm <= split::kMaxDynSmem && split::tmem_need(nk, 4 * wgroup) <= 512) best = nk;
-  }
-  return best;
+extern "C" int psb_split_max_nk_resident(int wgroup) {
+  if (wgroup == 8) return split::max_nk<8, true>();
+  if (wgroup == 4) return split::max_nk<4, true>();
+  return set_error(PSB_ERR_INVALID, "wgroup must be 4 or 8");
+}
+
+extern "C" int psb_split_smem_bytes(int nk, int wgroup) {
+  if (nk < 2 || nk > PSB_MAX_NK) return set_error(PSB_ERR_SIZE, "nk %d out of range", nk);
+  if (wgroup == 8)
+    return (int)(nk <= split::max_nk<8, true>() ? split::Layout<8, true>(nk).total
+                                                 : split::Layout<8, false>(nk).total);
+  if (wgroup == 4)
+    return (int)(nk <= split::max_nk<4, true>() ? split::Layout<4, true>(nk).total
+                                                 : split::Layout<4, false>(nk).total);
+  return set_error(PSB_ERR_INVALID, "wgroup must be 4 or 8");
 }
 
 extern "C" int psb_rk4_split(const PsbTable* d_tables, int ntab, const double* d_tabdata,
                              int64_t n_tabdata, PsbWire* d_wires, int nw,
                              const PsbSplitGroup* d_groups, int ngroups, int wgroup, int nkmax,
                              int limb, double* d_y, int64_t n_state, void* d_ws,
-                             int64_t n_ws_bytes,
-                             int nsteps, double dt, double* d_P, int64_t n_P, int p_stride,
-                             int p_cap, const PsbModel* model, void* stream) {
+                             int64_t n_ws_bytes, int nsteps, double dt, double* d_P,
+                             int64_t n_P, int p_stride, int p_cap, const PsbModel* model,
+                             void* stream) {
   if (!d_tables || !d_tabdata || !d_wires || !d_groups || !d_y || !d_ws || !model || ntab <= 0 ||
       nw < 0 || ngroups < 0)
     return set_error(PSB_ERR_INVALID, "psb_rk4_split: null pointer or bad count");
-  if (wgroup != 4 && wgroup != 8 && wgroup != 16)
-    return set_error(PSB_ERR_INVALID, "psb_rk4_split: wgroup must be 4, 8 or 16");
+  if (wgroup != 4 && wgroup != 8)
+    return set_error(PSB_ERR_INVALID, "psb_rk4_split: wgroup must be 4 or 8");
   if (limb != PSB_LIMB_BF16 && limb != PSB_LIMB_FP16)
     return set_error(PSB_ERR_INVALID, "psb_rk4_split: limb must be PSB_LIMB_BF16 or _FP16");
   if (nkmax < 2 || nkmax > psb_split_max_nk(wgroup))
@@ -745,8 +908,8 @@ extern "C" int psb_rk4_split(const PsbTable* d_tables, int ntab, const double* d
   a.ngroups = ngroups;
   a.y = d_y;
   a.n_state = n_state;
-  a.ws_ys = (double4*)d_ws;
-  a.ws_acc = (double4*)((uint8_t*)d_ws + 32 * n_state);
+  a.ws_ys = (float4*)d_ws;
+  a.ws_acc = (float4*)((uint8_t*)d_ws + 16 * n_state);
   a.nsteps = nsteps;
   a.dt = dt;
   a.P = d_P;
@@ -755,12 +918,7 @@ extern "C" int psb_rk4_split(const PsbTable* d_tables, int ntab, const double* d
   a.p_cap = p_cap;
   a.hbar = model->hbar;
   cudaStream_t st = (cudaStream_t)stream;
-  if (limb == PSB_LIMB_FP16) {
-    if (wgroup == 16) return split::launch<16, true>(a, nkmax, st);
-    if (wgroup == 8) return split::launch<8, true>(a, nkmax, st);
-    return split::launch<4, true>(a, nkmax, st);
-  }
-  if (wgroup == 16) return split::launch<16, false>(a, nkmax, st);
-  if (wgroup == 8) return split::launch<8, false>(a, nkmax, st);
-  return split::launch<4, false>(a, nkmax, st);
+  if (limb == PSB_LIMB_FP16)
+    return wgroup == 8 ? split::launch<8, true>(a, nkmax, st) : split::launch<4, true>(a, nkmax, st);
+  return wgroup == 8 ? split::launch<8, false>(a, nkmax, st) : split::launch<4, false>(a, nkmax, st);
 }

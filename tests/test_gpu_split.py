@@ -1,9 +1,15 @@
 """GPU parity of the split-precision tensor-core form (psb_rk4_split).
 
-Tolerance (bf16 hi+lo exchange products accumulated in FP32, FP64
-right-hand side and stage combination): normwise relative error <= 1e-6 in
-P(t) (the target of the split form) and <= 1e-5 in the final p_k, n_e,k,
-n_h,k against the FP64 oracle / the reference goldens.
+Tolerance (16-bit hi+lo exchange products, each 64-wide slice of k'
+accumulated on the tensor cores and drained at once, FP64 right-hand side,
+FP32 stage point and RK accumulator, FP64 state), normwise relative error
+against the FP64 oracle / the reference goldens:
+  fp16 limbs (default): <= 1e-6 in P(t) (the target of the split form) and
+      <= 1e-5 in the final p_k, n_e,k, n_h,k;
+  bf16 limbs: the 16-bit representation of the Coulomb matrix leaves
+      ~1e-6 in P(t) on small grids, so <= 5e-6 in P(t) and <= 5e-5 in the
+      state.
+
 """
 
 import numpy as np
@@ -19,6 +25,8 @@ pytestmark = pytest.mark.gpu
 
 TOL = 1e-6
 TOL_STATE = 1e-5
+TOL_BF16 = 5e-6
+TOL_STATE_BF16 = 5e-5
 
 
 def test_split_small_single_wire(cuda):
@@ -57,7 +65,7 @@ def test_split_uneven_batch_vs_oracle(cuda, limb):
                         relerr(y[s, 2], yo[s, 2]), relerr(y[s, 3], yo[s, 3])])
     e = np.array(allerrs)
     print(f"split {limb}: max P err {e[:, 0].max():.2e}, max state err {e[:, 1:].max():.2e}")
-    tol_p, tol_s = (TOL, TOL_STATE) if limb == "fp16" else (3 * TOL, 3 * TOL_STATE)
+    tol_p, tol_s = (TOL, TOL_STATE) if limb == "fp16" else (TOL_BF16, TOL_STATE_BF16)
     assert e[:, 0].max() < tol_p and e[:, 1:].max() < tol_s, e
 
 
