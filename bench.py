@@ -44,8 +44,6 @@ def parse():
     ap.add_argument("--chunk", type=int, default=100, help="time steps per bench step")
     ap.add_argument("--form", default="plain", choices=["plain", "split"],
                     help="plain FP64 kernel or split hi+lo tensor-core kernel")
-    ap.add_argument("--limb", default="fp16", choices=["bf16", "fp16"],
-                    help="16-bit limb format of the split form")
     ap.add_argument("--nwires", type=int, default=0, help="override the workload's wire count")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -197,8 +195,7 @@ def run_ours(a):
 
     wl = make_workload(a.workload, rank, a.nwires)
     S = a.chunk
-    b = WireBatch(wl.grids, wl.wires, screened=wl.screened, p_cap=S, form=a.form,
-                  limb=a.limb)
+    b = WireBatch(wl.grids, wl.wires, screened=wl.screened, p_cap=S, form=a.form)
     stream = torch.cuda.current_stream()
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
     units = wl.units_per_step * S
@@ -264,16 +261,19 @@ def run_ours(a):
         peak_source = "measured in this run: psb_probe_fp64_fma (FMA loop)"
         bound = "fp64"
     else:
-        # the split algorithm's tensor-core work: 3 bf16 products x 4 columns
-        # x Nk MACs per element and stage (unpadded grid)
-        flops_launch = float(np.sum(wl.nks.astype(np.float64) ** 2)) * 96.0 * S
+        # the split algorithm's tensor-core work: 6 int8 digit products x 4
+        # columns x Nk MACs (2 ops) per element and stage, 4 stages per step
+        # (unpadded grid)
+        flops_launch = float(np.sum(wl.nks.astype(np.float64) ** 2)) * 192.0 * S
         peak, peak_source = measured_bf16_peak()
+        # dense int8 tensor rate is twice the bf16 rate on B200
+        peak, peak_source = 2.0 * peak, "2 x " + peak_source
         bound = "tensor"
     achieved = flops_launch / (avg_launch_ms * 1e-3) / 1e12
 
     line = {
         "metric": ("SBE wire*k*steps/s (plain FP64 RK4)" if a.form == "plain" else
-                   f"SBE wire*k*steps/s (split {a.limb}x3 tensor-core RK4)"),
+                   "SBE wire*k*steps/s (split int8-digit tensor-core RK4)"),
         "value": value,
         "unit": "wire*k*steps/s",
         "n_gpus": world,
@@ -283,7 +283,7 @@ def run_ours(a):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64" if a.form == "plain" else f"{a.limb}x3+f32acc+f64",
+        "dtype": "f64" if a.form == "plain" else "int8x3digits+s32acc+f64",
         "data": "synthetic (seeded configuration draws)",
         "config": {"workload": wl.name, "wires_per_gpu": len(wl.wires),
                    "wire_k_per_time_step": wl.units_per_step, "time_steps_per_bench_step": S,
@@ -291,7 +291,7 @@ def run_ours(a):
                    "parallelism": f"wires sharded, {world} independent GPU(s)"},
         "e2e": {"value": units * a.steps * world / (e2e_ms * 1e-3), "unit": "wire*k*steps/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "roofline": {"bound": bound, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+        "roofline": {"bound": bound, "achieved": achieved, "peak": peak, "unit": "TFLOP/s" if a.form == "plain" else "TOP/s",
                      "frac": achieved / peak, "traffic": None, "peak_source": peak_source,
                      "flops_per_launch": flops_launch},
         "gpu_launches": a.steps * b.launches_per_call,

@@ -223,26 +223,22 @@ int psb_leapfrog_f64(const PsbTable* d_tables, int ntab, const double* d_tabdata
  * grid of nk points (for capacity planning; tab_flags as above). */
 int psb_f64_smem_bytes(int nk, int tab_flags);
 
-/* ---- split-precision tensor-core form (sm_100a tcgen05) ------------------- */
+/* ---- split-precision tensor-core form (sm_100a tcgen05, kind::i8) --------- */
 /*
  * The batched form of the same RK4 step: per group of wires sharing one k
  * grid, the exchange sums of all wires are one contraction
- *   D[k][(w,v)] = sum_k' T[k][k'] X[k'][(w,v)],  T[k][k'] = V(|k-k'|)/vscale,
- * computed on the tensor cores as hi+lo split products of 16-bit limbs
- * (Th Xh + Th Xl + Tl Xh; bf16 or fp16 limbs), with vscale the power of two
- * at or above max V.  Every 64-wide slice of k' is accumulated in a fresh
- * tensor-memory block and drained at once, so the tensor cores' FP32
- * accumulation never runs over more than four K = 16 steps.  The O(Nk)
- * right-hand side and the stage point / RK accumulator are FP32, the state
- * y and the P(t) sums FP64 (FP64 layout of the plain form).  Target
- * accuracy: normwise relative error <= 1e-6 in P(t) against the FP64 form.
- * Requires PSB_TAB_EXCITONS | PSB_TAB_SHARED_V tables without screening.
+ *   D[k][(w,v)] = sum_k' V(|k-k'|) X[k'][(w,v)]
+ * computed on the integer tensor cores: V and X are written as three
+ * signed base-254 int8 digits each (V scaled by a power of two, X by a
+ * power of two per column), the six digit products of weight <= 4 are
+ * accumulated exactly in int32 and combined in FP64.  The O(Nk) right-hand
+ * side is FP64, the stage point and RK accumulator FP32, the state y and the
+ * P(t) sums FP64 (FP64 layout of the plain form).  Target accuracy:
+ * normwise relative error <= 1e-6 in P(t) and <= 1e-5 in the state against
+ * the FP64 form.  Requires PSB_TAB_EXCITONS | PSB_TAB_SHARED_V tables
+ * without screening.
  */
 #define PSB_SPLIT_WMAX 16
-/* 16-bit limb format of the split: bf16 (hi+lo ~ 16 significant bits) or
- * fp16 (hi+lo ~ 22 significant bits; same tensor-core rate). */
-#define PSB_LIMB_BF16 0
-#define PSB_LIMB_FP16 1
 /* One CTA's work: 1..wgroup wires of one table (same k grid); wire slots
  * past nw are ignored. */
 typedef struct PsbSplitGroup {
@@ -274,7 +270,7 @@ int psb_split_max_nk_resident(int wgroup);
  */
 int psb_rk4_split(const PsbTable* d_tables, int ntab, const double* d_tabdata, int64_t n_tabdata,
                   PsbWire* d_wires, int nw, const PsbSplitGroup* d_groups, int ngroups,
-                  int wgroup, int nkmax, int limb, double* d_y, int64_t n_state, void* d_ws,
+                  int wgroup, int nkmax, double* d_y, int64_t n_state, void* d_ws,
                   int64_t n_ws_bytes, int nsteps, double dt, double* d_P, int64_t n_P,
                   int p_stride, int p_cap, const PsbModel* model, void* stream);
 

@@ -35,7 +35,7 @@ _SIGNATURES = {
     "psb_split_smem_bytes": ([i32, i32], i32),
     "psb_split_max_nk": ([i32], i32),
     "psb_split_max_nk_resident": ([i32], i32),
-    "psb_rk4_split": ([vp, i32, vp, i64, vp, i32, vp, i32, i32, i32, i32, vp, i64, vp, i64, i32,
+    "psb_rk4_split": ([vp, i32, vp, i64, vp, i32, vp, i32, i32, i32, vp, i64, vp, i64, i32,
                        f64, vp, i64, i32, i32, vp, vp], i32),
 }
 

@@ -58,8 +58,6 @@ WIRE_DTYPE = np.dtype(
 MODEL_DTYPE = np.dtype([("hbar", "<f8"), ("flags", "<i4"), ("reserved", "<i4")], align=True)
 
 PSB_SPLIT_WMAX = 16
-PSB_LIMB_BF16 = 0
-PSB_LIMB_FP16 = 1
 SPLIT_GROUP_DTYPE = np.dtype(
     [("table", "<i4"), ("nw", "<i4"), ("wire", "<i4", (PSB_SPLIT_WMAX,))], align=True)
 

@@ -20,18 +20,16 @@ from . import _lib, abi, coulomb, device
 
 class WireBatch:
     """``form`` selects the step kernel: "plain" (FP64 throughout,
-    psb_rk4_f64) or "split" (bf16 hi+lo tensor-core exchange with FP32
-    right-hand side and FP64 stage combination, psb_rk4_split)."""
+    psb_rk4_f64) or "split" (exchange sums on the int8 tensor cores as exact
+    products of base-254 digits, FP64 right-hand side and state,
+    psb_rk4_split)."""
 
     def __init__(self, grids, wires, screened=False, excitons=True, p_cap=0, tables=None,
-                 tabdata=None, form="plain", limb="fp16"):
+                 tabdata=None, form="plain"):
         device.require_cuda()
         if form not in ("plain", "split"):
             raise ValueError("form must be 'plain' or 'split'")
-        if limb not in ("bf16", "fp16"):
-            raise ValueError("limb must be 'bf16' or 'fp16'")
         self.form = form
-        self.limb = abi.PSB_LIMB_FP16 if limb == "fp16" else abi.PSB_LIMB_BF16
         self.grids = list(grids)
         self.screened = bool(screened)
         if tables is None:
@@ -187,7 +185,7 @@ class WireBatch:
                     s.wait_event(fork)
             for (wg, groups, ng, nkmax), s in zip(self.split_launches, streams):
                 _lib.call("psb_rk4_split", *self._common(), device.ptr(groups), ng, wg, nkmax,
-                          self.limb, device.ptr(self.y), self.n_state, device.ptr(self.ws), self.ws.numel(),
+                          device.ptr(self.y), self.n_state, device.ptr(self.ws), self.ws.numel(),
                           int(nsteps), float(dt), device.ptr(self.P), self.P.shape[0],
                           int(p_stride), self.p_cap, abi.as_ptr(self.model),
                           device.stream_ptr(s))

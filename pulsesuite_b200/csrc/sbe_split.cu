@@ -1,58 +1,55 @@
 // sbe_split.cu -- split-precision batched SBE RK4 step on the 5th-generation
-// tensor cores (tcgen05 / TMEM), sm_100a.
+// tensor cores (tcgen05 / TMEM, kind::i8), sm_100a.
 //
 // The exchange sums of every right-hand side (pulsesuite/PSTD3D/SBEs.py:
 // 896-921) are, for W wires sharing one k grid, one dense contraction
-//     D[k][(w,v)] = sum_k' T[k][k'] X[k'][(w,v)],   T[k][k'] = V(|k-k'|)/vscale
-// with X the stage point (v: p_re, p_im, ne, nh).  T and X are split into
-// 16-bit hi + lo limbs and D = Th Xh + (Th Xl + Tl Xh) is formed on the
-// tensor cores (Tl Xl is below the resolution of the sum).
-//
-// Accuracy.  The tensor cores' FP32 accumulation aligns every product of a
-// K = 16 step to the largest term, accumulator included, and drops the bits
-// below: the error of one step grows with the accumulator, and it is biased.
-// Accumulated over all of k' (K up to 1024) that bias reached ~3e-6 in P(t).
-// So every 64-wide slice of k' goes into a fresh tensor-memory block (main
-// product and corrections apart, each at most four K = 16 steps deep) and is
-// drained at once; the slices are summed with round-to-nearest on the CUDA
-// cores.  What remains is the representation of T and X: T enters every
-// step unchanged, so its rounding acts as a small static change of the
-// Coulomb matrix and shifts the phase of p linearly in time.  bf16 limbs
-// (hi + lo: 16 bits) leave ~1e-6 in P(t) on small grids; fp16 limbs (22
-// bits, the default) reach ~1e-7 once T is scaled by 2^14 and every X column
-// by the power of two that puts its largest value in [2^14, 2^15), so that
-// no lo limb falls into the fp16 subnormals.  The right-hand side is FP64
-// (the band energies set the phase of p and must not be rounded), the stage
-// point and the RK accumulator FP32 and the state y FP64.
+//     D[k][(w,v)] = sum_k' T[k][k'] X[k'][(w,v)],   T[k][k'] = V(|k-k'|)
+// with X the stage point (v: p_re, p_im, ne, nh).  T and X are written as
+// three signed base-254 digits each (Ozaki-style slicing onto the integer
+// tensor cores):
+//     t = V / VS  (|t| < 1/2),    254 t  ~ a1 + a2/254 + a3/254^2
+//     x' = x * sc (|x'| < 1/2),   254 x' ~ b1 + b2/254 + b3/254^2
+// with int8 digits in [-127, 127], VS a power of two and sc a power of two
+// per X column (wire, variable) chosen each stage from the column's largest
+// value.  The products of digit weight i + j <= 4,
+//     D2 = sum a1 b1,  D3 = sum a1 b2 + a2 b1,  D4 = sum a1 b3 + a2 b2 + a3 b1,
+// are exact in int32 (|D| < 3 * 1024 * 127^2 < 2^31), so the tensor cores
+// add no rounding at all; the exchange sum is
+//     VS / (254^2 sc) * (D2 + D3/254 + D4/254^2)
+// in FP64.  The digits represent t and x' to 2^-24.6 of their scale (the
+// static part, from T, is ~5e-8 of a sum); the dropped products are below
+// that.  (FP32 accumulation of 16-bit limbs was measured to truncate every
+// K = 16 step with a bias of ~1e-7 of the sum, which compounds into the
+// phase of p.)  The right-hand side is FP64 (the band energies set the phase
+// of p), the stage point and the RK accumulator FP32 and the state y FP64.
 //
 // One CTA owns a group of W (4 or 8) wires for all `nsteps` RK4 steps,
 // 128-row tiles of k at a time:
-//   * X (the MMA B operand, N = 4W columns, wire-major) lives in shared
-//     memory, double buffered: stage s reads X[s & 1], its epilogue writes
-//     X[(s + 1) & 1], so the epilogue of a k tile overlaps the MMAs of the
-//     next tile;
+//   * X (the MMA B operand: three int8 digit planes, K-major, N = 4W
+//     columns) lives in shared memory, double buffered: stage s reads
+//     X[s & 1]; at the end of stage s the epilogue warps write X[(s+1) & 1]
+//     from the stage points;
 //   * T is Toeplitz and never stored as a matrix: each 128 x 64 tile of the
-//     A operand is generated straight into tensor memory by four generator
-//     warps from a table of limb pairs (Tv(d), Tv(d-1)) in shared memory --
-//     one 32-bit lookup per TMEM cell.  A tile depends only on 2 mi - kj
-//     (mi the row tile, kj the k' slice); when all distinct tiles fit in
-//     tensor memory (nk <= 256) they are generated once per call, else they
-//     stream through a double buffer;
-//   * one thread issues tcgen05.mma (M = 128, N = 4W, K = 16), three
-//     products per K step, into a double-buffered pair of slice blocks;
-//   * eight drain/epilogue warps sum the slices of a row tile and then
+//     A operand (three digit planes) is generated straight into tensor
+//     memory by four generator warps from tables of digit quads
+//     (a(d), a(d-1), a(d-2), a(d-3)) in shared memory -- one 32-bit lookup
+//     per TMEM cell.  A tile depends only on 2 mi - kj (mi the row tile, kj
+//     the 64-wide k' slice); when all distinct tiles fit in tensor memory
+//     they are generated once per call, else they stream through a double
+//     buffer;
+//   * one thread issues tcgen05.mma (M = 128, N = 4W, K = 32), six digit
+//     products per K step, into the three accumulators of a row tile; the
+//     accumulators are double buffered per row tile, so the epilogue of
+//     tile mi overlaps the MMAs of tile mi + 1;
+//   * eight drain/epilogue warps read a finished tile's accumulators and
 //     evaluate the diagonal SBE right-hand side and the RK4 stage
 //     combination (stage order of libpulsesuite/integrator.py:143-157);
-//     at the end of a stage they write the next X from the stage points
-//     with the column scales of that stage;
 //   * the per-element state (y FP64, stage point and accumulator FP32) stays
 //     in shared memory for the whole call when it fits (psb_split_max_nk_
 //     resident), else in the caller's workspace.
 // Every mbarrier wait is bounded; on a timeout the CTA records
 // PSB_ERR_TIMEOUT in its wires' status, waits for its MMAs, frees TMEM and
 // returns.
-#include <cuda_bf16.h>
-#include <cuda_fp16.h>
 #include <math.h>
 
 #include "psb_common.cuh"
@@ -65,10 +62,15 @@ constexpr int kGenWarp0 = 8;    // warps 8..11: A-tile generators
 constexpr int kGenWarps = 4;
 constexpr int kMmaWarp = 12;    // warp 12: TMEM owner + MMA issuer
 constexpr int kThreadsS = 32 * 13;
+constexpr int kEpiThreads = 32 * kEpiWarps;
 constexpr int kTileRows = 128;  // M of one MMA
-constexpr int kTileK = 64;      // k' per A tile and per drained slice
-constexpr int kACols = kTileK / 2;  // TMEM columns of one 16-bit limb of an A tile
+constexpr int kTileK = 64;      // k' per A tile
+constexpr int kKStep = 32;      // K of one kind::i8 MMA
+constexpr int kDigits = 3;
+constexpr int kPlaneCols = kTileK / 4;            // TMEM columns of one digit plane of a tile
+constexpr int kTileCols = kDigits * kPlaneCols;   // 48
 constexpr int kTmemCols = 512;
+constexpr double kBase = 254.0;
 constexpr uint32_t kSpinLimit = 1u << 26;
 // dynamic shared memory per CTA (the 227 KiB limit less the static
 // shared memory and alignment padding)
@@ -108,16 +110,14 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volati
   *abort = 1;
   return false;
 }
-// D[tmem] (+)= A[tmem] * B[smem desc]
-__device__ __forceinline__ void umma_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t bdesc,
+// D[tmem] (+)= A[tmem] * B[smem desc], int8 x int8 -> int32
+__device__ __forceinline__ void umma_i8(uint32_t d_tmem, uint32_t a_tmem, uint64_t bdesc,
                                         uint32_t idesc, uint32_t accum) {
-  uint32_t m0 = 0, m1 = 0, m2 = 0, m3 = 0;
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(
-          d_tmem),
-      "r"(a_tmem), "l"(bdesc), "r"(idesc), "r"(accum), "r"(m0), "r"(m1), "r"(m2), "r"(m3));
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "r"(a_tmem), "l"(bdesc), "r"(idesc), "r"(accum));
 }
 __device__ __forceinline__ void umma_commit(uint64_t* bar) {
   asm volatile(
@@ -159,48 +159,39 @@ __device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t* r) {
       : "memory");
 }
 
-// One 16-bit limb of the split: bf16 (8 significant bits) or fp16 (11
-// significant bits; values are O(1) after the vscale normalisation).
-template <bool F16>
-__device__ __forceinline__ uint16_t limb_bits(float v, float& back) {
-  if (F16) {
-    const __half hv = __float2half_rn(v);
-    back = __half2float(hv);
-    return __half_as_ushort(hv);
-  }
-  const __nv_bfloat16 bv = __float2bfloat16_rn(v);
-  back = __bfloat162float(bv);
-  return __bfloat16_as_ushort(bv);
-}
-// hi and lo limbs of v (v ~ hi + lo)
-template <bool F16>
-__device__ __forceinline__ void split2(float v, uint16_t& hi, uint16_t& lo) {
-  float b;
-  hi = limb_bits<F16>(v, b);
-  float b2;
-  lo = limb_bits<F16>(v - b, b2);
+// Three balanced base-254 digits of v, |v| < 1/2 (so |254 v| < 127): each
+// remainder is formed exactly with an FMA, every digit lies in [-127, 127].
+__device__ __forceinline__ void digits3(float v, int& d1, int& d2, int& d3) {
+  const float f1 = rintf(v * 254.f);
+  const float r1 = fmaf(v, 254.f, -f1);
+  const float f2 = rintf(r1 * 254.f);
+  const float r2 = fmaf(r1, 254.f, -f2);
+  const float f3 = rintf(r2 * 254.f);
+  d1 = max(-127, min(127, (int)f1));
+  d2 = max(-127, min(127, (int)f2));
+  d3 = max(-127, min(127, (int)f3));
 }
 
-// Shared-memory matrix descriptor, no swizzle (canonical interleaved layout
-// of 8 x 16-byte core matrices): start address, leading-dimension (K) and
-// stride-dimension (M/N) byte offsets, descriptor version 1.
+// Shared-memory matrix descriptor, no swizzle (canonical layout of 8-row x
+// 16-byte core matrices): start address, leading-dimension (K) byte offset,
+// stride-dimension (M/N) byte offset, descriptor version 1.
 __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
   return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
          ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 
-// Instruction descriptor of kind::f16: D f32, A and B bf16 (format 1) or
-// fp16 (format 0), A K-major (required for A in TMEM), B MN-major, M = 128,
-// N = n.
-__host__ __device__ constexpr uint32_t idesc_f16(int n, bool f16) {
-  return (1u << 4) | ((f16 ? 0u : 1u) << 7) | ((f16 ? 0u : 1u) << 10) | (1u << 16) |
-         ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kTileRows >> 4) << 24);
+// Instruction descriptor of kind::i8: D s32, A and B signed 8-bit, both
+// K-major, M = 128, N = n.
+__host__ __device__ constexpr uint32_t idesc_i8(int n) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) |
+         ((uint32_t)(kTileRows >> 4) << 24);
 }
 
-// Byte offset of element (k, col) in the X operand (MN-major, N columns
-// contiguous inside a core matrix): column groups at sbo, k groups at 128 B.
+// Byte offset of element (k, col) in one digit plane of X (K-major: 16 k of
+// a column contiguous in a core-matrix row, 8 columns per core matrix; core
+// matrices at 128 B along k, column groups at sbo = 8 kpad).
 __device__ __forceinline__ uint32_t x_off(int k, int col, uint32_t sbo) {
-  return (uint32_t)((col >> 3) * sbo + (k >> 3) * 128 + (k & 7) * 16 + (col & 7) * 2);
+  return (uint32_t)((col >> 3) * sbo + (k >> 4) * 128 + (col & 7) * 16 + (k & 15));
 }
 
 __host__ __device__ inline int kpad_of(int nk) { return (nk + kTileK - 1) / kTileK * kTileK; }
@@ -209,15 +200,15 @@ __host__ __device__ inline int mtiles_of(int nk) { return (nk + kTileRows - 1) /
 __host__ __device__ inline int ntiles_of(int nk) {
   return kpad_of(nk) / kTileK + 2 * (mtiles_of(nk) - 1);
 }
-// TMEM columns: two slice blocks of main product + corrections (4 N), then
-// the A slots (hi + lo limbs, 2 kACols each): all distinct tiles when they
-// fit (persistent), else a double buffer.
+// TMEM columns: two row-tile accumulator sets (D2, D3, D4: 3 N each), then
+// the A slots (3 digit planes): all distinct tiles when they fit
+// (persistent), else a double buffer.
 __host__ __device__ inline bool persistent_tiles(int nk, int n) {
-  return 4 * n + 2 * kACols * ntiles_of(nk) <= kTmemCols;
+  return 6 * n + kTileCols * ntiles_of(nk) <= kTmemCols;
 }
 __host__ __device__ inline int tmem_cols(int nk, int n) {
   const int slots = persistent_tiles(nk, n) ? ntiles_of(nk) : 2;
-  const int need = 4 * n + 2 * kACols * slots;
+  const int need = 6 * n + kTileCols * slots;
   int c = 32;
   while (c < need) c <<= 1;
   return c;
@@ -251,29 +242,30 @@ struct Args {
 template <int W, bool RES>
 struct Layout {
   static constexpr int N = 4 * W;
-  uint32_t xbuf, st, tab, bars, misc, total;
+  uint32_t plane, xbuf, st, tab, bars, misc, total;
   int ntab_words;
   __host__ __device__ Layout(int nk) {
     const int kpad = kpad_of(nk), nM = mtiles_of(nk);
-    xbuf = 2u * (uint32_t)kpad * N * 2;  // one stage buffer: hi + lo limbs
+    plane = (uint32_t)kpad * N;  // one digit plane of X
+    xbuf = kDigits * plane;      // one stage buffer
     st = 2 * xbuf;
     tab = st + (RES ? 64u * W * (uint32_t)kpad : 0u);
     ntab_words = kTileRows * nM + kpad;
-    bars = tab + 2 * 4 * (uint32_t)ntab_words;  // hi and lo pair tables
+    bars = tab + kDigits * 4 * (uint32_t)ntab_words;  // digit-quad tables
     bars = (bars + 15) & ~15u;
     misc = bars + 8 * 12;  // afull[2], afree[2], dfull[2], dfree[2], final
-    // misc: tmem base (16 B), abort + snapshots (16 B), M re/im double2[W],
-    // wire params (gap, gamma, mscale, pscale: double4[W]), t double[W],
-    // off int64[W], P partials double[2][4][W], X column decode factors
-    // double[2][N], column maxima float[4][N]
-    total = misc + 32 + 256 * W;
+    // misc: tmem base (16 B), abort + snapshots (16 B), pulse constants
+    // double[W][2][4], wire params double4[W], t double[W], off int64[W],
+    // P partials double[2][4][W], X column decode factors double[2][N],
+    // column maxima float[4][N]
+    total = misc + 32 + 368 * W;
   }
 };
 
 // ---------------------------------------------------------------------------
 // The kernel.
 // ---------------------------------------------------------------------------
-template <int W, bool F16, bool RES>
+template <int W, bool RES>
 __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   constexpr int N = 4 * W;
   constexpr int WH = W / 2;  // wires per drain/epilogue warp
@@ -294,7 +286,8 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
     for (int i = 0; ok && i < grp.nw; ++i) {
       const int wi = grp.wire[i];
       ok = wi >= 0 && wi < a.nw && a.wires[wi].table == grp.table && a.wires[wi].off >= 0 &&
-           a.wires[wi].off + tb.nk <= a.n_state;
+           a.wires[wi].off + tb.nk <= a.n_state && a.wires[wi].npulse >= 0 &&
+           a.wires[wi].npulse <= 2;
     }
   }
   if (!ok) {
@@ -306,12 +299,11 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   const Layout<W, RES> L(nk);
   const bool persist = persistent_tiles(nk, N);
   const int ntile = ntiles_of(nk);
-  uint8_t* xbase = smem;  // X[b]: hi at xbase + b xbuf, lo at + xbuf/2
+  uint8_t* xbase = smem;  // X[b] digit plane p at xbase + b xbuf + p plane
   double4* s_y = reinterpret_cast<double4*>(smem + L.st);
   float4* s_ys = reinterpret_cast<float4*>(smem + L.st + 32u * W * kpad);
   float4* s_acc = reinterpret_cast<float4*>(smem + L.st + 48u * W * kpad);
-  uint32_t* tab_hi = reinterpret_cast<uint32_t*>(smem + L.tab);
-  uint32_t* tab_lo = tab_hi + L.ntab_words;
+  uint32_t* tabq = reinterpret_cast<uint32_t*>(smem + L.tab);  // [digit][word]
   uint64_t* afull = reinterpret_cast<uint64_t*>(smem + L.bars);
   uint64_t* afree = afull + 2;
   uint64_t* dfull = afree + 2;
@@ -322,21 +314,20 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   // abort as seen at each stage's end barrier (written by one participant
   // before the barrier, read by all after it, so every role breaks together)
   volatile int* snap = reinterpret_cast<volatile int*>(smem + L.misc + 20);
-  double2* Msh = reinterpret_cast<double2*>(smem + L.misc + 32);
-  double4* wpar = reinterpret_cast<double4*>(smem + L.misc + 32 + 16 * W);
-  double* wt = reinterpret_cast<double*>(smem + L.misc + 32 + 48 * W);
-  int64_t* woff = reinterpret_cast<int64_t*>(smem + L.misc + 32 + 56 * W);
-  double* ppart = reinterpret_cast<double*>(smem + L.misc + 32 + 64 * W);
-  double* xfac = reinterpret_cast<double*>(smem + L.misc + 32 + 128 * W);
-  float* colmax = reinterpret_cast<float*>(smem + L.misc + 32 + 192 * W);
-  const uint32_t xsbo = (uint32_t)(kpad / 8) * 128;
-  const uint32_t xlimb = L.xbuf / 2;
+  double* pulse = reinterpret_cast<double*>(smem + L.misc + 32);  // [W][2][4]
+  double4* wpar = reinterpret_cast<double4*>(smem + L.misc + 32 + 64 * W);
+  double* wt = reinterpret_cast<double*>(smem + L.misc + 32 + 96 * W);
+  int64_t* woff = reinterpret_cast<int64_t*>(smem + L.misc + 32 + 104 * W);
+  double* ppart = reinterpret_cast<double*>(smem + L.misc + 32 + 112 * W);
+  double* xfac = reinterpret_cast<double*>(smem + L.misc + 32 + 176 * W);
+  float* colmax = reinterpret_cast<float*>(smem + L.misc + 32 + 240 * W);
+  const uint32_t xsbo = (uint32_t)kpad * 8;
   const double* blk = a.tabdata + tb.off;
   const double* Ee = blk + 3 * nk;
   const double* Eh = blk + 4 * nk;
 
   // ---- set-up ---------------------------------------------------------------
-  // vscale: the power of two at or above max V, so T = V/vscale is exact.
+  // VS: the power of two with max V < VS / 2, so |t| < 1/2.
   __shared__ double vmax_w[kThreadsS / 32];
   double vm = 0.0;
   for (int qq = 1 + tid; qq < nk; qq += kThreadsS) vm = fmax(vm, fabs(blk[qq]));
@@ -359,15 +350,31 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (tid < W) {
+    // per pulse: t0, -4 ln2 / fwhm^2, and -mscale * amp * (cos, sin)(phase),
+    // so M(t) = sum (c2, c3) exp(c1 (t - t0)^2)  (SBEs drive, E(t) Gaussian)
+    double* pc = pulse + tid * 8;
     if (tid < grp.nw) {
       const PsbWire& w = a.wires[grp.wire[tid]];
       wpar[tid] = make_double4(w.gap, w.gamma, w.mscale, w.pscale);
       wt[tid] = w.t;
       woff[tid] = w.off;
+      for (int j = 0; j < 2; ++j) {
+        if (j < w.npulse) {
+          double sn, cs;
+          sincos(w.phase[j], &sn, &cs);
+          pc[4 * j + 0] = w.t0[j];
+          pc[4 * j + 1] = -4.0 * log(2.0) / (w.fwhm[j] * w.fwhm[j]);
+          pc[4 * j + 2] = -w.mscale * w.amp[j] * cs;
+          pc[4 * j + 3] = -w.mscale * w.amp[j] * sn;
+        } else {
+          pc[4 * j + 0] = pc[4 * j + 1] = pc[4 * j + 2] = pc[4 * j + 3] = 0.0;
+        }
+      }
     } else {
       wpar[tid] = make_double4(0.0, 0.0, 0.0, 0.0);
       wt[tid] = 0.0;
       woff[tid] = -1;
+      for (int j = 0; j < 8; ++j) pc[j] = 0.0;
     }
   }
   const int ncols = tmem_cols(nk, N);
@@ -381,33 +388,40 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
-  // TMEM column map: slice blocks Dm[b] at 2N b, Dc[b] at 2N b + N; A slot i
-  // at acol0 + 2 kACols i (hi limb, then lo limb).
-  const uint32_t acol0 = (uint32_t)(4 * N);
+  // TMEM column map: accumulator set b at 3 N b (D2, D3, D4 at +0, +N,
+  // +2N); A slot i at acol0 + kTileCols i (digit plane p at + kPlaneCols p).
+  const uint32_t acol0 = (uint32_t)(6 * N);
   double vmax = 0.0;
 #pragma unroll
   for (int i = 0; i < kThreadsS / 32; ++i) vmax = fmax(vmax, vmax_w[i]);
   int ex = 0;
-  frexp(vmax > 0.0 ? vmax : 1.0, &ex);
-  // fp16 limbs: T scaled by 2^14 so that its lo limbs stay normal numbers
-  const int tsh = F16 ? 14 : 0;
-  const double vscale = ldexp(1.0, ex - tsh);  // V = vscale * T
-  const double inv_vscale = ldexp(1.0, tsh - ex);
-  // Pair tables: word(d) = (Tv(d), Tv(d-1)) for d in [2 - kpad, 128 nM - 1],
-  // Tv(d) = limb of V(|d|)/vscale (0 at d = 0 and outside the grid).
-  const int dlo = 2 - kpad;
+  frexp(vmax > 0.0 ? vmax : 1.0, &ex);  // vmax < 2^ex
+  const double VS = ldexp(1.0, ex + 1);
+  const double inv_VS = ldexp(1.0, -ex - 1);
+  // Digit-quad tables: word(d) = bytes (a(d), a(d-1), a(d-2), a(d-3)) of one
+  // digit plane for d in [dlo, dlo + ntab_words), a(d) = digit of
+  // V(|d|)/VS (0 at d = 0 and outside the grid).
+  const int dlo = 4 - kpad;
   for (int i = tid; i < L.ntab_words; i += kThreadsS) {
     const int d = dlo + i;
-    uint16_t h[2], l[2];
+    uint32_t wq[kDigits] = {0u, 0u, 0u};
 #pragma unroll
-    for (int u = 0; u < 2; ++u) {
+    for (int u = 0; u < 4; ++u) {
       const int dd = d - u;
       const int ad = dd < 0 ? -dd : dd;
-      const float v = (ad > 0 && ad < nk) ? (float)(blk[ad] * inv_vscale) : 0.f;
-      split2<F16>(v, h[u], l[u]);
+      const double t = (ad > 0 && ad < nk) ? blk[ad] * inv_VS : 0.0;
+      // digits of t from its FP64 value
+      const double f1 = rint(t * kBase);
+      const double r1 = t * kBase - f1;
+      const double f2 = rint(r1 * kBase);
+      const double r2 = r1 * kBase - f2;
+      const double f3 = rint(r2 * kBase);
+      const int dg[3] = {(int)f1, (int)f2, (int)f3};
+#pragma unroll
+      for (int p = 0; p < kDigits; ++p) wq[p] |= ((uint32_t)(dg[p] & 0xFF)) << (8 * u);
     }
-    tab_hi[i] = (uint32_t)h[0] | ((uint32_t)h[1] << 16);
-    tab_lo[i] = (uint32_t)l[0] | ((uint32_t)l[1] << 16);
+#pragma unroll
+    for (int p = 0; p < kDigits; ++p) tabq[p * L.ntab_words + i] = wq[p];
   }
 
   // ---- element ownership of the drain/epilogue warps -----------------------------
@@ -420,9 +434,8 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   auto ys_ptr = [&](int w, int k) -> float4* {
     return RES ? s_ys + (w * kpad + k) : a.ws_ys + (woff[w] + k);
   };
-  // Largest |value| of each of this warp's X columns (fp16 limbs only),
-  // published per lane quarter q.
-  auto publish_colmax = [&](float* cm) {
+  // Largest |value| of each of this warp's X columns, per lane quarter q.
+  auto publish_colmax = [&](const float* cm) {
 #pragma unroll
     for (int c = 0; c < 4 * WH; ++c) {
       float m = cm[c];
@@ -431,64 +444,73 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
       if (lane == 0) colmax[q * N + 4 * w0 + c] = m;
     }
   };
-  // X[b] = split(stage point * column scale) for this thread's elements.
-  // fp16: the column scale is the power of two that puts the column's
-  // largest value in [2^14, 2^15) (lo limbs stay normal, nothing
-  // overflows); xfac[b] = vscale / scale decodes the exchange sums.
+  auto track = [&](float* cm, int j, float4 v) {
+    cm[4 * j + 0] = fmaxf(cm[4 * j + 0], fabsf(v.x));
+    cm[4 * j + 1] = fmaxf(cm[4 * j + 1], fabsf(v.y));
+    cm[4 * j + 2] = fmaxf(cm[4 * j + 2], fabsf(v.z));
+    cm[4 * j + 3] = fmaxf(cm[4 * j + 3], fabsf(v.w));
+  };
+  // Column scale exponent: the power of two that puts the column's largest
+  // value in [1/4, 1/2).
+  auto col_exp = [&](int col) -> int {
+    const float m = fmaxf(fmaxf(colmax[col], colmax[N + col]),
+                          fmaxf(colmax[2 * N + col], colmax[3 * N + col]));
+    int sexp = 0;
+    if (m > 0.f && isfinite(m)) {
+      int e2;
+      frexpf(m, &e2);  // m < 2^e2
+      sexp = min(max(-1 - e2, -120), 120);
+    }
+    return sexp;
+  };
+  // X[b] = digits(stage point * column scale), all elements of the group:
+  // one item = 4 consecutive k of one wire (a 32-bit word per variable and
+  // digit plane).  xfac[b] decodes the exchange sums.
   auto x_pass = [&](int b) {
-    float sc[4 * WH];
+    const int et = tid;  // 0 .. kEpiThreads-1
+    if (et < N) {
+      const int sexp = col_exp(et);
+      xfac[b * N + et] = ldexp(VS / (kBase * kBase), -sexp);
+    }
+    const int nq = (nk + 3) >> 2;
+    uint8_t* xb = xbase + b * L.xbuf;
+    for (int item = et; item < grp.nw * nq; item += kEpiThreads) {
+      const int w = item / nq;
+      const int k0 = (item - w * nq) * 4;
+      float sc[4];
 #pragma unroll
-    for (int c = 0; c < 4 * WH; ++c) {
-      int sexp = 0;
-      if (F16) {
-        const int col = 4 * w0 + c;
-        const float m = fmaxf(fmaxf(colmax[col], colmax[N + col]),
-                              fmaxf(colmax[2 * N + col], colmax[3 * N + col]));
-        if (m > 0.f && isfinite(m)) {
-          int e2;
-          frexpf(m, &e2);  // m < 2^e2
-          sexp = min(max(15 - e2, -100), 100);
+      for (int v = 0; v < 4; ++v) sc[v] = ldexpf(1.f, col_exp(4 * w + v));
+      uint32_t word[4][kDigits];
+#pragma unroll
+      for (int v = 0; v < 4; ++v)
+#pragma unroll
+        for (int p = 0; p < kDigits; ++p) word[v][p] = 0u;
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        if (k0 + u >= nk) break;
+        const float4 yv = *ys_ptr(w, k0 + u);
+        const float vv[4] = {yv.x, yv.y, yv.z, yv.w};
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          int d1, d2, d3;
+          digits3(vv[v] * sc[v], d1, d2, d3);
+          word[v][0] |= ((uint32_t)(d1 & 0xFF)) << (8 * u);
+          word[v][1] |= ((uint32_t)(d2 & 0xFF)) << (8 * u);
+          word[v][2] |= ((uint32_t)(d3 & 0xFF)) << (8 * u);
         }
       }
-      sc[c] = ldexpf(1.f, sexp);
-      if (q == 0 && lane == c) xfac[b * N + 4 * w0 + c] = ldexp(vscale, -sexp);
-    }
-    uint8_t* xh = xbase + b * L.xbuf;
-    for (int mi = 0; mi < nM; ++mi) {
-      const int k = mi * kTileRows + 32 * q + lane;
-      if (k >= nk) continue;
 #pragma unroll
-      for (int j = 0; j < WH; ++j) {
-        const int w = w0 + j;
-        if (w >= grp.nw) break;
-        const float4 v = *ys_ptr(w, k);
-        uint16_t hi[4], lo[4];
-        split2<F16>(v.x * sc[4 * j + 0], hi[0], lo[0]);
-        split2<F16>(v.y * sc[4 * j + 1], hi[1], lo[1]);
-        split2<F16>(v.z * sc[4 * j + 2], hi[2], lo[2]);
-        split2<F16>(v.w * sc[4 * j + 3], hi[3], lo[3]);
-        const uint32_t o = x_off(k, 4 * w, xsbo);
-        uint2 ph, pl;
-        ph.x = (uint32_t)hi[0] | ((uint32_t)hi[1] << 16);
-        ph.y = (uint32_t)hi[2] | ((uint32_t)hi[3] << 16);
-        pl.x = (uint32_t)lo[0] | ((uint32_t)lo[1] << 16);
-        pl.y = (uint32_t)lo[2] | ((uint32_t)lo[3] << 16);
-        *reinterpret_cast<uint2*>(xh + o) = ph;
-        *reinterpret_cast<uint2*>(xh + xlimb + o) = pl;
+      for (int v = 0; v < 4; ++v) {
+        const uint32_t o = x_off(k0, 4 * w + v, xsbo);
+#pragma unroll
+        for (int p = 0; p < kDigits; ++p)
+          *reinterpret_cast<uint32_t*>(xb + p * L.plane + o) = word[v][p];
       }
     }
     fence_async_smem();
   };
-  auto track = [&](float* cm, int j, float4 v) {
-    if (F16) {
-      cm[4 * j + 0] = fmaxf(cm[4 * j + 0], fabsf(v.x));
-      cm[4 * j + 1] = fmaxf(cm[4 * j + 1], fabsf(v.y));
-      cm[4 * j + 2] = fmaxf(cm[4 * j + 2], fabsf(v.z));
-      cm[4 * j + 3] = fmaxf(cm[4 * j + 3], fabsf(v.w));
-    }
-  };
 
-  // Stage-0 input: X[0] = split(y), stage point = y.
+  // Stage-0 input: stage point = y, X[0] = digits(y).
   if (warp < kEpiWarps) {
     float cm0[4 * WH];
 #pragma unroll
@@ -508,75 +530,89 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
       }
     }
     publish_colmax(cm0);
-    named_sync(2, 32 * kEpiWarps);
+    named_sync(2, kEpiThreads);
     x_pass(0);
   }
   __syncthreads();
 
-  const uint32_t idesc = idesc_f16(N, F16);
+  const uint32_t idesc = idesc_i8(N);
   const int total_stages = a.nsteps * 4;
   const double h = a.dt;
   const double inv_hbar = 1.0 / a.hbar;
 
   if (warp == kMmaWarp) {
     // ---- MMA issuer -----------------------------------------------------------
-    uint32_t it = 0;
+    uint32_t it = 0;  // row tiles issued
+    uint32_t ct = 0;  // streamed A tiles consumed
     for (int s = 0; s < total_stages; ++s) {
       if (lane == 0 && !*abort) {
         if (s == 0 && persist) mbar_wait(&afull[0], 0, abort);
         tc_fence_after();
-        const uint32_t xh = smem_u32(xbase + (s & 1) * L.xbuf);
-        const uint32_t xl = xh + xlimb;
-        for (int mi = 0; mi < nM && !*abort; ++mi) {
-          for (int kj = 0; kj < nK; ++kj, ++it) {
-            const int b = it & 1;
-            if (!persist && !mbar_wait(&afull[b], (it >> 1) & 1, abort)) break;
-            if (it >= 2 && !mbar_wait(&dfree[b], ((it >> 1) - 1) & 1, abort)) break;
-            tc_fence_after();
-            const int slot = persist ? 2 * mi - kj + nK - 1 : b;
-            const uint32_t ah = tmem + acol0 + (uint32_t)(slot * 2 * kACols);
-            const uint32_t al = ah + kACols;
-            const uint32_t dm = tmem + (uint32_t)(2 * N * b);
-            const uint32_t dc = dm + (uint32_t)N;
-#pragma unroll
-            for (int ks = 0; ks < kTileK / 16; ++ks) {
-              const int k0 = kj * kTileK + ks * 16;
-              const uint64_t dbh = smem_desc(xh + (k0 >> 3) * 128, 128, xsbo);
-              const uint64_t dbl = smem_desc(xl + (k0 >> 3) * 128, 128, xsbo);
-              umma_ts(dm, ah + ks * 8, dbh, idesc, ks != 0);
-              umma_ts(dc, ah + ks * 8, dbl, idesc, ks != 0);
-              umma_ts(dc, al + ks * 8, dbh, idesc, 1);
+        const uint32_t x0 = smem_u32(xbase + (s & 1) * L.xbuf);
+        for (int mi = 0; mi < nM && !*abort; ++mi, ++it) {
+          const int b = it & 1;
+          if (it >= 2 && !mbar_wait(&dfree[b], ((it >> 1) - 1) & 1, abort)) break;
+          tc_fence_after();
+          const uint32_t d2 = tmem + (uint32_t)(3 * N * b);
+          const uint32_t d3 = d2 + (uint32_t)N;
+          const uint32_t d4 = d2 + (uint32_t)(2 * N);
+          for (int kj = 0; kj < nK; ++kj) {
+            int slot;
+            if (persist) {
+              slot = 2 * mi - kj + nK - 1;
+            } else {
+              slot = ct & 1;
+              if (!mbar_wait(&afull[slot], (ct >> 1) & 1, abort)) break;
+              tc_fence_after();
             }
-            if (!persist) umma_commit(&afree[b]);  // A slot reusable once these finish
-            umma_commit(&dfull[b]);                // the slice is ready to drain
+            const uint32_t a1 = tmem + acol0 + (uint32_t)(slot * kTileCols);
+            const uint32_t a2 = a1 + kPlaneCols;
+            const uint32_t a3 = a2 + kPlaneCols;
+#pragma unroll
+            for (int ks = 0; ks < kTileK / kKStep; ++ks) {
+              const int k0 = kj * kTileK + ks * kKStep;
+              const uint32_t xo = x0 + (uint32_t)(k0 >> 4) * 128;
+              const uint64_t b1 = smem_desc(xo, 128, xsbo);
+              const uint64_t b2 = smem_desc(xo + L.plane, 128, xsbo);
+              const uint64_t b3 = smem_desc(xo + 2 * L.plane, 128, xsbo);
+              const uint32_t first = (kj | ks) != 0;
+              const uint32_t ac = ks * (kKStep / 4);  // TMEM columns of this K step
+              umma_i8(d2, a1 + ac, b1, idesc, first);
+              umma_i8(d3, a1 + ac, b2, idesc, first);
+              umma_i8(d3, a2 + ac, b1, idesc, 1);
+              umma_i8(d4, a1 + ac, b3, idesc, first);
+              umma_i8(d4, a2 + ac, b2, idesc, 1);
+              umma_i8(d4, a3 + ac, b1, idesc, 1);
+            }
+            if (!persist) {
+              umma_commit(&afree[slot]);  // A slot reusable once these finish
+              ++ct;
+            }
           }
+          umma_commit(&dfull[b]);  // the row tile is ready to drain
         }
       }
       __syncwarp();
       // wait for the epilogue to publish the next stage's X
-      named_sync(1, 32 * (kEpiWarps + 1));
+      named_sync(1, kEpiThreads + 32);
       if (snap[s & 1]) break;
     }
   } else if (warp >= kGenWarp0) {
     // ---- A-tile generators ------------------------------------------------------
-    // Row r = 32 gq + lane of the tile for 2 mi - kj = dl is Tv(d0 - c),
-    // c = 0..63, d0 = 64 dl + r; TMEM column j of a limb holds c = 2j, 2j+1,
-    // i.e. word(d0 - 2j).
+    // Row r = 32 gq + lane of the tile for 2 mi - kj = dl is a(d0 - c),
+    // c = 0..63, d0 = 64 dl + r; TMEM column j of a digit plane holds
+    // c = 4j .. 4j+3, i.e. word(d0 - 4j).
     const int gq = warp - kGenWarp0;
     auto gen_tile = [&](int dl, int slot) {
       const int base = 64 * dl + 32 * gq + lane - dlo;
       const uint32_t ta = tmem + ((uint32_t)(32 * gq) << 16) + acol0 +
-                          (uint32_t)(slot * 2 * kACols);
+                          (uint32_t)(slot * kTileCols);
 #pragma unroll
-      for (int half = 0; half < 2; ++half) {
-        uint32_t rh[16], rl[16];
+      for (int p = 0; p < kDigits; ++p) {
+        uint32_t r[16];
 #pragma unroll
-        for (int jj = 0; jj < 16; ++jj) {
-          rh[jj] = tab_hi[base - 2 * (16 * half + jj)];
-          rl[jj] = tab_lo[base - 2 * (16 * half + jj)];
-        }
-        tmem_st16(ta + 16 * half, rh);
-        tmem_st16(ta + kACols + 16 * half, rl);
+        for (int j = 0; j < 16; ++j) r[j] = tabq[p * L.ntab_words + base - 4 * j];
+        tmem_st16(ta + p * kPlaneCols, r);
       }
     };
     if (persist) {
@@ -586,12 +622,12 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
       __syncwarp();
       if (lane == 0) mbar_arrive(&afull[0]);
     } else {
-      uint32_t it = 0;
+      uint32_t ct = 0;
       for (int s = 0; s < total_stages && !*abort; ++s) {
         for (int mi = 0; mi < nM && !*abort; ++mi) {
-          for (int kj = 0; kj < nK; ++kj, ++it) {
-            const int b = it & 1;
-            bool got = it < 2 || mbar_wait(&afree[b], ((it >> 1) - 1) & 1, abort);
+          for (int kj = 0; kj < nK; ++kj, ++ct) {
+            const int b = ct & 1;
+            bool got = ct < 2 || mbar_wait(&afree[b], ((ct >> 1) - 1) & 1, abort);
             got = __all_sync(0xffffffffu, got);
             if (!got) break;
             tc_fence_after();
@@ -608,24 +644,23 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
     // ---- drain / epilogue warps -----------------------------------------------------
     uint32_t it = 0;
     const uint32_t lrow = tmem + ((uint32_t)(32 * q) << 16);
+    // lane j < WH keeps the time of wire w0 + j
+    double tj = (lane < WH) ? wt[w0 + lane] : 0.0;
     for (int s = 0; s < total_stages; ++s) {
       const int stg = s & 3;
-      // drive of this stage for the group's wires
-      if (warp == 0 && lane < grp.nw) {
-        const PsbWire& w = a.wires[grp.wire[lane]];
-        const double t = wt[lane] + (stg == 0 ? 0.0 : (stg == 3 ? h : h / 2.0));
-        double er = 0.0, ei = 0.0;
-        for (int j = 0; j < w.npulse && j < 2; ++j) {
-          const double u = (t - w.t0[j]) / w.fwhm[j];
-          const double env = w.amp[j] * exp(-4.0 * log(2.0) * u * u);
-          double sn, cs;
-          sincos(w.phase[j], &sn, &cs);
-          er += env * cs;
-          ei += env * sn;
+      // drive of this stage: lane j < WH evaluates wire w0 + j
+      double Mr = 0.0, Mi = 0.0;
+      if (lane < WH) {
+        const double t = tj + (stg == 0 ? 0.0 : (stg == 3 ? h : h / 2.0));
+        const double* pc = pulse + (w0 + lane) * 8;
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          const double u = t - pc[4 * j + 0];
+          const double env = exp(pc[4 * j + 1] * u * u);
+          Mr += pc[4 * j + 2] * env;
+          Mi += pc[4 * j + 3] * env;
         }
-        Msh[lane] = make_double2(-w.mscale * er, -w.mscale * ei);
       }
-      named_sync(2, 32 * kEpiWarps);
       double pr[WH], pim[WH];
 #pragma unroll
       for (int j = 0; j < WH; ++j) pr[j] = pim[j] = 0.0;
@@ -633,96 +668,103 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
 #pragma unroll
       for (int c = 0; c < 4 * WH; ++c) cm[c] = 0.f;
       const double* fx = xfac + (s & 1) * N;
-      for (int mi = 0; mi < nM; ++mi) {
+      for (int mi = 0; mi < nM; ++mi, ++it) {
         const int k = mi * kTileRows + 32 * q + lane;
-        // exchange sums of this row for this warp's wires: slice blocks
-        // summed with round-to-nearest
-        float exs[4 * WH];
+        const int b = it & 1;
+        bool got = mbar_wait(&dfull[b], (it >> 1) & 1, abort);
+        got = __all_sync(0xffffffffu, got);
+        if (got) tc_fence_after();
+        const double ee = k < nk ? Ee[k] : 0.0, eh = k < nk ? Eh[k] : 0.0;
 #pragma unroll
-        for (int c = 0; c < 4 * WH; ++c) exs[c] = 0.f;
-        for (int kj = 0; kj < nK; ++kj, ++it) {
-          const int b = it & 1;
-          bool got = mbar_wait(&dfull[b], (it >> 1) & 1, abort);
-          got = __all_sync(0xffffffffu, got);
-          if (!got) break;
-          tc_fence_after();
-          const uint32_t dm = lrow + (uint32_t)(2 * N * b + 4 * w0);
-          uint32_t rm[4 * WH], rc[4 * WH];
-#pragma unroll
-          for (int c = 0; c < 4 * WH; c += 8) {
-            tmem_ld8(dm + c, rm + c);
-            tmem_ld8(dm + N + c, rc + c);
+        for (int jp = 0; jp < WH; jp += 2) {
+          // accumulators of wires w0+jp, w0+jp+1 (8 columns each)
+          uint32_t r2[8], r3[8], r4[8];
+          if (got) {
+            const uint32_t col = lrow + (uint32_t)(3 * N * b + 4 * (w0 + jp));
+            tmem_ld8(col, r2);
+            tmem_ld8(col + N, r3);
+            tmem_ld8(col + 2 * N, r4);
+            tmem_ld_wait();
           }
-          tmem_ld_wait();
-          tc_fence_before();
-          __syncwarp();
-          if (lane == 0) mbar_arrive(&dfree[b]);
 #pragma unroll
-          for (int c = 0; c < 4 * WH; ++c)
-            exs[c] += __uint_as_float(rm[c]) + __uint_as_float(rc[c]);
-        }
-        if (*abort || k >= nk) continue;
-        // ---- epilogue of this k tile ----
-        const double ee = Ee[k], eh = Eh[k];
+          for (int u = 0; u < 2; ++u) {
+            const int j = jp + u;
+            const int w = w0 + j;
+            const double Mjr = __shfl_sync(0xffffffffu, Mr, j);
+            const double Mji = __shfl_sync(0xffffffffu, Mi, j);
+            if (!got || k >= nk || w >= grp.nw || *abort) continue;
+            double exv[4];
 #pragma unroll
-        for (int j = 0; j < WH; ++j) {
-          const int w = w0 + j;
-          if (w >= grp.nw) break;
-          const int64_t eg = woff[w] + k;
-          const int es = w * kpad + k;
-          double4* yp = RES ? s_y + es : g_y + eg;
-          float4* ysp = ys_ptr(w, k);
-          float4* accp = RES ? s_acc + es : a.ws_acc + eg;
-          const double4 par = wpar[w];
-          const double2 M = Msh[w];
-          const float4 ysf = *ysp;
-          const double ys[4] = {ysf.x, ysf.y, ysf.z, ysf.w};
-          // exchange sums (SBEs.py:896-921) from the tensor cores, the
-          // diagonal RHS (SBEs.py:1962-1975, 2325-2337, 2623-2636) in fp64
-          const double omr = M.x + fx[4 * w + 0] * (double)exs[4 * j + 0];
-          const double omi = M.y + fx[4 * w + 1] * (double)exs[4 * j + 1];
-          const double se = (ee + par.x) - fx[4 * w + 2] * (double)exs[4 * j + 2];
-          const double sh = eh - fx[4 * w + 3] * (double)exs[4 * j + 3];
-          const double sum = se + sh;
-          const double nn = ys[2] + ys[3] - 1.0;
-          const double xr = sum * ys[0] - omr * nn;
-          const double xi = sum * ys[1] - omi * nn;
-          const double hg = par.y;  // gamma
-          double f[4];
-          f[0] = xi * inv_hbar - hg * ys[0];
-          f[1] = -xr * inv_hbar - hg * ys[1];
-          f[2] = 2.0 * (omi * ys[0] - omr * ys[1]) * inv_hbar;
-          f[3] = f[2];
-          // RK4 stage combination (integrator.py:143-157): acc = k1 + 2 k2
-          // + 2 k3 (FP32 store), y += h/6 (acc + k4) in FP64
-          const double4 yv = *yp;
-          const double yy[4] = {yv.x, yv.y, yv.z, yv.w};
-          double nxt[4];
-          if (stg == 0) {
-            *accp = make_float4((float)f[0], (float)f[1], (float)f[2], (float)f[3]);
+            for (int c = 0; c < 4; ++c) {
+              const int cc = 4 * u + c;
+              exv[c] = fx[4 * w + c] *
+                       ((double)(int)r2[cc] +
+                        ((double)(int)r3[cc] + (double)(int)r4[cc] * (1.0 / kBase)) *
+                            (1.0 / kBase));
+            }
+            const int64_t eg = woff[w] + k;
+            const int es = w * kpad + k;
+            double4* yp = RES ? s_y + es : g_y + eg;
+            float4* ysp = ys_ptr(w, k);
+            float4* accp = RES ? s_acc + es : a.ws_acc + eg;
+            const double4 par = wpar[w];
+            const float4 ysf = *ysp;
+            const double ys[4] = {ysf.x, ysf.y, ysf.z, ysf.w};
+            // exchange sums (SBEs.py:896-921) from the tensor cores, the
+            // diagonal RHS (SBEs.py:1962-1975, 2325-2337, 2623-2636) in fp64
+            const double omr = Mjr + exv[0];
+            const double omi = Mji + exv[1];
+            const double se = (ee + par.x) - exv[2];
+            const double sh = eh - exv[3];
+            const double sum = se + sh;
+            const double nn = ys[2] + ys[3] - 1.0;
+            const double xr = sum * ys[0] - omr * nn;
+            const double xi = sum * ys[1] - omi * nn;
+            const double hg = par.y;  // gamma
+            double f[4];
+            f[0] = xi * inv_hbar - hg * ys[0];
+            f[1] = -xr * inv_hbar - hg * ys[1];
+            f[2] = 2.0 * (omi * ys[0] - omr * ys[1]) * inv_hbar;
+            f[3] = f[2];
+            // RK4 stage combination (integrator.py:143-157): acc = k1 + 2 k2
+            // + 2 k3 (FP32 store), y += h/6 (acc + k4) in FP64
+            const double4 yv = *yp;
+            const double yy[4] = {yv.x, yv.y, yv.z, yv.w};
+            double nxt[4];
+            if (stg == 0) {
+              *accp = make_float4((float)f[0], (float)f[1], (float)f[2], (float)f[3]);
 #pragma unroll
-            for (int c = 0; c < 4; ++c) nxt[c] = yy[c] + (h / 2.0) * f[c];
-          } else if (stg == 3) {
-            const float4 af = *accp;
-            const double ac[4] = {af.x, af.y, af.z, af.w};
+              for (int c = 0; c < 4; ++c) nxt[c] = yy[c] + (h / 2.0) * f[c];
+            } else if (stg == 3) {
+              const float4 af = *accp;
+              const double ac[4] = {af.x, af.y, af.z, af.w};
 #pragma unroll
-            for (int c = 0; c < 4; ++c) nxt[c] = yy[c] + (h / 6.0) * (ac[c] + f[c]);
-            *yp = make_double4(nxt[0], nxt[1], nxt[2], nxt[3]);
-            pr[j] += nxt[0];
-            pim[j] += nxt[1];
-          } else {
-            const float4 af = *accp;
-            *accp = make_float4((float)((double)af.x + 2.0 * f[0]), (float)((double)af.y + 2.0 * f[1]),
-                                (float)((double)af.z + 2.0 * f[2]), (float)((double)af.w + 2.0 * f[3]));
-            const double c2 = stg == 1 ? h / 2.0 : h;
+              for (int c = 0; c < 4; ++c) nxt[c] = yy[c] + (h / 6.0) * (ac[c] + f[c]);
+              *yp = make_double4(nxt[0], nxt[1], nxt[2], nxt[3]);
+              pr[j] += nxt[0];
+              pim[j] += nxt[1];
+            } else {
+              const float4 af = *accp;
+              *accp = make_float4((float)((double)af.x + 2.0 * f[0]),
+                                  (float)((double)af.y + 2.0 * f[1]),
+                                  (float)((double)af.z + 2.0 * f[2]),
+                                  (float)((double)af.w + 2.0 * f[3]));
+              const double c2 = stg == 1 ? h / 2.0 : h;
 #pragma unroll
-            for (int c = 0; c < 4; ++c) nxt[c] = yy[c] + c2 * f[c];
+              for (int c = 0; c < 4; ++c) nxt[c] = yy[c] + c2 * f[c];
+            }
+            const float4 nf =
+                make_float4((float)nxt[0], (float)nxt[1], (float)nxt[2], (float)nxt[3]);
+            *ysp = nf;
+            track(cm, j, nf);
           }
-          const float4 nf = make_float4((float)nxt[0], (float)nxt[1], (float)nxt[2], (float)nxt[3]);
-          *ysp = nf;
-          track(cm, j, nf);
         }
+        // accumulators of this row tile are free again
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0 && got) mbar_arrive(&dfree[b]);
       }
+      publish_colmax(cm);
       if (stg == 3) {
         // P(t) = pscale * sum_k p_k, reduced in a fixed order
 #pragma unroll
@@ -739,42 +781,45 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
           }
         }
       }
-      if (F16) publish_colmax(cm);
-      named_sync(2, 32 * kEpiWarps);
-      // next stage's X from the stage points (after every column maximum
-      // is in)
+      named_sync(2, kEpiThreads);
+      // next stage's X from the stage points (every column maximum is in)
       if (!*abort) x_pass((s + 1) & 1);
-      if (stg == 3 && warp == 0 && lane < grp.nw) {
-        const int w = lane;
-        const int step = s >> 2;
-        wt[w] = wt[w] + h;
-        if (a.P && a.p_stride > 0 && (step + 1) % a.p_stride == 0) {
-          const int r = (step + 1) / a.p_stride - 1;
-          const PsbWire& wd = a.wires[grp.wire[w]];
-          if (r < a.p_cap && wd.p_off >= 0 && wd.p_off + r < a.n_P) {
-            double sr = 0.0, si = 0.0;
-            for (int qq = 0; qq < 4; ++qq) {
-              sr += ppart[(0 * 4 + qq) * W + w];
-              si += ppart[(1 * 4 + qq) * W + w];
+      if (stg == 3) {
+        if (q == 0 && lane < WH && w0 + lane < grp.nw) {
+          const int w = w0 + lane;
+          const int step = s >> 2;
+          if (a.P && a.p_stride > 0 && (step + 1) % a.p_stride == 0) {
+            const int r = (step + 1) / a.p_stride - 1;
+            const PsbWire& wd = a.wires[grp.wire[w]];
+            if (r < a.p_cap && wd.p_off >= 0 && wd.p_off + r < a.n_P) {
+              double sr = 0.0, si = 0.0;
+              for (int qq = 0; qq < 4; ++qq) {
+                sr += ppart[(0 * 4 + qq) * W + w];
+                si += ppart[(1 * 4 + qq) * W + w];
+              }
+              a.P[2 * (wd.p_off + r)] = wpar[w].w * sr;
+              a.P[2 * (wd.p_off + r) + 1] = wpar[w].w * si;
             }
-            a.P[2 * (wd.p_off + r)] = wpar[w].w * sr;
-            a.P[2 * (wd.p_off + r) + 1] = wpar[w].w * si;
           }
         }
+        tj = tj + h;
       }
       if (warp == 0 && lane == 0) snap[s & 1] = *abort;
-      named_sync(1, 32 * (kEpiWarps + 1));
+      named_sync(1, kEpiThreads + 32);
       if (snap[s & 1]) break;
     }
-    // resident state back to the caller's y
-    if (RES && !*abort) {
-      for (int mi = 0; mi < nM; ++mi) {
-        const int k = mi * kTileRows + 32 * q + lane;
-        if (k >= nk) continue;
-        for (int j = 0; j < WH; ++j) {
-          const int w = w0 + j;
-          if (w >= grp.nw) break;
-          g_y[woff[w] + k] = s_y[w * kpad + k];
+    if (!*abort) {
+      if (q == 0 && lane < WH) wt[w0 + lane] = tj;
+      // resident state back to the caller's y
+      if (RES) {
+        for (int mi = 0; mi < nM; ++mi) {
+          const int k = mi * kTileRows + 32 * q + lane;
+          if (k >= nk) continue;
+          for (int j = 0; j < WH; ++j) {
+            const int w = w0 + j;
+            if (w >= grp.nw) break;
+            g_y[woff[w] + k] = s_y[w * kpad + k];
+          }
         }
       }
     }
@@ -819,25 +864,25 @@ int max_nk() {
   return best;
 }
 
-template <int W, bool F16, bool RES>
+template <int W, bool RES>
 int launch_res(Args a, int nkmax, cudaStream_t s) {
   const uint32_t smem = Layout<W, RES>(nkmax).total;  // monotone in nk
   if (smem > kMaxDynSmem)
     return set_error(PSB_ERR_SIZE, "split form: nk %d does not fit a group of %d wires", nkmax,
                      W);
-  cudaError_t e = cudaFuncSetAttribute(split_rk4_kernel<W, F16, RES>,
+  cudaError_t e = cudaFuncSetAttribute(split_rk4_kernel<W, RES>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess)
     return set_error(PSB_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
   a.smem_bytes = smem;
-  split_rk4_kernel<W, F16, RES><<<a.ngroups, kThreadsS, smem, s>>>(a);
+  split_rk4_kernel<W, RES><<<a.ngroups, kThreadsS, smem, s>>>(a);
   return check_cuda("split_rk4_kernel");
 }
 
-template <int W, bool F16>
+template <int W>
 int launch(const Args& a, int nkmax, cudaStream_t s) {
-  if (nkmax <= max_nk<W, true>()) return launch_res<W, F16, true>(a, nkmax, s);
-  return launch_res<W, F16, false>(a, nkmax, s);
+  if (nkmax <= max_nk<W, true>()) return launch_res<W, true>(a, nkmax, s);
+  return launch_res<W, false>(a, nkmax, s);
 }
 
 }  // namespace split
@@ -876,17 +921,14 @@ extern "C" int psb_split_smem_bytes(int nk, int wgroup) {
 extern "C" int psb_rk4_split(const PsbTable* d_tables, int ntab, const double* d_tabdata,
                              int64_t n_tabdata, PsbWire* d_wires, int nw,
                              const PsbSplitGroup* d_groups, int ngroups, int wgroup, int nkmax,
-                             int limb, double* d_y, int64_t n_state, void* d_ws,
-                             int64_t n_ws_bytes, int nsteps, double dt, double* d_P,
-                             int64_t n_P, int p_stride, int p_cap, const PsbModel* model,
-                             void* stream) {
+                             double* d_y, int64_t n_state, void* d_ws, int64_t n_ws_bytes,
+                             int nsteps, double dt, double* d_P, int64_t n_P, int p_stride,
+                             int p_cap, const PsbModel* model, void* stream) {
   if (!d_tables || !d_tabdata || !d_wires || !d_groups || !d_y || !d_ws || !model || ntab <= 0 ||
       nw < 0 || ngroups < 0)
     return set_error(PSB_ERR_INVALID, "psb_rk4_split: null pointer or bad count");
   if (wgroup != 4 && wgroup != 8)
     return set_error(PSB_ERR_INVALID, "psb_rk4_split: wgroup must be 4 or 8");
-  if (limb != PSB_LIMB_BF16 && limb != PSB_LIMB_FP16)
-    return set_error(PSB_ERR_INVALID, "psb_rk4_split: limb must be PSB_LIMB_BF16 or _FP16");
   if (nkmax < 2 || nkmax > psb_split_max_nk(wgroup))
     return set_error(PSB_ERR_SIZE, "psb_rk4_split: nkmax %d too large for wgroup %d", nkmax,
                      wgroup);
@@ -918,7 +960,5 @@ extern "C" int psb_rk4_split(const PsbTable* d_tables, int ntab, const double* d
   a.p_cap = p_cap;
   a.hbar = model->hbar;
   cudaStream_t st = (cudaStream_t)stream;
-  if (limb == PSB_LIMB_FP16)
-    return wgroup == 8 ? split::launch<8, true>(a, nkmax, st) : split::launch<4, true>(a, nkmax, st);
-  return wgroup == 8 ? split::launch<8, false>(a, nkmax, st) : split::launch<4, false>(a, nkmax, st);
+  return wgroup == 8 ? split::launch<8>(a, nkmax, st) : split::launch<4>(a, nkmax, st);
 }

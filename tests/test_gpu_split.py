@@ -1,15 +1,10 @@
 """GPU parity of the split-precision tensor-core form (psb_rk4_split).
 
-Tolerance (16-bit hi+lo exchange products, each 64-wide slice of k'
-accumulated on the tensor cores and drained at once, FP64 right-hand side,
-FP32 stage point and RK accumulator, FP64 state), normwise relative error
-against the FP64 oracle / the reference goldens:
-  fp16 limbs (default): <= 1e-6 in P(t) (the target of the split form) and
-      <= 1e-5 in the final p_k, n_e,k, n_h,k;
-  bf16 limbs: the 16-bit representation of the Coulomb matrix leaves
-      ~1e-6 in P(t) on small grids, so <= 5e-6 in P(t) and <= 5e-5 in the
-      state.
-
+Tolerance (exchange sums as exact int8-digit products on the tensor cores,
+FP64 right-hand side, FP32 stage point and RK accumulator, FP64 state):
+normwise relative error <= 1e-6 in P(t) (the target of the split form) and
+<= 1e-5 in the final p_k, n_e,k, n_h,k against the FP64 oracle / the
+reference goldens.
 """
 
 import numpy as np
@@ -25,8 +20,6 @@ pytestmark = pytest.mark.gpu
 
 TOL = 1e-6
 TOL_STATE = 1e-5
-TOL_BF16 = 5e-6
-TOL_STATE_BF16 = 5e-5
 
 
 def test_split_small_single_wire(cuda):
@@ -45,13 +38,12 @@ def test_split_small_single_wire(cuda):
     assert relerr(y[:, 2], yo[:, 2]) < TOL_STATE
 
 
-@pytest.mark.parametrize("limb", ["bf16", "fp16"])
-def test_split_uneven_batch_vs_oracle(cuda, limb):
+def test_split_uneven_batch_vs_oracle(cuda):
     nks = [64, 512, 96, 128, 320, 64, 256, 480, 160, 1024, 64, 512, 128, 96, 1024, 256,
            64, 64, 64, 64, 64, 64, 64, 64, 64, 64, 64, 64, 64, 64, 64, 64, 64]
     grids, w = uneven_case(nks, seed=21, nsteps=300)
     n, dt = 300, 1e-15
-    b = WireBatch(grids, w, p_cap=n, form="split", limb=limb)
+    b = WireBatch(grids, w, p_cap=n, form="split")
     b.rk4(n, dt)
     st = b.wires()
     assert (st["status"] == 0).all(), st["status"]
@@ -64,9 +56,8 @@ def test_split_uneven_batch_vs_oracle(cuda, limb):
                         relerr(y[s, 0] + 1j * y[s, 1], yo[s, 0] + 1j * yo[s, 1]),
                         relerr(y[s, 2], yo[s, 2]), relerr(y[s, 3], yo[s, 3])])
     e = np.array(allerrs)
-    print(f"split {limb}: max P err {e[:, 0].max():.2e}, max state err {e[:, 1:].max():.2e}")
-    tol_p, tol_s = (TOL, TOL_STATE) if limb == "fp16" else (TOL_BF16, TOL_STATE_BF16)
-    assert e[:, 0].max() < tol_p and e[:, 1:].max() < tol_s, e
+    print(f"split: max P err {e[:, 0].max():.2e}, max state err {e[:, 1:].max():.2e}")
+    assert e[:, 0].max() < TOL and e[:, 1:].max() < TOL_STATE, e
 
 
 def test_split_full_config0_vs_reference(cuda):
