@@ -274,6 +274,38 @@ int psb_rk4_split(const PsbTable* d_tables, int ntab, const double* d_tabdata, i
                   int64_t n_ws_bytes, int nsteps, double dt, double* d_P, int64_t n_P,
                   int p_stride, int p_cap, const PsbModel* model, void* stream);
 
+/*
+ * psb_rk4_split without a caller workspace, for callers that cannot
+ * allocate device memory: code that runs where cudaMalloc is unavailable or
+ * forbidden (inside another framework's memory pool or allocator hooks, or a
+ * host that owns every allocation and hands this library only its inputs
+ * and outputs).  No counterpart in the reference (its step allocates
+ * through numpy); this is an addition of this library.
+ *
+ * The workspace lives in one static device array of
+ * PSB_SPLIT_NOALLOC_SCRATCH_BYTES bytes that every GPU loading the library
+ * holds until the process exits.  Limit: n_state <=
+ * PSB_SPLIT_NOALLOC_MAX_STATE elements; larger batches get PSB_ERR_SIZE
+ * (use psb_rk4_split with your own workspace).  Nothing is allocated:
+ * no cudaMalloc, cudaFree or allocating library call.
+ * - The first call on a device looks up the array's device address
+ *   (cudaGetSymbolAddress) with that device current; make that first call
+ *   before any stream capture.
+ * - All calls share the array, and it keeps what the last call wrote.  The
+ *   kernel writes every workspace element before reading it, so nothing
+ *   needs to start at zero.  Calls whose kernels overlap on the GPU (other
+ *   streams, other host threads) race on the array: serialize them.
+ * Other arguments and results as psb_rk4_split.
+ */
+#define PSB_SPLIT_NOALLOC_SCRATCH_BYTES (8 * 1024 * 1024)
+#define PSB_SPLIT_NOALLOC_MAX_STATE ((PSB_SPLIT_NOALLOC_SCRATCH_BYTES - 32) / 64)
+int psb_rk4_split_noalloc(const PsbTable* d_tables, int ntab, const double* d_tabdata,
+                          int64_t n_tabdata, PsbWire* d_wires, int nw,
+                          const PsbSplitGroup* d_groups, int ngroups, int wgroup, int nkmax,
+                          double* d_y, int64_t n_state, int nsteps, double dt, double* d_P,
+                          int64_t n_P, int p_stride, int p_cap, const PsbModel* model,
+                          void* stream);
+
 /* ---- measurement --------------------------------------------------------- */
 /*
  * FP64 FMA throughput of the current device: runs an in-register FMA loop

@@ -37,6 +37,8 @@ _SIGNATURES = {
     "psb_split_max_nk_resident": ([i32], i32),
     "psb_rk4_split": ([vp, i32, vp, i64, vp, i32, vp, i32, i32, i32, vp, i64, vp, i64, i32,
                        f64, vp, i64, i32, i32, vp, vp], i32),
+    "psb_rk4_split_noalloc": ([vp, i32, vp, i64, vp, i32, vp, i32, i32, i32, vp, i64, i32, f64,
+                               vp, i64, i32, i32, vp, vp], i32),
 }
 
 

@@ -58,6 +58,8 @@ WIRE_DTYPE = np.dtype(
 MODEL_DTYPE = np.dtype([("hbar", "<f8"), ("flags", "<i4"), ("reserved", "<i4")], align=True)
 
 PSB_SPLIT_WMAX = 16
+PSB_SPLIT_NOALLOC_SCRATCH_BYTES = 8 * 1024 * 1024
+PSB_SPLIT_NOALLOC_MAX_STATE = (PSB_SPLIT_NOALLOC_SCRATCH_BYTES - 32) // 64
 SPLIT_GROUP_DTYPE = np.dtype(
     [("table", "<i4"), ("nw", "<i4"), ("wire", "<i4", (PSB_SPLIT_WMAX,))], align=True)
 

@@ -962,3 +962,61 @@ extern "C" int psb_rk4_split(const PsbTable* d_tables, int ntab, const double* d
   cudaStream_t st = (cudaStream_t)stream;
   return wgroup == 8 ? split::launch<8>(a, nkmax, st) : split::launch<4>(a, nkmax, st);
 }
+
+// ---------------------------------------------------------------------------
+// psb_rk4_split without a caller workspace: the workspace is one file-scope
+// device array (held by every GPU that loads the library).  Host code only
+// sees a host-side stand-in under the array's name, so its device address
+// is looked up once per device with cudaGetSymbolAddress and cached.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace psb {
+namespace split {
+static __device__ __align__(256) uint8_t g_noalloc_ws[PSB_SPLIT_NOALLOC_SCRATCH_BYTES];
+constexpr int kMaxDevices = 64;
+static void* g_noalloc_ptr[kMaxDevices] = {};
+static std::mutex g_noalloc_mu;
+
+// Device address of g_noalloc_ws on the current device (set-up on first use).
+static int noalloc_scratch(void** out) {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess)
+    return set_error(PSB_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
+  if (dev < 0 || dev >= kMaxDevices)
+    return set_error(PSB_ERR_UNSUPPORTED, "device ordinal %d beyond %d", dev, kMaxDevices);
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_ws);
+    if (e != cudaSuccess || !p)
+      return set_error(PSB_ERR_CUDA, "cudaGetSymbolAddress(workspace): %s",
+                       cudaGetErrorString(e));
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return PSB_OK;
+}
+}  // namespace split
+}  // namespace psb
+
+extern "C" int psb_rk4_split_noalloc(const PsbTable* d_tables, int ntab, const double* d_tabdata,
+                                     int64_t n_tabdata, PsbWire* d_wires, int nw,
+                                     const PsbSplitGroup* d_groups, int ngroups, int wgroup,
+                                     int nkmax, double* d_y, int64_t n_state, int nsteps,
+                                     double dt, double* d_P, int64_t n_P, int p_stride,
+                                     int p_cap, const PsbModel* model, void* stream) {
+  if (n_state < 0) return set_error(PSB_ERR_INVALID, "psb_rk4_split_noalloc: n_state < 0");
+  if (n_state > PSB_SPLIT_NOALLOC_MAX_STATE)
+    return set_error(PSB_ERR_SIZE,
+                     "psb_rk4_split_noalloc: n_state %lld exceeds the built-in workspace "
+                     "(at most %lld elements); use psb_rk4_split with a caller workspace",
+                     (long long)n_state, (long long)PSB_SPLIT_NOALLOC_MAX_STATE);
+  void* ws = nullptr;
+  const int rc = split::noalloc_scratch(&ws);
+  if (rc != PSB_OK) return rc;
+  return psb_rk4_split(d_tables, ntab, d_tabdata, n_tabdata, d_wires, nw, d_groups, ngroups,
+                       wgroup, nkmax, d_y, n_state, ws, PSB_SPLIT_NOALLOC_SCRATCH_BYTES, nsteps,
+                       dt, d_P, n_P, p_stride, p_cap, model, stream);
+}
