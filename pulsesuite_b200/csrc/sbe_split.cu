@@ -16,19 +16,31 @@
 // are exact in int32 (|D| < 3 * 1024 * 127^2 < 2^31), so the tensor cores
 // add no rounding at all; the exchange sum is
 //     VS / (254^2 sc) * (D2 + D3/254 + D4/254^2)
-// in FP64.  The digits represent t and x' to 2^-24.6 of their scale (the
-// static part, from T, is ~5e-8 of a sum); the dropped products are below
-// that.  (FP32 accumulation of 16-bit limbs was measured to truncate every
-// K = 16 step with a bias of ~1e-7 of the sum, which compounds into the
-// phase of p.)  The right-hand side is FP64 (the band energies set the phase
-// of p), the stage point and the RK accumulator FP32 and the state y FP64.
+// (rounded once to FP32).  The digits represent t and x' to 2^-24.6 of
+// their scale (the static part, from T, is ~5e-8 of a sum); the dropped
+// products are below that.  (FP32 accumulation of 16-bit limbs was measured
+// to truncate every K = 16 step with a bias of ~1e-7 of the sum, which
+// compounds into the phase of p.)  The three digit products of one K step
+// are issued as three MMAs with the X digit planes stacked along N:
+// T1 [X1|X2|X3] -> (D2|D3|D4), T2 [X1|X2] -> (D3|D4), T3 X1 -> D4.
+//
+// Precision of the right-hand side.  The phase of p is set by the band
+// energies: (Se + Sh)/hbar * p and the dephasing gamma p are formed in FP64
+// (rounding a static energy to FP32 drifts the phase linearly in time).  The
+// Rabi frequency and the exchange terms are formed as Omega/hbar in FP32
+// (Omega itself, ~V p, leaves the FP32 range once p has dephased), the
+// stage point, the RK accumulator and an FP32 copy of y in FP32, the state y
+// and the P(t) sums in FP64.
 //
 // One CTA owns a group of W (4 or 8) wires for all `nsteps` RK4 steps,
 // 128-row tiles of k at a time:
 //   * X (the MMA B operand: three int8 digit planes, K-major, N = 4W
 //     columns) lives in shared memory, double buffered: stage s reads
-//     X[s & 1]; at the end of stage s the epilogue warps write X[(s+1) & 1]
-//     from the stage points;
+//     X[s & 1] while its epilogue writes the digits of the next stage point
+//     into X[(s+1) & 1], with each column's scale taken from the previous
+//     stage's column maximum and one bit of headroom; a column whose values
+//     outgrow that headroom is re-digitised with its exact scale at the end
+//     of the stage;
 //   * T is Toeplitz and never stored as a matrix: each 128 x 64 tile of the
 //     A operand (three digit planes) is generated straight into tensor
 //     memory by four generator warps from tables of digit quads
@@ -44,7 +56,8 @@
 //   * eight drain/epilogue warps read a finished tile's accumulators and
 //     evaluate the diagonal SBE right-hand side and the RK4 stage
 //     combination (stage order of libpulsesuite/integrator.py:143-157);
-//   * the per-element state (y FP64, stage point and accumulator FP32) stays
+//   * the per-element state (y FP64, FP32 copy of y, stage point and
+//     accumulator FP32) stays
 //     in shared memory for the whole call when it fits (psb_split_max_nk_
 //     resident), else in the caller's workspace.
 // Every mbarrier wait is bounded; on a timeout the CTA records
@@ -227,6 +240,7 @@ struct Args {
   int64_t n_state;
   float4* ws_ys;   // stage point per element (workspace layout)
   float4* ws_acc;  // RK accumulator per element (workspace layout)
+  float4* ws_yf;   // FP32 copy of y per element (workspace layout)
   int nsteps;
   double dt;
   double* P;
@@ -238,7 +252,8 @@ struct Args {
 };
 
 // Shared-memory layout of one CTA.  RES: the element state (y double4,
-// stage point float4, accumulator float4 per (wire, k)) is resident here.
+// stage point, accumulator and FP32 copy of y float4 per (wire, k)) is
+// resident here.
 template <int W, bool RES>
 struct Layout {
   static constexpr int N = 4 * W;
@@ -249,16 +264,17 @@ struct Layout {
     plane = (uint32_t)kpad * N;  // one digit plane of X
     xbuf = kDigits * plane;      // one stage buffer
     st = 2 * xbuf;
-    tab = st + (RES ? 64u * W * (uint32_t)kpad : 0u);
+    tab = st + (RES ? 80u * W * (uint32_t)kpad : 0u);
     ntab_words = kTileRows * nM + kpad;
     bars = tab + kDigits * 4 * (uint32_t)ntab_words;  // digit-quad tables
     bars = (bars + 15) & ~15u;
     misc = bars + 8 * 12;  // afull[2], afree[2], dfull[2], dfree[2], final
     // misc: tmem base (16 B), abort + snapshots (16 B), pulse constants
     // double[W][2][4], wire params double4[W], t double[W], off int64[W],
-    // P partials double[2][4][W], X column decode factors double[2][N],
-    // column maxima float[4][N]
-    total = misc + 32 + 368 * W;
+    // P partials double[2][4][W], X column decode factors float[2][N],
+    // column maxima float[4][N], column write scales float[N], column
+    // overflow flags int[2][N], gap/hbar double[W]
+    total = misc + 32 + 328 * W;
   }
 };
 
@@ -303,6 +319,7 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   double4* s_y = reinterpret_cast<double4*>(smem + L.st);
   float4* s_ys = reinterpret_cast<float4*>(smem + L.st + 32u * W * kpad);
   float4* s_acc = reinterpret_cast<float4*>(smem + L.st + 48u * W * kpad);
+  float4* s_yf = reinterpret_cast<float4*>(smem + L.st + 64u * W * kpad);
   uint32_t* tabq = reinterpret_cast<uint32_t*>(smem + L.tab);  // [digit][word]
   uint64_t* afull = reinterpret_cast<uint64_t*>(smem + L.bars);
   uint64_t* afree = afull + 2;
@@ -319,8 +336,12 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   double* wt = reinterpret_cast<double*>(smem + L.misc + 32 + 96 * W);
   int64_t* woff = reinterpret_cast<int64_t*>(smem + L.misc + 32 + 104 * W);
   double* ppart = reinterpret_cast<double*>(smem + L.misc + 32 + 112 * W);
-  double* xfac = reinterpret_cast<double*>(smem + L.misc + 32 + 176 * W);
-  float* colmax = reinterpret_cast<float*>(smem + L.misc + 32 + 240 * W);
+  float* xfach = reinterpret_cast<float*>(smem + L.misc + 32 + 176 * W);  // [2][N]
+  float* colmax = reinterpret_cast<float*>(smem + L.misc + 32 + 208 * W);  // [4][N]
+  float* scw = reinterpret_cast<float*>(smem + L.misc + 32 + 272 * W);     // [N]
+  int* ovf = reinterpret_cast<int*>(smem + L.misc + 32 + 288 * W);         // [2][N]
+  double* gaph = reinterpret_cast<double*>(smem + L.misc + 32 + 320 * W);  // [W]
+  const double inv_hbar = 1.0 / a.hbar;
   const uint32_t xsbo = (uint32_t)kpad * 8;
   const double* blk = a.tabdata + tb.off;
   const double* Ee = blk + 3 * nk;
@@ -356,6 +377,7 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
     if (tid < grp.nw) {
       const PsbWire& w = a.wires[grp.wire[tid]];
       wpar[tid] = make_double4(w.gap, w.gamma, w.mscale, w.pscale);
+      gaph[tid] = w.gap * inv_hbar;
       wt[tid] = w.t;
       woff[tid] = w.off;
       for (int j = 0; j < 2; ++j) {
@@ -372,6 +394,7 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
       }
     } else {
       wpar[tid] = make_double4(0.0, 0.0, 0.0, 0.0);
+      gaph[tid] = 0.0;
       wt[tid] = 0.0;
       woff[tid] = -1;
       for (int j = 0; j < 8; ++j) pc[j] = 0.0;
@@ -431,9 +454,6 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   const int hh = (warp >> 2) & 1;
   const int w0 = hh * WH;
   double4* g_y = reinterpret_cast<double4*>(a.y);
-  auto ys_ptr = [&](int w, int k) -> float4* {
-    return RES ? s_ys + (w * kpad + k) : a.ws_ys + (woff[w] + k);
-  };
   // Largest |value| of each of this warp's X columns, per lane quarter q.
   auto publish_colmax = [&](const float* cm) {
 #pragma unroll
@@ -450,67 +470,89 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
     cm[4 * j + 2] = fmaxf(cm[4 * j + 2], fabsf(v.z));
     cm[4 * j + 3] = fmaxf(cm[4 * j + 3], fabsf(v.w));
   };
-  // Column scale exponent: the power of two that puts the column's largest
-  // value in [1/4, 1/2).
-  auto col_exp = [&](int col) -> int {
-    const float m = fmaxf(fmaxf(colmax[col], colmax[N + col]),
-                          fmaxf(colmax[2 * N + col], colmax[3 * N + col]));
-    int sexp = 0;
-    if (m > 0.f && isfinite(m)) {
-      int e2;
-      frexpf(m, &e2);  // m < 2^e2
-      sexp = min(max(-1 - e2, -120), 120);
+  auto ws_ptrs = [&](int w, int k, float4*& ysp, float4*& accp, float4*& yfp) {
+    if (RES) {
+      const int es = w * kpad + k;
+      ysp = s_ys + es;
+      accp = s_acc + es;
+      yfp = s_yf + es;
+    } else {
+      const int64_t eg = woff[w] + k;
+      ysp = a.ws_ys + eg;
+      accp = a.ws_acc + eg;
+      yfp = a.ws_yf + eg;
     }
-    return sexp;
   };
-  // X[b] = digits(stage point * column scale), all elements of the group:
-  // one item = 4 consecutive k of one wire (a 32-bit word per variable and
-  // digit plane).  xfac[b] decodes the exchange sums.
-  auto x_pass = [&](int b) {
-    const int et = tid;  // 0 .. kEpiThreads-1
-    if (et < N) {
-      const int sexp = col_exp(et);
-      xfac[b * N + et] = ldexp(VS / (kBase * kBase), -sexp);
-    }
+  // Largest |value| of column col over the four lane quarters.
+  auto col_max = [&](int col) -> float {
+    return fmaxf(fmaxf(colmax[col], colmax[N + col]),
+                 fmaxf(colmax[2 * N + col], colmax[3 * N + col]));
+  };
+  // Exact column scale: the power of two that puts the column's largest
+  // value m in [1/4, 1/2).  Lagged scale (for values of the next stage,
+  // which may grow): m in [1/8, 1/4), and 1/4 for an all-zero column
+  // (|p| <= 1/2 and n <= 1 for any physical state).
+  auto sexp_exact = [](float m) -> int {
+    int e2 = 0;
+    if (!(m > 0.f) || !isfinite(m)) return 0;
+    frexpf(m, &e2);  // m < 2^e2
+    return min(max(-1 - e2, -120), 120);
+  };
+  auto sexp_lag = [](float m) -> int {
+    int e2 = 0;
+    if (!(m > 0.f) || !isfinite(m)) return -2;
+    frexpf(m, &e2);
+    return min(max(-2 - e2, -120), 120);
+  };
+  // Decode factor of a column digitised with scale 2^sexp: exchange sum / hbar
+  // = VS / (hbar 254^2) 2^-sexp (D2 + (D3 + D4/254)/254).
+  const double dec0 = VS * inv_hbar / (kBase * kBase);
+  // Digitise the stage points of X[b] column by column with the exact scale
+  // of each column: all columns (only_flagged false) or the columns whose
+  // lagged scale overflowed (ovf[b][col] set).  One item = 4 consecutive k
+  // of one column (a 32-bit word per digit plane).  Sets xfach[b][col].
+  auto x_pass = [&](int b, bool only_flagged) {
     const int nq = (nk + 3) >> 2;
     uint8_t* xb = xbase + b * L.xbuf;
-    for (int item = et; item < grp.nw * nq; item += kEpiThreads) {
-      const int w = item / nq;
-      const int k0 = (item - w * nq) * 4;
-      float sc[4];
-#pragma unroll
-      for (int v = 0; v < 4; ++v) sc[v] = ldexpf(1.f, col_exp(4 * w + v));
-      uint32_t word[4][kDigits];
-#pragma unroll
-      for (int v = 0; v < 4; ++v)
-#pragma unroll
-        for (int p = 0; p < kDigits; ++p) word[v][p] = 0u;
+    for (int item = tid; item < 4 * grp.nw * nq; item += kEpiThreads) {
+      const int col = item / nq;
+      const int k0 = (item - col * nq) * 4;
+      if (only_flagged && !ovf[b * N + col]) continue;
+      const int sexp = sexp_exact(col_max(col));
+      if (k0 == 0) xfach[b * N + col] = (float)ldexp(dec0, -sexp);
+      const float sc = ldexpf(1.f, sexp);
+      const int w = col >> 2, v = col & 3;
+      uint32_t word[kDigits] = {0u, 0u, 0u};
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
         if (k0 + u >= nk) break;
-        const float4 yv = *ys_ptr(w, k0 + u);
-        const float vv[4] = {yv.x, yv.y, yv.z, yv.w};
-#pragma unroll
-        for (int v = 0; v < 4; ++v) {
-          int d1, d2, d3;
-          digits3(vv[v] * sc[v], d1, d2, d3);
-          word[v][0] |= ((uint32_t)(d1 & 0xFF)) << (8 * u);
-          word[v][1] |= ((uint32_t)(d2 & 0xFF)) << (8 * u);
-          word[v][2] |= ((uint32_t)(d3 & 0xFF)) << (8 * u);
-        }
+        float4* ysp; float4* accp; float4* yfp;
+        ws_ptrs(w, k0 + u, ysp, accp, yfp);
+        const float4 yv = *ysp;
+        const float x = v == 0 ? yv.x : (v == 1 ? yv.y : (v == 2 ? yv.z : yv.w));
+        int d1, d2, d3;
+        digits3(x * sc, d1, d2, d3);
+        word[0] |= ((uint32_t)(d1 & 0xFF)) << (8 * u);
+        word[1] |= ((uint32_t)(d2 & 0xFF)) << (8 * u);
+        word[2] |= ((uint32_t)(d3 & 0xFF)) << (8 * u);
       }
+      const uint32_t o = x_off(k0, col, xsbo);
 #pragma unroll
-      for (int v = 0; v < 4; ++v) {
-        const uint32_t o = x_off(k0, 4 * w + v, xsbo);
-#pragma unroll
-        for (int p = 0; p < kDigits; ++p)
-          *reinterpret_cast<uint32_t*>(xb + p * L.plane + o) = word[v][p];
-      }
+      for (int p = 0; p < kDigits; ++p) *reinterpret_cast<uint32_t*>(xb + p * L.plane + o) = word[p];
     }
-    fence_async_smem();
+  };
+  // Lagged write scales for the next stage's digits (from this stage's column
+  // maxima) and their decode factors xfach[b]; run by threads < N.
+  auto set_write_scales = [&](int b) {
+    if (tid < N) {
+      const int sexp = sexp_lag(col_max(tid));
+      scw[tid] = ldexpf(1.f, sexp);
+      xfach[b * N + tid] = (float)ldexp(dec0, -sexp);
+    }
   };
 
-  // Stage-0 input: stage point = y, X[0] = digits(y).
+  // Stage-0 input: stage point = FP32 copy of y = y, X[0] = digits(y) with
+  // exact column scales, write scales of stage 0 from the same maxima.
   if (warp < kEpiWarps) {
     float cm0[4 * WH];
 #pragma unroll
@@ -525,20 +567,26 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
         const double4 yv = g_y[woff[w] + k];
         const float4 yf = make_float4((float)yv.x, (float)yv.y, (float)yv.z, (float)yv.w);
         if (RES) s_y[w * kpad + k] = yv;
-        *ys_ptr(w, k) = yf;
+        float4* ysp; float4* accp; float4* yfp;
+        ws_ptrs(w, k, ysp, accp, yfp);
+        *ysp = yf;
+        *yfp = yf;
         track(cm0, j, yf);
       }
     }
+    if (tid < 2 * N) ovf[tid] = 0;
     publish_colmax(cm0);
     named_sync(2, kEpiThreads);
-    x_pass(0);
+    x_pass(0, false);
+    set_write_scales(1);
+    fence_async_smem();
   }
   __syncthreads();
 
-  const uint32_t idesc = idesc_i8(N);
+  static_assert(3 * N <= 256, "stacked MMA width 3N must be <= 256");
+  const uint32_t idesc1 = idesc_i8(N), idesc2 = idesc_i8(2 * N), idesc3 = idesc_i8(3 * N);
   const int total_stages = a.nsteps * 4;
   const double h = a.dt;
-  const double inv_hbar = 1.0 / a.hbar;
 
   if (warp == kMmaWarp) {
     // ---- MMA issuer -----------------------------------------------------------
@@ -571,18 +619,14 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
 #pragma unroll
             for (int ks = 0; ks < kTileK / kKStep; ++ks) {
               const int k0 = kj * kTileK + ks * kKStep;
-              const uint32_t xo = x0 + (uint32_t)(k0 >> 4) * 128;
-              const uint64_t b1 = smem_desc(xo, 128, xsbo);
-              const uint64_t b2 = smem_desc(xo + L.plane, 128, xsbo);
-              const uint64_t b3 = smem_desc(xo + 2 * L.plane, 128, xsbo);
+              // the three digit planes of X are consecutive column blocks of
+              // one N' = 3N operand
+              const uint64_t bx = smem_desc(x0 + (uint32_t)(k0 >> 4) * 128, 128, xsbo);
               const uint32_t first = (kj | ks) != 0;
               const uint32_t ac = ks * (kKStep / 4);  // TMEM columns of this K step
-              umma_i8(d2, a1 + ac, b1, idesc, first);
-              umma_i8(d3, a1 + ac, b2, idesc, first);
-              umma_i8(d3, a2 + ac, b1, idesc, 1);
-              umma_i8(d4, a1 + ac, b3, idesc, first);
-              umma_i8(d4, a2 + ac, b2, idesc, 1);
-              umma_i8(d4, a3 + ac, b1, idesc, 1);
+              umma_i8(d2, a1 + ac, bx, idesc3, first);  // T1 [X1|X2|X3] -> D2|D3|D4
+              umma_i8(d3, a2 + ac, bx, idesc2, 1);      // T2 [X1|X2]    -> D3|D4
+              umma_i8(d4, a3 + ac, bx, idesc1, 1);      // T3 X1         -> D4
             }
             if (!persist) {
               umma_commit(&afree[slot]);  // A slot reusable once these finish
@@ -644,37 +688,45 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
     // ---- drain / epilogue warps -----------------------------------------------------
     uint32_t it = 0;
     const uint32_t lrow = tmem + ((uint32_t)(32 * q) << 16);
+    const float inv_base = 1.f / 254.f;
+    const float hf = (float)h, h2f = (float)(h / 2.0), h6f = (float)(h / 6.0);
     // lane j < WH keeps the time of wire w0 + j
     double tj = (lane < WH) ? wt[w0 + lane] : 0.0;
     for (int s = 0; s < total_stages; ++s) {
       const int stg = s & 3;
-      // drive of this stage: lane j < WH evaluates wire w0 + j
-      double Mr = 0.0, Mi = 0.0;
+      const int bn = (s + 1) & 1;  // X buffer this stage's epilogue writes
+      // drive of this stage as M/hbar: lane j < WH evaluates wire w0 + j
+      float Mr = 0.f, Mi = 0.f;
       if (lane < WH) {
         const double t = tj + (stg == 0 ? 0.0 : (stg == 3 ? h : h / 2.0));
         const double* pc = pulse + (w0 + lane) * 8;
+        double mr = 0.0, mim = 0.0;
 #pragma unroll
-        for (int j = 0; j < 2; ++j) {
-          const double u = t - pc[4 * j + 0];
-          const double env = exp(pc[4 * j + 1] * u * u);
-          Mr += pc[4 * j + 2] * env;
-          Mi += pc[4 * j + 3] * env;
+        for (int jj = 0; jj < 2; ++jj) {
+          const double u = t - pc[4 * jj + 0];
+          const double env = exp(pc[4 * jj + 1] * u * u);
+          mr += pc[4 * jj + 2] * env;
+          mim += pc[4 * jj + 3] * env;
         }
+        Mr = (float)(mr * inv_hbar);
+        Mi = (float)(mim * inv_hbar);
       }
       double pr[WH], pim[WH];
 #pragma unroll
-      for (int j = 0; j < WH; ++j) pr[j] = pim[j] = 0.0;
+      for (int jj = 0; jj < WH; ++jj) pr[jj] = pim[jj] = 0.0;
       float cm[4 * WH];
 #pragma unroll
       for (int c = 0; c < 4 * WH; ++c) cm[c] = 0.f;
-      const double* fx = xfac + (s & 1) * N;
+      const float* fx = xfach + (s & 1) * N;
+      uint8_t* xn = xbase + bn * L.xbuf;
+      int* ovn = ovf + bn * N;
       for (int mi = 0; mi < nM; ++mi, ++it) {
         const int k = mi * kTileRows + 32 * q + lane;
         const int b = it & 1;
         bool got = mbar_wait(&dfull[b], (it >> 1) & 1, abort);
         got = __all_sync(0xffffffffu, got);
         if (got) tc_fence_after();
-        const double ee = k < nk ? Ee[k] : 0.0, eh = k < nk ? Eh[k] : 0.0;
+        const double ekh = k < nk ? (Ee[k] + Eh[k]) * inv_hbar : 0.0;
 #pragma unroll
         for (int jp = 0; jp < WH; jp += 2) {
           // accumulators of wires w0+jp, w0+jp+1 (8 columns each)
@@ -690,73 +742,77 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
           for (int u = 0; u < 2; ++u) {
             const int j = jp + u;
             const int w = w0 + j;
-            const double Mjr = __shfl_sync(0xffffffffu, Mr, j);
-            const double Mji = __shfl_sync(0xffffffffu, Mi, j);
+            const float Mjr = __shfl_sync(0xffffffffu, Mr, j);
+            const float Mji = __shfl_sync(0xffffffffu, Mi, j);
             if (!got || k >= nk || w >= grp.nw || *abort) continue;
-            double exv[4];
+            // exchange sums / hbar (SBEs.py:896-921) from the exact digit
+            // products, rounded once to FP32
+            float exh[4];
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
               const int cc = 4 * u + c;
-              exv[c] = fx[4 * w + c] *
-                       ((double)(int)r2[cc] +
-                        ((double)(int)r3[cc] + (double)(int)r4[cc] * (1.0 / kBase)) *
-                            (1.0 / kBase));
+              const float e = (float)(int)r2[cc] +
+                              ((float)(int)r3[cc] + (float)(int)r4[cc] * inv_base) * inv_base;
+              exh[c] = e * fx[4 * w + c];
             }
-            const int64_t eg = woff[w] + k;
-            const int es = w * kpad + k;
-            double4* yp = RES ? s_y + es : g_y + eg;
-            float4* ysp = ys_ptr(w, k);
-            float4* accp = RES ? s_acc + es : a.ws_acc + eg;
-            const double4 par = wpar[w];
+            float4* ysp; float4* accp; float4* yfp;
+            ws_ptrs(w, k, ysp, accp, yfp);
             const float4 ysf = *ysp;
-            const double ys[4] = {ysf.x, ysf.y, ysf.z, ysf.w};
-            // exchange sums (SBEs.py:896-921) from the tensor cores, the
-            // diagonal RHS (SBEs.py:1962-1975, 2325-2337, 2623-2636) in fp64
-            const double omr = Mjr + exv[0];
-            const double omi = Mji + exv[1];
-            const double se = (ee + par.x) - exv[2];
-            const double sh = eh - exv[3];
-            const double sum = se + sh;
-            const double nn = ys[2] + ys[3] - 1.0;
-            const double xr = sum * ys[0] - omr * nn;
-            const double xi = sum * ys[1] - omi * nn;
-            const double hg = par.y;  // gamma
-            double f[4];
-            f[0] = xi * inv_hbar - hg * ys[0];
-            f[1] = -xr * inv_hbar - hg * ys[1];
-            f[2] = 2.0 * (omi * ys[0] - omr * ys[1]) * inv_hbar;
-            f[3] = f[2];
+            // diagonal RHS (SBEs.py:1962-1975, 2325-2337, 2623-2636) / hbar:
+            // phase and dephasing terms in FP64, Rabi terms in FP32
+            const float omr = Mjr + exh[0];
+            const float omi = Mji + exh[1];
+            const double sumh = (ekh + gaph[w]) - (double)(exh[2] + exh[3]);
+            const float nn = ysf.z + ysf.w - 1.f;
+            const double prd = ysf.x, pid = ysf.y;
+            const double gw = wpar[w].y;  // gamma
+            const float f0 = (float)(sumh * pid - gw * prd) - omi * nn;
+            const float f1 = (float)(-(sumh * prd) - gw * pid) + omr * nn;
+            const float f2 = 2.f * (omi * ysf.x - omr * ysf.y);
             // RK4 stage combination (integrator.py:143-157): acc = k1 + 2 k2
-            // + 2 k3 (FP32 store), y += h/6 (acc + k4) in FP64
-            const double4 yv = *yp;
-            const double yy[4] = {yv.x, yv.y, yv.z, yv.w};
-            double nxt[4];
+            // + 2 k3 and the stage points in FP32, y += h/6 (acc + k4) in FP64
+            float4 nxt;
             if (stg == 0) {
-              *accp = make_float4((float)f[0], (float)f[1], (float)f[2], (float)f[3]);
-#pragma unroll
-              for (int c = 0; c < 4; ++c) nxt[c] = yy[c] + (h / 2.0) * f[c];
+              *accp = make_float4(f0, f1, f2, f2);
+              // the stage-0 point is the FP32 copy of y
+              nxt = make_float4(ysf.x + h2f * f0, ysf.y + h2f * f1, ysf.z + h2f * f2,
+                                ysf.w + h2f * f2);
             } else if (stg == 3) {
               const float4 af = *accp;
-              const double ac[4] = {af.x, af.y, af.z, af.w};
-#pragma unroll
-              for (int c = 0; c < 4; ++c) nxt[c] = yy[c] + (h / 6.0) * (ac[c] + f[c]);
-              *yp = make_double4(nxt[0], nxt[1], nxt[2], nxt[3]);
-              pr[j] += nxt[0];
-              pim[j] += nxt[1];
+              double4* yp = RES ? s_y + (w * kpad + k) : g_y + (woff[w] + k);
+              double4 yv = *yp;
+              yv.x += (double)(h6f * (af.x + f0));
+              yv.y += (double)(h6f * (af.y + f1));
+              yv.z += (double)(h6f * (af.z + f2));
+              yv.w += (double)(h6f * (af.w + f2));
+              *yp = yv;
+              nxt = make_float4((float)yv.x, (float)yv.y, (float)yv.z, (float)yv.w);
+              *yfp = nxt;
+              pr[j] += yv.x;
+              pim[j] += yv.y;
             } else {
               const float4 af = *accp;
-              *accp = make_float4((float)((double)af.x + 2.0 * f[0]),
-                                  (float)((double)af.y + 2.0 * f[1]),
-                                  (float)((double)af.z + 2.0 * f[2]),
-                                  (float)((double)af.w + 2.0 * f[3]));
-              const double c2 = stg == 1 ? h / 2.0 : h;
-#pragma unroll
-              for (int c = 0; c < 4; ++c) nxt[c] = yy[c] + c2 * f[c];
+              *accp = make_float4(af.x + 2.f * f0, af.y + 2.f * f1, af.z + 2.f * f2,
+                                  af.w + 2.f * f2);
+              const float4 yf = *yfp;
+              const float c2 = stg == 1 ? h2f : hf;
+              nxt = make_float4(yf.x + c2 * f0, yf.y + c2 * f1, yf.z + c2 * f2, yf.w + c2 * f2);
             }
-            const float4 nf =
-                make_float4((float)nxt[0], (float)nxt[1], (float)nxt[2], (float)nxt[3]);
-            *ysp = nf;
-            track(cm, j, nf);
+            *ysp = nxt;
+            track(cm, j, nxt);
+            // digits of the next stage point with the lagged column scales
+            const float4 sc = *reinterpret_cast<const float4*>(scw + 4 * w);
+            const float xv[4] = {nxt.x * sc.x, nxt.y * sc.y, nxt.z * sc.z, nxt.w * sc.w};
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+              int d1, d2, d3;
+              digits3(xv[c], d1, d2, d3);
+              const uint32_t o = x_off(k, 4 * w + c, xsbo);
+              xn[o] = (uint8_t)d1;
+              xn[L.plane + o] = (uint8_t)d2;
+              xn[2 * L.plane + o] = (uint8_t)d3;
+              if (!(fabsf(xv[c]) < 0.5f)) ovn[4 * w + c] = 1;
+            }
           }
         }
         // accumulators of this row tile are free again
@@ -768,22 +824,28 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
       if (stg == 3) {
         // P(t) = pscale * sum_k p_k, reduced in a fixed order
 #pragma unroll
-        for (int j = 0; j < WH; ++j) {
-          double sr = pr[j], si = pim[j];
+        for (int jj = 0; jj < WH; ++jj) {
+          double sr = pr[jj], si = pim[jj];
 #pragma unroll
           for (int o = 16; o > 0; o >>= 1) {
             sr += __shfl_xor_sync(0xffffffffu, sr, o);
             si += __shfl_xor_sync(0xffffffffu, si, o);
           }
           if (lane == 0) {
-            ppart[(0 * 4 + q) * W + w0 + j] = sr;
-            ppart[(1 * 4 + q) * W + w0 + j] = si;
+            ppart[(0 * 4 + q) * W + w0 + jj] = sr;
+            ppart[(1 * 4 + q) * W + w0 + jj] = si;
           }
         }
       }
       named_sync(2, kEpiThreads);
-      // next stage's X from the stage points (every column maximum is in)
-      if (!*abort) x_pass((s + 1) & 1);
+      if (!*abort) {
+        // columns whose values outgrew the lagged scale: exact re-digitising
+        x_pass(bn, true);
+        // flags of X[s & 1] were consumed at the end of the previous stage
+        if (tid < N) ovf[(s & 1) * N + tid] = 0;
+        // write scales of the next stage (digits into X[s & 1])
+        set_write_scales(s & 1);
+      }
       if (stg == 3) {
         if (q == 0 && lane < WH && w0 + lane < grp.nw) {
           const int w = w0 + lane;
@@ -804,6 +866,8 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
         }
         tj = tj + h;
       }
+      // this thread's digit stores become visible to the tensor cores
+      fence_async_smem();
       if (warp == 0 && lane == 0) snap[s & 1] = *abort;
       named_sync(1, kEpiThreads + 32);
       if (snap[s & 1]) break;
@@ -952,6 +1016,7 @@ extern "C" int psb_rk4_split(const PsbTable* d_tables, int ntab, const double* d
   a.n_state = n_state;
   a.ws_ys = (float4*)d_ws;
   a.ws_acc = (float4*)((uint8_t*)d_ws + 16 * n_state);
+  a.ws_yf = (float4*)((uint8_t*)d_ws + 32 * n_state);
   a.nsteps = nsteps;
   a.dt = dt;
   a.P = d_P;
