@@ -113,11 +113,25 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait; false when the limit ran out (which also sets abort) or
-// another role aborted.
+// Non-blocking probe of a phase (no suspension of the waiting thread).
+__device__ __forceinline__ bool mbar_test_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded spin on a phase; false when the limit ran out (which also sets
+// abort) or another role aborted.  Spinning with test_wait rather than
+// suspending in try_wait keeps the hand-off latency between the MMA issuer,
+// the generators and the drain warps short.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort) {
   for (uint32_t i = 0; i < kSpinLimit; ++i) {
-    if (mbar_try_wait(bar, parity)) return true;
+    if (mbar_test_wait(bar, parity)) return true;
     if (*abort) return false;
   }
   *abort = 1;
@@ -174,15 +188,17 @@ __device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t* r) {
 
 // Three balanced base-254 digits of v, |v| < 1/2 (so |254 v| < 127): each
 // remainder is formed exactly with an FMA, every digit lies in [-127, 127].
+// (Values outside the range give meaningless digits; the callers detect
+// them and re-digitise the column with a wider scale.)
 __device__ __forceinline__ void digits3(float v, int& d1, int& d2, int& d3) {
   const float f1 = rintf(v * 254.f);
   const float r1 = fmaf(v, 254.f, -f1);
   const float f2 = rintf(r1 * 254.f);
   const float r2 = fmaf(r1, 254.f, -f2);
   const float f3 = rintf(r2 * 254.f);
-  d1 = max(-127, min(127, (int)f1));
-  d2 = max(-127, min(127, (int)f2));
-  d3 = max(-127, min(127, (int)f3));
+  d1 = (int)f1;
+  d2 = (int)f2;
+  d3 = (int)f3;
 }
 
 // Shared-memory matrix descriptor, no swizzle (canonical layout of 8-row x
@@ -215,12 +231,19 @@ __host__ __device__ inline int ntiles_of(int nk) {
 }
 // TMEM columns: two row-tile accumulator sets (D2, D3, D4: 3 N each), then
 // the A slots (3 digit planes): all distinct tiles when they fit
-// (persistent), else a double buffer.
+// (persistent), else a ring of streamed slots in the remaining columns (up
+// to kMaxSlots), deep enough that the generators run ahead of the MMA
+// completion latency.
+constexpr int kMaxSlots = 8;
 __host__ __device__ inline bool persistent_tiles(int nk, int n) {
   return 6 * n + kTileCols * ntiles_of(nk) <= kTmemCols;
 }
+__host__ __device__ inline int ring_slots(int n) {
+  const int r = (kTmemCols - 6 * n) / kTileCols;
+  return r < kMaxSlots ? r : kMaxSlots;
+}
 __host__ __device__ inline int tmem_cols(int nk, int n) {
-  const int slots = persistent_tiles(nk, n) ? ntiles_of(nk) : 2;
+  const int slots = persistent_tiles(nk, n) ? ntiles_of(nk) : ring_slots(n);
   const int need = 6 * n + kTileCols * slots;
   int c = 32;
   while (c < need) c <<= 1;
@@ -268,13 +291,13 @@ struct Layout {
     ntab_words = kTileRows * nM + kpad;
     bars = tab + kDigits * 4 * (uint32_t)ntab_words;  // digit-quad tables
     bars = (bars + 15) & ~15u;
-    misc = bars + 8 * 12;  // afull[2], afree[2], dfull[2], dfree[2], final
+    misc = bars + 8 * 24;  // afull[8], afree[8], dfull[2], dfree[2], final
     // misc: tmem base (16 B), abort + snapshots (16 B), pulse constants
     // double[W][2][4], wire params double4[W], t double[W], off int64[W],
     // P partials double[2][4][W], X column decode factors float[2][N],
     // column maxima float[4][N], column write scales float[N], column
     // overflow flags int[2][N], gap/hbar double[W]
-    total = misc + 32 + 328 * W;
+    total = misc + 32 + 328 * W + 16;  // + any-overflow flags int[2]
   }
 };
 
@@ -314,6 +337,7 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   const int nk = tb.nk, kpad = kpad_of(nk), nM = mtiles_of(nk), nK = kpad / kTileK;
   const Layout<W, RES> L(nk);
   const bool persist = persistent_tiles(nk, N);
+  const int nslot = ring_slots(N);  // streamed A slots
   const int ntile = ntiles_of(nk);
   uint8_t* xbase = smem;  // X[b] digit plane p at xbase + b xbuf + p plane
   double4* s_y = reinterpret_cast<double4*>(smem + L.st);
@@ -322,8 +346,8 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   float4* s_yf = reinterpret_cast<float4*>(smem + L.st + 64u * W * kpad);
   uint32_t* tabq = reinterpret_cast<uint32_t*>(smem + L.tab);  // [digit][word]
   uint64_t* afull = reinterpret_cast<uint64_t*>(smem + L.bars);
-  uint64_t* afree = afull + 2;
-  uint64_t* dfull = afree + 2;
+  uint64_t* afree = afull + kMaxSlots;
+  uint64_t* dfull = afree + kMaxSlots;
   uint64_t* dfree = dfull + 2;
   uint64_t* final_bar = dfree + 2;  // teardown: all MMAs of this CTA done
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + L.misc);
@@ -341,6 +365,7 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   float* scw = reinterpret_cast<float*>(smem + L.misc + 32 + 272 * W);     // [N]
   int* ovf = reinterpret_cast<int*>(smem + L.misc + 32 + 288 * W);         // [2][N]
   double* gaph = reinterpret_cast<double*>(smem + L.misc + 32 + 320 * W);  // [W]
+  volatile int* ovf_any = reinterpret_cast<volatile int*>(smem + L.misc + 32 + 328 * W);  // [2]
   const double inv_hbar = 1.0 / a.hbar;
   const uint32_t xsbo = (uint32_t)kpad * 8;
   const double* blk = a.tabdata + tb.off;
@@ -358,9 +383,11 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   for (uint32_t i = tid * 16; i < 2 * L.xbuf; i += kThreadsS * 16)
     *reinterpret_cast<uint4*>(xbase + i) = make_uint4(0, 0, 0, 0);
   if (tid == 0) {
-    for (int b = 0; b < 2; ++b) {
+    for (int b = 0; b < kMaxSlots; ++b) {
       mbar_init(&afull[b], kGenWarps);
       mbar_init(&afree[b], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
       mbar_init(&dfull[b], 1);
       mbar_init(&dfree[b], kEpiWarps);
     }
@@ -543,11 +570,12 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   };
   // Lagged write scales for the next stage's digits (from this stage's column
   // maxima) and their decode factors xfach[b]; run by threads < N.
+  const float dec0f = (float)dec0;
   auto set_write_scales = [&](int b) {
     if (tid < N) {
       const int sexp = sexp_lag(col_max(tid));
       scw[tid] = ldexpf(1.f, sexp);
-      xfach[b * N + tid] = (float)ldexp(dec0, -sexp);
+      xfach[b * N + tid] = ldexpf(dec0f, -sexp);
     }
   };
 
@@ -575,6 +603,7 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
       }
     }
     if (tid < 2 * N) ovf[tid] = 0;
+    if (tid < 2) ovf_any[tid] = 0;
     publish_colmax(cm0);
     named_sync(2, kEpiThreads);
     x_pass(0, false);
@@ -590,13 +619,19 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
 
   if (warp == kMmaWarp) {
     // ---- MMA issuer -----------------------------------------------------------
+    // One thread issues every MMA, so its own instruction latency bounds the
+    // issue rate of these narrow MMAs: descriptors and TMEM addresses are
+    // advanced incrementally, the streamed slot ring by counters.
     uint32_t it = 0;  // row tiles issued
-    uint32_t ct = 0;  // streamed A tiles consumed
+    int rs = 0;       // streamed slot of the next A tile
+    uint32_t rph = 0; // parity of that slot's current fill
     for (int s = 0; s < total_stages; ++s) {
       if (lane == 0 && !*abort) {
         if (s == 0 && persist) mbar_wait(&afull[0], 0, abort);
         tc_fence_after();
-        const uint32_t x0 = smem_u32(xbase + (s & 1) * L.xbuf);
+        // B descriptor of X[s & 1] at k' = 0; +32 per 64-wide slice, +16 per
+        // K step (start address in 16-byte units: 256 B per 32 k')
+        const uint64_t bdesc0 = smem_desc(smem_u32(xbase + (s & 1) * L.xbuf), 128, xsbo);
         for (int mi = 0; mi < nM && !*abort; ++mi, ++it) {
           const int b = it & 1;
           if (it >= 2 && !mbar_wait(&dfree[b], ((it >> 1) - 1) & 1, abort)) break;
@@ -604,35 +639,34 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
           const uint32_t d2 = tmem + (uint32_t)(3 * N * b);
           const uint32_t d3 = d2 + (uint32_t)N;
           const uint32_t d4 = d2 + (uint32_t)(2 * N);
-          for (int kj = 0; kj < nK; ++kj) {
-            int slot;
-            if (persist) {
-              slot = 2 * mi - kj + nK - 1;
-            } else {
-              slot = ct & 1;
-              if (!mbar_wait(&afull[slot], (ct >> 1) & 1, abort)) break;
-              tc_fence_after();
-            }
-            const uint32_t a1 = tmem + acol0 + (uint32_t)(slot * kTileCols);
-            const uint32_t a2 = a1 + kPlaneCols;
-            const uint32_t a3 = a2 + kPlaneCols;
-#pragma unroll
-            for (int ks = 0; ks < kTileK / kKStep; ++ks) {
-              const int k0 = kj * kTileK + ks * kKStep;
-              // the three digit planes of X are consecutive column blocks of
-              // one N' = 3N operand
-              const uint64_t bx = smem_desc(x0 + (uint32_t)(k0 >> 4) * 128, 128, xsbo);
-              const uint32_t first = (kj | ks) != 0;
-              const uint32_t ac = ks * (kKStep / 4);  // TMEM columns of this K step
-              umma_i8(d2, a1 + ac, bx, idesc3, first);  // T1 [X1|X2|X3] -> D2|D3|D4
-              umma_i8(d3, a2 + ac, bx, idesc2, 1);      // T2 [X1|X2]    -> D3|D4
-              umma_i8(d4, a3 + ac, bx, idesc1, 1);      // T3 X1         -> D4
-            }
+          // persistent slot of slice kj is 2 mi - kj + nK - 1
+          uint32_t apers = tmem + acol0 + (uint32_t)((2 * mi + nK - 1) * kTileCols);
+          uint64_t bd = bdesc0;
+          bool ok = true;
+          for (int kj = 0; kj < nK; ++kj, apers -= kTileCols, bd += 32) {
+            uint32_t a1 = apers;
             if (!persist) {
-              umma_commit(&afree[slot]);  // A slot reusable once these finish
-              ++ct;
+              if (!mbar_wait(&afull[rs], rph, abort)) { ok = false; break; }
+              tc_fence_after();
+              a1 = tmem + acol0 + (uint32_t)(rs * kTileCols);
+            }
+            // K step 0 of the slice (the first slice overwrites the tile's
+            // accumulators), then K step 1
+            umma_i8(d2, a1, bd, idesc3, kj != 0);        // T1 [X1|X2|X3] -> D2|D3|D4
+            umma_i8(d3, a1 + kPlaneCols, bd, idesc2, 1);     // T2 [X1|X2] -> D3|D4
+            umma_i8(d4, a1 + 2 * kPlaneCols, bd, idesc1, 1); // T3 X1 -> D4
+            umma_i8(d2, a1 + 8, bd + 16, idesc3, 1);
+            umma_i8(d3, a1 + kPlaneCols + 8, bd + 16, idesc2, 1);
+            umma_i8(d4, a1 + 2 * kPlaneCols + 8, bd + 16, idesc1, 1);
+            if (!persist) {
+              umma_commit(&afree[rs]);  // slot reusable once these finish
+              if (++rs == nslot) {
+                rs = 0;
+                rph ^= 1u;
+              }
             }
           }
+          if (!ok) break;
           umma_commit(&dfull[b]);  // the row tile is ready to drain
         }
       }
@@ -666,20 +700,26 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
       __syncwarp();
       if (lane == 0) mbar_arrive(&afull[0]);
     } else {
-      uint32_t ct = 0;
+      int gs = 0;           // slot of the next tile
+      uint32_t gph = 0;     // parity of that slot's current fill
+      bool first = true;    // first pass over the ring: no slot to wait for
       for (int s = 0; s < total_stages && !*abort; ++s) {
         for (int mi = 0; mi < nM && !*abort; ++mi) {
-          for (int kj = 0; kj < nK; ++kj, ++ct) {
-            const int b = ct & 1;
-            bool got = ct < 2 || mbar_wait(&afree[b], ((ct >> 1) - 1) & 1, abort);
+          for (int kj = 0; kj < nK; ++kj) {
+            bool got = first || mbar_wait(&afree[gs], gph ^ 1u, abort);
             got = __all_sync(0xffffffffu, got);
             if (!got) break;
             tc_fence_after();
-            gen_tile(2 * mi - kj, b);
+            gen_tile(2 * mi - kj, gs);
             asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
             tc_fence_before();
             __syncwarp();
-            if (lane == 0) mbar_arrive(&afull[b]);
+            if (lane == 0) mbar_arrive(&afull[gs]);
+            if (++gs == nslot) {
+              gs = 0;
+              gph ^= 1u;
+              first = false;
+            }
           }
         }
       }
@@ -727,6 +767,7 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
         got = __all_sync(0xffffffffu, got);
         if (got) tc_fence_after();
         const double ekh = k < nk ? (Ee[k] + Eh[k]) * inv_hbar : 0.0;
+        const uint32_t kofs = (uint32_t)(k >> 4) * 128 + (uint32_t)(k & 15);
 #pragma unroll
         for (int jp = 0; jp < WH; jp += 2) {
           // accumulators of wires w0+jp, w0+jp+1 (8 columns each)
@@ -803,15 +844,20 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
             // digits of the next stage point with the lagged column scales
             const float4 sc = *reinterpret_cast<const float4*>(scw + 4 * w);
             const float xv[4] = {nxt.x * sc.x, nxt.y * sc.y, nxt.z * sc.z, nxt.w * sc.w};
+            // x_off(k, 4w + c): columns 4w..4w+3 share a core matrix
+            const uint32_t obase = (uint32_t)(w >> 1) * xsbo + (uint32_t)(w & 1) * 64 + kofs;
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
               int d1, d2, d3;
               digits3(xv[c], d1, d2, d3);
-              const uint32_t o = x_off(k, 4 * w + c, xsbo);
+              const uint32_t o = obase + 16 * c;
               xn[o] = (uint8_t)d1;
               xn[L.plane + o] = (uint8_t)d2;
               xn[2 * L.plane + o] = (uint8_t)d3;
-              if (!(fabsf(xv[c]) < 0.5f)) ovn[4 * w + c] = 1;
+              if (!(fabsf(xv[c]) < 0.5f)) {
+                ovn[4 * w + c] = 1;
+                ovf_any[bn] = 1;
+              }
             }
           }
         }
@@ -840,9 +886,10 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
       named_sync(2, kEpiThreads);
       if (!*abort) {
         // columns whose values outgrew the lagged scale: exact re-digitising
-        x_pass(bn, true);
+        if (ovf_any[bn]) x_pass(bn, true);
         // flags of X[s & 1] were consumed at the end of the previous stage
         if (tid < N) ovf[(s & 1) * N + tid] = 0;
+        if (tid == 0) ovf_any[s & 1] = 0;
         // write scales of the next stage (digits into X[s & 1])
         set_write_scales(s & 1);
       }
