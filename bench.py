@@ -5,9 +5,14 @@
                     [--workload c1] [--chunk S]
 
 A bench step advances every wire of the workload by S time steps (one launch
-of the fused step kernel); the metric counts wire*k*steps, i.e.
-sum_w Nk_w * S per bench step.  Default workload: configuration 1 (1024
-wires, Nk ~ U[64,512] rounded to 32, RK4 with dt = 1 fs), plain FP64 form.
+of the fused step kernel per size class); the metric counts wire*k*steps,
+i.e. sum_w Nk_w * S per bench step.  Default workload: configuration 1 (1024
+wires, Nk ~ U[64,512] rounded to 32, RK4 with dt = 1 fs) in the batched
+split form (exchange sums as exact int8-digit products on the tensor cores,
+<= 1e-6 in P(t) against FP64); the plain FP64 form of the same workload is
+timed in the same run and reported beside it ("plain").  --workload c4 runs
+the continuous-batching server on the Poisson request stream of
+configuration 4 and reports p50/p99 solve latency with the throughput.
 
 Timing: W untimed bench steps, then K bench steps each bracketed by CUDA
 events on the launching stream, with a 256 MiB write between them (L2 is
@@ -32,6 +37,7 @@ REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
 L2_FLUSH_BYTES = 256 << 20
+METRIC = "SBE wire*k*steps/s at <=1e-6 rel err vs FP64 (batched vs plain); p50/p99 latency"
 
 
 def parse():
@@ -40,10 +46,16 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c1", choices=["c1", "c2", "c3"])
+    ap.add_argument("--workload", default="c1", choices=["c1", "c2", "c3", "c4"])
     ap.add_argument("--chunk", type=int, default=100, help="time steps per bench step")
-    ap.add_argument("--form", default="plain", choices=["plain", "split"],
-                    help="plain FP64 kernel or split hi+lo tensor-core kernel")
+    ap.add_argument("--form", default="split", choices=["plain", "split"],
+                    help="split int8-digit tensor-core kernel or plain FP64 kernel")
+    ap.add_argument("--no-plain", action="store_true",
+                    help="skip the plain-form comparison of the split run")
+    ap.add_argument("--rate", type=float, default=2000.0, help="c4: requests per second")
+    ap.add_argument("--serve-seconds", type=float, default=60.0, help="c4: stream length")
+    ap.add_argument("--capacity-requests", type=int, default=1500,
+                    help="c4: requests of the saturated capacity run of each form")
     ap.add_argument("--nwires", type=int, default=0, help="override the workload's wire count")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -53,6 +65,18 @@ def parse():
 def make_workload(name, rank, nwires):
     from pulsesuite_b200 import workloads
 
+    if name == "c4":
+        # the request mix of the serving stream as a fixed batch of wires
+        from pulsesuite_b200 import grid as pgrid
+        from pulsesuite_b200 import abi, serve
+
+        reqs = serve.poisson_stream(rate=2000.0, seconds=(nwires or 256) / 2000.0,
+                                    seed=4 + 1000 * rank)
+        grids = [pgrid.wire_grid(nk) for nk in serve.C4_NKS]
+        w = np.concatenate([serve.wire_record(r, grids[serve.C4_NKS.index(r.nk)],
+                                              table=serve.C4_NKS.index(r.nk)) for r in reqs])
+        assert w.dtype == abi.WIRE_DTYPE
+        return workloads.Workload(f"c4 request mix: {len(w)} wires", grids, w, 2500, 1e-15)
     kw = {"seed": 1 + 1000 * rank + {"c1": 0, "c2": 1, "c3": 2}[name]}
     if nwires:
         kw["nwires"] = nwires
@@ -194,6 +218,8 @@ def run_ours(a):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     wl = make_workload(a.workload, rank, a.nwires)
+    if wl.screened and a.form == "split":
+        a.form = "plain"  # the split form has no screened exchange
     S = a.chunk
     b = WireBatch(wl.grids, wl.wires, screened=wl.screened, p_cap=S, form=a.form)
     stream = torch.cuda.current_stream()
@@ -230,6 +256,30 @@ def run_ours(a):
         dist.barrier()
     value = units * a.steps * world / (total_ms * 1e-3)
     status = b.wires()["status"]
+    plain = None
+    if a.form == "split" and not a.no_plain:
+        # the plain FP64 form of the same workload, same timing rules
+        bp = WireBatch(wl.grids, wl.wires, screened=wl.screened, p_cap=S, form="plain")
+        for _ in range(a.warmup):
+            bp.rk4(S, wl.dt, stream=stream)
+        pev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(a.steps)]
+        torch.cuda.synchronize()
+        for i in range(a.steps):
+            flush.fill_(float(i))
+            pev[i][0].record(stream)
+            bp.rk4(S, wl.dt, p_stride=1, stream=stream)
+            pev[i][1].record(stream)
+        torch.cuda.synchronize()
+        pms = float(sum(e0.elapsed_time(e1) for e0, e1 in pev))
+        if world > 1:
+            t = torch.tensor([pms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            pms = float(t.item())
+        pval = units * a.steps * world / (pms * 1e-3)
+        plain = {"value": pval, "ms_per_step": pms / a.steps, "split_over_plain": value / pval,
+                 "gpu_launches": a.steps * bp.launches_per_call}
+        del bp
 
     # -- end to end through the public API: pinned host state in, P + state out
     y_host = torch.zeros((b.n_state, 4), dtype=torch.float64).pin_memory()
@@ -272,8 +322,7 @@ def run_ours(a):
     achieved = flops_launch / (avg_launch_ms * 1e-3) / 1e12
 
     line = {
-        "metric": ("SBE wire*k*steps/s (plain FP64 RK4)" if a.form == "plain" else
-                   "SBE wire*k*steps/s (split int8-digit tensor-core RK4)"),
+        "metric": METRIC,
         "value": value,
         "unit": "wire*k*steps/s",
         "n_gpus": world,
@@ -295,6 +344,7 @@ def run_ours(a):
                      "frac": achieved / peak, "traffic": None, "peak_source": peak_source,
                      "flops_per_launch": flops_launch},
         "gpu_launches": a.steps * b.launches_per_call,
+        "plain": plain,
         "clocks": clk.summary(),
         "wire_status_ok": bool((status == 0).all()),
     }
@@ -323,7 +373,7 @@ def run_reference(a):
     cb["value"] = v
     line = {
         "impl": "reference",
-        "metric": "SBE wire*k*steps/s (plain FP64 RK4)",
+        "metric": METRIC,
         "value": v,
         "unit": "wire*k*steps/s",
         "n_gpus": world,
@@ -344,10 +394,80 @@ def run_reference(a):
     print(json.dumps(line), flush=True)
 
 
+def run_serve(a):
+    """Configuration 4: the continuous-batching server on the Poisson stream
+    (split form), plus a saturated capacity run of both forms on the same
+    request mix."""
+    import torch
+
+    from pulsesuite_b200 import serve
+
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    torch.cuda.set_device(local)
+    chunk = 50
+    reqs = serve.poisson_stream(rate=a.rate, seconds=a.serve_seconds, seed=4 + 1000 * rank,
+                                chunk=chunk)
+    # warm-up: a few requests through each form
+    warm = serve.poisson_stream(rate=200.0, seconds=0.1, seed=99, chunk=chunk)
+    srv = serve.Server(form="split", chunk=chunk)
+    srv.run(warm, realtime=False)
+    with Clocks(local) as clk:
+        res = srv.run(reqs, realtime=True)
+    thr = srv.throughput()
+    lat = srv.latency_percentiles((50, 99))
+    ok = all(r.status == 0 for r in res)
+    # saturated capacity of both forms on the same mix (all requests queued)
+    cap = {}
+    sat = serve.poisson_stream(rate=1e6, seconds=a.capacity_requests / 1e6, seed=5, chunk=chunk)
+    for form in ("split", "plain"):
+        s2 = serve.Server(form=form, chunk=chunk)
+        s2.run(warm, realtime=False)
+        s2.run(sat, realtime=False)
+        cap[form] = s2.throughput()
+        del s2
+    h2d = 136 * len(res)
+    d2h = sum(16 * r.nsteps + 32 * r.nk for r in res)
+    line = {
+        "metric": METRIC,
+        "value": thr,
+        "unit": "wire*k*steps/s",
+        "n_gpus": world,
+        "steps": len(res),
+        "warmup": len(warm),
+        "ms_per_step": None,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "int8x3digits+s32acc+f64",
+        "data": "synthetic Poisson request stream (seeded)",
+        "config": {"workload": f"c4: Poisson {a.rate:g}/s for {a.serve_seconds:g} s, Nk in "
+                               "{64,128,256,512,1024} p={.3,.3,.2,.15,.05}, 1-4 ps at 1 fs, "
+                               "150 GB HBM budget", "requests": len(res), "tick_steps": chunk,
+                   "form": "split, continuous batching"},
+        "latency_p50_s": lat.get(50),
+        "latency_p99_s": lat.get(99),
+        "capacity": {"split": cap["split"], "plain": cap["plain"],
+                     "split_over_plain": cap["split"] / cap["plain"],
+                     "requests": len(sat)},
+        "e2e": {"value": thr, "unit": "wire*k*steps/s", "h2d_bytes_per_step": h2d / max(1, len(res)),
+                "d2h_bytes_per_step": d2h / max(1, len(res))},
+        "roofline": None,
+        "gpu_launches": None,
+        "clocks": clk.summary(),
+        "wire_status_ok": ok,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.workload == "c4":
+        run_serve(a)
     else:
         run_ours(a)
 
