@@ -188,6 +188,19 @@ int psb_rhs_f64(const PsbTable* d_tables, int ntab, const double* d_tabdata, int
                 const PsbWire* d_wires, int nw, const double* d_y, double* d_dy,
                 int64_t n_state, int nkmax, int tab_flags, const PsbModel* model, void* stream);
 /*
+ * Renormalised single-particle Hamiltonian diagonals of every wire (the
+ * diagonal of CalcH, SBEs.py:669-935 / _CalcH_jit SBEs.py:819-935, with the
+ * exchange sums over k' and, for screened tables, the per-call screening):
+ * d_h[e] = (Re Heh, Im Heh, Hee, Hhh) per element, where Heh = M(t_w) +
+ * sum_{q!=0} Veh(q) p_{k+q}, Hee = Ee + gap - sum Vee(q) n_e,k+q and
+ * Hhh = Eh - sum Vhh(q) n_h,k+q.  M(t_w) is the wire's drive at its own t
+ * (zero for npulse = 0).
+ */
+int psb_calch_f64(const PsbTable* d_tables, int ntab, const double* d_tabdata, int64_t n_tabdata,
+                  const PsbWire* d_wires, int nw, const double* d_y, double* d_h,
+                  int64_t n_state, int nkmax, int tab_flags, const PsbModel* model,
+                  void* stream);
+/*
  * nsteps classical RK4 steps of size dt on every wire, in the stage order of
  * the reference integrator (libpulsesuite/integrator.py:143-157, rk4_dpc),
  * the whole step fused in one kernel with the wire's state resident on chip.

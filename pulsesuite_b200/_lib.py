@@ -25,6 +25,7 @@ _SIGNATURES = {
     "psb_chi1d": ([vp, i32, f64, f64, f64, f64, vp, vp], i32),
     "psb_screen_f64": ([vp, i32, vp, vp, i32, vp, vp, i32, vp], i32),
     "psb_rhs_f64": ([vp, i32, vp, i64, vp, i32, vp, vp, i64, i32, i32, vp, vp], i32),
+    "psb_calch_f64": ([vp, i32, vp, i64, vp, i32, vp, vp, i64, i32, i32, vp, vp], i32),
     "psb_rk4_f64": ([vp, i32, vp, i64, vp, i32, vp, i32, vp, i64, i32, i32, i32, f64, vp, i64,
                      i32, i32, vp, vp], i32),
     "psb_leapfrog_f64": ([vp, i32, vp, i64, vp, i32, vp, i32, vp, vp, i64, i32, i32, vp, i64,

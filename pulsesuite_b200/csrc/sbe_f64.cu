@@ -28,7 +28,7 @@ namespace psb {
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 
-enum Mode { kRhs = 0, kRk4 = 1, kLeapfrog = 2 };
+enum Mode { kRhs = 0, kRk4 = 1, kLeapfrog = 2, kCalcH = 3 };
 
 struct Geo {
   int nk, nkp, nb, kc, chunk, yslen, doff, vlen, vphys;
@@ -353,7 +353,7 @@ __global__ void __launch_bounds__(kThreads, EPT <= 2 ? 2 : 1) sbe_f64_kernel(Bat
   if (exc && !scr) fill_tables<R, NT, false>(g, blk, vs, eps);
   __syncthreads();
 
-  const int nst = MODE == kRhs ? 1 : bt.nsteps;
+  const int nst = (MODE == kRhs || MODE == kCalcH) ? 1 : bt.nsteps;
   const int nstage = MODE == kRk4 ? 4 : 1;
   const double h = bt.dt;
   double t = w.t;
@@ -391,6 +391,24 @@ __global__ void __launch_bounds__(kThreads, EPT <= 2 ? 2 : 1) sbe_f64_kernel(Bat
         const int k = tid + e * kThreads;
         if (k >= g.nk) continue;
         double f[4];
+        if (MODE == kCalcH) {
+          // renormalised H diagonals (CalcH, SBEs.py:819-935): Heh (Rabi
+          // frequency), Hee, Hhh in the slots of dy
+          double omr = mr, omi = mi, xe = 0.0, xh = 0.0;
+          if (exc) {
+            for (int c = 0; c < g.kc; ++c) {
+              const double* rr = red + (size_t)c * 4 * g.nkp;
+              omr += rr[k];
+              omi += rr[g.nkp + k];
+              xe += rr[2 * g.nkp + k];
+              xh += rr[3 * g.nkp + k];
+            }
+          }
+          double2* d2 = reinterpret_cast<double2*>(bt.dy + 4 * w.off);
+          d2[2 * k] = make_double2(omr, omi);
+          d2[2 * k + 1] = make_double2((Ee[k] + w.gap) - xe, Eh[k] - xh);
+          continue;
+        }
         rhs_element(g, k, ys, red, Ee, Eh, w.gap, hg, hbar, mr, mi, exc, f);
         if (MODE == kRhs) {
           double2* d2 = reinterpret_cast<double2*>(bt.dy + 4 * w.off);
@@ -427,7 +445,7 @@ __global__ void __launch_bounds__(kThreads, EPT <= 2 ? 2 : 1) sbe_f64_kernel(Bat
       }
       __syncthreads();
     }
-    if (MODE == kRhs) break;
+    if (MODE == kRhs || MODE == kCalcH) break;
     if (MODE == kLeapfrog) {
       // Population neutrality and reshuffle (SBEs.py:5704-5718).
       double v[4] = {0.0, 0.0, 0.0, 0.0};
@@ -482,7 +500,7 @@ __global__ void __launch_bounds__(kThreads, EPT <= 2 ? 2 : 1) sbe_f64_kernel(Bat
       }
     }
   }
-  if (MODE == kRhs) return;
+  if (MODE == kRhs || MODE == kCalcH) return;
 
   // Write the state back; flag non-finite wires.
   bool bad = false;
@@ -569,6 +587,7 @@ int launch_sbe_f64(Batch bt, int mode, int n_order, int nkmax, int tab_flags, cu
   const int grid = bt.order ? n_order : bt.nw;
   if (grid <= 0) return PSB_OK;
   if (mode == kRhs) return launch_mode<kRhs>(bt, ept, grid, smem, screened, shared, st);
+  if (mode == kCalcH) return launch_mode<kCalcH>(bt, ept, grid, smem, screened, shared, st);
   if (mode == kRk4) return launch_mode<kRk4>(bt, ept, grid, smem, screened, shared, st);
   return launch_mode<kLeapfrog>(bt, ept, grid, smem, screened, shared, st);
 }
@@ -613,6 +632,28 @@ extern "C" int psb_rhs_f64(const PsbTable* d_tables, int ntab, const double* d_t
   bt.nsteps = 1;
   bt.hbar = model->hbar;
   return launch_sbe_f64(bt, kRhs, 0, nkmax, tab_flags, (cudaStream_t)stream);
+}
+
+extern "C" int psb_calch_f64(const PsbTable* d_tables, int ntab, const double* d_tabdata,
+                             int64_t n_tabdata, const PsbWire* d_wires, int nw, const double* d_y,
+                             double* d_h, int64_t n_state, int nkmax, int tab_flags,
+                             const PsbModel* model, void* stream) {
+  int rc = common_checks(d_tables, ntab, d_tabdata, d_wires, nw, d_y, model, nkmax);
+  if (rc) return rc;
+  if (!d_h) return set_error(PSB_ERR_INVALID, "d_h is null");
+  Batch bt{};
+  bt.tables = d_tables;
+  bt.ntab = ntab;
+  bt.tabdata = d_tabdata;
+  bt.n_tabdata = n_tabdata;
+  bt.wires = const_cast<PsbWire*>(d_wires);
+  bt.nw = nw;
+  bt.y = const_cast<double*>(d_y);
+  bt.dy = d_h;
+  bt.n_state = n_state;
+  bt.nsteps = 1;
+  bt.hbar = model->hbar;
+  return launch_sbe_f64(bt, kCalcH, 0, nkmax, tab_flags, (cudaStream_t)stream);
 }
 
 extern "C" int psb_rk4_f64(const PsbTable* d_tables, int ntab, const double* d_tabdata,
