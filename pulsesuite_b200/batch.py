@@ -25,11 +25,14 @@ class WireBatch:
     psb_rk4_split)."""
 
     def __init__(self, grids, wires, screened=False, excitons=True, p_cap=0, tables=None,
-                 tabdata=None, form="plain"):
+                 tabdata=None, form="plain", split_w=None):
         device.require_cuda()
         if form not in ("plain", "split"):
             raise ValueError("form must be 'plain' or 'split'")
         self.form = form
+        # split form: wires per CTA group by grid size, {nk: 4 or 8}; grids
+        # not listed use the built-in rule (see _setup_split)
+        self.split_w = dict(split_w or {})
         self.grids = list(grids)
         self.screened = bool(screened)
         if tables is None:
@@ -111,6 +114,10 @@ class WireBatch:
             wg = 4
             if nk <= resnk[8] and 8 * nk * nk <= max(target, 4 * nk * nk):
                 wg = 8
+            if nk in self.split_w:
+                wg = int(self.split_w[nk])
+                if wg not in (4, 8):
+                    raise ValueError("split_w values must be 4 or 8")
             if nk > maxnk[wg]:
                 raise _lib.PsbError(f"split form: nk {nk} exceeds the supported maximum")
             key = (wg, nk <= resnk[wg])

@@ -619,22 +619,33 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
 
   if (warp == kMmaWarp) {
     // ---- MMA issuer -----------------------------------------------------------
+    // The whole warp runs the issue loop (uniform control flow, every lane
+    // polls the barriers) and lane 0 alone issues the MMAs and commits.
     // One thread issues every MMA, so its own instruction latency bounds the
-    // issue rate of these narrow MMAs: descriptors and TMEM addresses are
-    // advanced incrementally, the streamed slot ring by counters.
+    // issue rate of these narrow MMAs: descriptors and TMEM addresses
+    // advance incrementally, the streamed slot ring by counters.
+    const bool issuer = lane == 0;
     uint32_t it = 0;  // row tiles issued
     int rs = 0;       // streamed slot of the next A tile
     uint32_t rph = 0; // parity of that slot's current fill
+    auto warp_wait = [&](uint64_t* bar, uint32_t parity) -> bool {
+      const bool got = mbar_wait(bar, parity, abort);
+      return __all_sync(0xffffffffu, got);
+    };
     for (int s = 0; s < total_stages; ++s) {
-      if (lane == 0 && !*abort) {
-        if (s == 0 && persist) mbar_wait(&afull[0], 0, abort);
+      const bool run = __all_sync(0xffffffffu, !*abort);
+      if (run) {
+        bool ok = !(s == 0 && persist) || warp_wait(&afull[0], 0);
         tc_fence_after();
         // B descriptor of X[s & 1] at k' = 0; +32 per 64-wide slice, +16 per
         // K step (start address in 16-byte units: 256 B per 32 k')
         const uint64_t bdesc0 = smem_desc(smem_u32(xbase + (s & 1) * L.xbuf), 128, xsbo);
-        for (int mi = 0; mi < nM && !*abort; ++mi, ++it) {
+        for (int mi = 0; ok && mi < nM; ++mi, ++it) {
           const int b = it & 1;
-          if (it >= 2 && !mbar_wait(&dfree[b], ((it >> 1) - 1) & 1, abort)) break;
+          if (it >= 2 && !warp_wait(&dfree[b], ((it >> 1) - 1) & 1)) {
+            ok = false;
+            break;
+          }
           tc_fence_after();
           const uint32_t d2 = tmem + (uint32_t)(3 * N * b);
           const uint32_t d3 = d2 + (uint32_t)N;
@@ -642,32 +653,36 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
           // persistent slot of slice kj is 2 mi - kj + nK - 1
           uint32_t apers = tmem + acol0 + (uint32_t)((2 * mi + nK - 1) * kTileCols);
           uint64_t bd = bdesc0;
-          bool ok = true;
           for (int kj = 0; kj < nK; ++kj, apers -= kTileCols, bd += 32) {
             uint32_t a1 = apers;
             if (!persist) {
-              if (!mbar_wait(&afull[rs], rph, abort)) { ok = false; break; }
+              if (!warp_wait(&afull[rs], rph)) {
+                ok = false;
+                break;
+              }
               tc_fence_after();
               a1 = tmem + acol0 + (uint32_t)(rs * kTileCols);
             }
-            // K step 0 of the slice (the first slice overwrites the tile's
-            // accumulators), then K step 1
-            umma_i8(d2, a1, bd, idesc3, kj != 0);        // T1 [X1|X2|X3] -> D2|D3|D4
-            umma_i8(d3, a1 + kPlaneCols, bd, idesc2, 1);     // T2 [X1|X2] -> D3|D4
-            umma_i8(d4, a1 + 2 * kPlaneCols, bd, idesc1, 1); // T3 X1 -> D4
-            umma_i8(d2, a1 + 8, bd + 16, idesc3, 1);
-            umma_i8(d3, a1 + kPlaneCols + 8, bd + 16, idesc2, 1);
-            umma_i8(d4, a1 + 2 * kPlaneCols + 8, bd + 16, idesc1, 1);
-            if (!persist) {
-              umma_commit(&afree[rs]);  // slot reusable once these finish
-              if (++rs == nslot) {
-                rs = 0;
-                rph ^= 1u;
-              }
+            if (issuer) {
+              // K step 0 of the slice (the first slice overwrites the tile's
+              // accumulators), then K step 1
+              umma_i8(d2, a1, bd, idesc3, kj != 0);            // T1 [X1|X2|X3] -> D2|D3|D4
+              umma_i8(d3, a1 + kPlaneCols, bd, idesc2, 1);     // T2 [X1|X2] -> D3|D4
+              umma_i8(d4, a1 + 2 * kPlaneCols, bd, idesc1, 1); // T3 X1 -> D4
+              umma_i8(d2, a1 + 8, bd + 16, idesc3, 1);
+              umma_i8(d3, a1 + kPlaneCols + 8, bd + 16, idesc2, 1);
+              umma_i8(d4, a1 + 2 * kPlaneCols + 8, bd + 16, idesc1, 1);
+              if (!persist) umma_commit(&afree[rs]);  // slot reusable once these finish
+            }
+            __syncwarp();
+            if (!persist && ++rs == nslot) {
+              rs = 0;
+              rph ^= 1u;
             }
           }
           if (!ok) break;
-          umma_commit(&dfull[b]);  // the row tile is ready to drain
+          if (issuer) umma_commit(&dfull[b]);  // the row tile is ready to drain
+          __syncwarp();
         }
       }
       __syncwarp();
