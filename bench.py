@@ -54,7 +54,7 @@ def parse():
                     help="skip the plain-form comparison of the split run")
     ap.add_argument("--rate", type=float, default=2000.0, help="c4: requests per second")
     ap.add_argument("--serve-seconds", type=float, default=60.0, help="c4: stream length")
-    ap.add_argument("--capacity-requests", type=int, default=1500,
+    ap.add_argument("--capacity-requests", type=int, default=6000,
                     help="c4: requests of the saturated capacity run of each form")
     ap.add_argument("--nwires", type=int, default=0, help="override the workload's wire count")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)

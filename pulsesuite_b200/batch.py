@@ -91,10 +91,11 @@ class WireBatch:
         A group holds up to W in {4, 8} wires of one grid.  The exchange work
         of a group per step is ~W Nk^2, so W is chosen per grid to give
         roughly two waves of equal CTAs over the SMs (W = 4 for large grids,
-        W = 8 once a grid has enough wires).  Groups are launched in classes
-        of (W, state resident in shared memory or not) so that a large grid
-        does not push the small ones out of the resident layout; the classes
-        run concurrently on side streams."""
+        W = 8 once a grid has enough wires: the MMAs are twice as wide at the
+        same issue cost).  Groups are launched in classes of (W, state
+        resident in shared memory or not) so that a large grid does not push
+        the small ones out of the resident layout; the classes run
+        concurrently on side streams, the one with the largest grid first."""
         need = abi.PSB_TAB_EXCITONS | abi.PSB_TAB_SHARED_V
         f = self.h_tables["flags"]
         if ((f & need) != need).any() or (f & abi.PSB_TAB_SCREENED).any():
@@ -112,7 +113,7 @@ class WireBatch:
             if counts[t] == 0:
                 continue
             wg = 4
-            if nk <= resnk[8] and 8 * nk * nk <= max(target, 4 * nk * nk):
+            if nk <= maxnk[8] and 8 * nk * nk <= max(target, 4 * nk * nk):
                 wg = 8
             if nk in self.split_w:
                 wg = int(self.split_w[nk])
@@ -130,10 +131,12 @@ class WireBatch:
                 g["wire"][0, :g["nw"][0]] = ws[i:i + wg]
                 classes.setdefault(key, []).append(g)
         self.split_launches = []
-        for key in sorted(classes, key=lambda kk: (-kk[0], not kk[1])):
+        for key in classes:
             ga = np.concatenate(classes[key])
             nkmax = int(nks[ga["table"]].max())
             self.split_launches.append((key[0], device.to_device(ga), len(ga), nkmax))
+        # the class with the largest grid first: its CTAs run longest
+        self.split_launches.sort(key=lambda l: -l[3])
         self.side_streams = [torch.cuda.Stream() for _ in self.split_launches[1:]]
         self.ws = torch.zeros(int(lib.psb_split_ws_bytes(self.n_state)), dtype=torch.uint8,
                               device="cuda")

@@ -231,9 +231,9 @@ __host__ __device__ inline int ntiles_of(int nk) {
 }
 // TMEM columns: two row-tile accumulator sets (D2, D3, D4: 3 N each), then
 // the A slots (3 digit planes): all distinct tiles when they fit
-// (persistent), else a ring of streamed slots in the remaining columns (up
-// to kMaxSlots), deep enough that the generators run ahead of the MMA
-// completion latency.
+// (persistent), else streamed slots in the remaining columns (up to
+// kMaxSlots), used as two buffers of nslot / 2 slots: the generators fill
+// one group while the MMAs read the other.
 constexpr int kMaxSlots = 8;
 __host__ __device__ inline bool persistent_tiles(int nk, int n) {
   return 6 * n + kTileCols * ntiles_of(nk) <= kTmemCols;
@@ -619,15 +619,19 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
 
   if (warp == kMmaWarp) {
     // ---- MMA issuer -----------------------------------------------------------
-    // The whole warp runs the issue loop (uniform control flow, every lane
-    // polls the barriers) and lane 0 alone issues the MMAs and commits.
-    // One thread issues every MMA, so its own instruction latency bounds the
-    // issue rate of these narrow MMAs: descriptors and TMEM addresses
-    // advance incrementally, the streamed slot ring by counters.
+    // The whole warp polls the barriers (uniform control flow) and lane 0
+    // alone issues the MMAs and commits.  One thread issues every MMA, and
+    // these narrow MMAs are short, so the issuing thread's own instructions
+    // between them set the rate: a barrier poll whose result it branches on
+    // stalls the issue for ~150-180 cycles (measured), about the time of
+    // three MMAs.  So the MMAs of a row tile (persistent A) or of a group of
+    // streamed slots go out in one unbroken sequence, with one poll before
+    // it; descriptors and TMEM addresses advance incrementally.
     const bool issuer = lane == 0;
     uint32_t it = 0;  // row tiles issued
-    int rs = 0;       // streamed slot of the next A tile
-    uint32_t rph = 0; // parity of that slot's current fill
+    int gb = 0;       // streamed group buffer of the next slices (two of G slots)
+    uint32_t gph = 0; // parity of that buffer's current fill
+    const int G = nslot / 2;
     auto warp_wait = [&](uint64_t* bar, uint32_t parity) -> bool {
       const bool got = mbar_wait(bar, parity, abort);
       return __all_sync(0xffffffffu, got);
@@ -650,36 +654,44 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
           const uint32_t d2 = tmem + (uint32_t)(3 * N * b);
           const uint32_t d3 = d2 + (uint32_t)N;
           const uint32_t d4 = d2 + (uint32_t)(2 * N);
-          // persistent slot of slice kj is 2 mi - kj + nK - 1
-          uint32_t apers = tmem + acol0 + (uint32_t)((2 * mi + nK - 1) * kTileCols);
+          // one 64-wide K slice: K step 0 (the tile's first slice overwrites
+          // its accumulators), then K step 1
+          auto slice = [&](uint32_t a1, uint64_t bd, bool acc) {
+            umma_i8(d2, a1, bd, idesc3, acc);                // T1 [X1|X2|X3] -> D2|D3|D4
+            umma_i8(d3, a1 + kPlaneCols, bd, idesc2, 1);     // T2 [X1|X2] -> D3|D4
+            umma_i8(d4, a1 + 2 * kPlaneCols, bd, idesc1, 1); // T3 X1 -> D4
+            umma_i8(d2, a1 + 8, bd + 16, idesc3, 1);
+            umma_i8(d3, a1 + kPlaneCols + 8, bd + 16, idesc2, 1);
+            umma_i8(d4, a1 + 2 * kPlaneCols + 8, bd + 16, idesc1, 1);
+          };
           uint64_t bd = bdesc0;
-          for (int kj = 0; kj < nK; ++kj, apers -= kTileCols, bd += 32) {
-            uint32_t a1 = apers;
-            if (!persist) {
-              if (!warp_wait(&afull[rs], rph)) {
+          if (persist) {
+            // persistent slot of slice kj is 2 mi - kj + nK - 1
+            if (issuer) {
+              uint32_t a1 = tmem + acol0 + (uint32_t)((2 * mi + nK - 1) * kTileCols);
+              for (int kj = 0; kj < nK; ++kj, a1 -= kTileCols, bd += 32) slice(a1, bd, kj != 0);
+            }
+          } else {
+            // streamed: slices k0 .. k0 + gn - 1 sit in slots gb G .. gb G + gn - 1
+            for (int k0 = 0; k0 < nK; k0 += G) {
+              const int gn = min(G, nK - k0);
+              if (!warp_wait(&afull[gb], gph)) {
                 ok = false;
                 break;
               }
               tc_fence_after();
-              a1 = tmem + acol0 + (uint32_t)(rs * kTileCols);
-            }
-            if (issuer) {
-              // K step 0 of the slice (the first slice overwrites the tile's
-              // accumulators), then K step 1
-              umma_i8(d2, a1, bd, idesc3, kj != 0);            // T1 [X1|X2|X3] -> D2|D3|D4
-              umma_i8(d3, a1 + kPlaneCols, bd, idesc2, 1);     // T2 [X1|X2] -> D3|D4
-              umma_i8(d4, a1 + 2 * kPlaneCols, bd, idesc1, 1); // T3 X1 -> D4
-              umma_i8(d2, a1 + 8, bd + 16, idesc3, 1);
-              umma_i8(d3, a1 + kPlaneCols + 8, bd + 16, idesc2, 1);
-              umma_i8(d4, a1 + 2 * kPlaneCols + 8, bd + 16, idesc1, 1);
-              if (!persist) umma_commit(&afree[rs]);  // slot reusable once these finish
-            }
-            __syncwarp();
-            if (!persist && ++rs == nslot) {
-              rs = 0;
-              rph ^= 1u;
+              if (issuer) {
+                uint32_t a1 = tmem + acol0 + (uint32_t)(gb * G * kTileCols);
+                for (int j = 0; j < gn; ++j, a1 += kTileCols, bd += 32) slice(a1, bd, k0 + j != 0);
+                umma_commit(&afree[gb]);  // the group's slots are reusable once these finish
+              }
+              if (++gb == 2) {
+                gb = 0;
+                gph ^= 1u;
+              }
             }
           }
+          __syncwarp();
           if (!ok) break;
           if (issuer) umma_commit(&dfull[b]);  // the row tile is ready to drain
           __syncwarp();
@@ -715,23 +727,27 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
       __syncwarp();
       if (lane == 0) mbar_arrive(&afull[0]);
     } else {
-      int gs = 0;           // slot of the next tile
-      uint32_t gph = 0;     // parity of that slot's current fill
-      bool first = true;    // first pass over the ring: no slot to wait for
+      // the issuer's group sequence: per row tile, slices in groups of at
+      // most G, alternating between two buffers of G slots
+      const int G = nslot / 2;
+      int gb = 0;           // group buffer of the next group
+      uint32_t gph = 0;     // parity of that buffer's current fill
+      bool first = true;    // first pass over both buffers: nothing to wait for
       for (int s = 0; s < total_stages && !*abort; ++s) {
         for (int mi = 0; mi < nM && !*abort; ++mi) {
-          for (int kj = 0; kj < nK; ++kj) {
-            bool got = first || mbar_wait(&afree[gs], gph ^ 1u, abort);
+          for (int k0 = 0; k0 < nK; k0 += G) {
+            const int gn = min(G, nK - k0);
+            bool got = first || mbar_wait(&afree[gb], gph ^ 1u, abort);
             got = __all_sync(0xffffffffu, got);
             if (!got) break;
             tc_fence_after();
-            gen_tile(2 * mi - kj, gs);
+            for (int j = 0; j < gn; ++j) gen_tile(2 * mi - (k0 + j), gb * G + j);
             asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
             tc_fence_before();
             __syncwarp();
-            if (lane == 0) mbar_arrive(&afull[gs]);
-            if (++gs == nslot) {
-              gs = 0;
+            if (lane == 0) mbar_arrive(&afull[gb]);
+            if (++gb == 2) {
+              gb = 0;
               gph ^= 1u;
               first = false;
             }

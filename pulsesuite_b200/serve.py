@@ -180,8 +180,9 @@ class Server:
         if form == "split":
             self.ws = torch.empty(int(lib.psb_split_ws_bytes(self.n_state)), dtype=torch.uint8,
                                   device="cuda")
-            self.wg = {nk: (8 if nk <= int(lib.psb_split_max_nk_resident(8)) else 4)
-                       for nk in self.nks}
+            # 8 wires per CTA wherever that group fits (twice the MMA width
+            # at the same issue cost), else 4
+            self.wg = {nk: (8 if nk <= int(lib.psb_split_max_nk(8)) else 4) for nk in self.nks}
         self.model = abi.model_array(hbar)
         self.streams = [torch.cuda.Stream() for _ in self.nks]
         self.copy_stream = torch.cuda.Stream()
@@ -299,7 +300,9 @@ class Server:
             self._fin = None
         tables = self.h_wires["table"][slots]
         plan = []
-        for ti, nk in enumerate(self.nks):
+        # largest grids first: their CTAs run longest, so they start before
+        # the short ones fill the SMs
+        for ti, nk in sorted(enumerate(self.nks), key=lambda t: -t[1]):
             sel = slots[tables == ti]
             if sel.size == 0:
                 continue
