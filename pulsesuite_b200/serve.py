@@ -36,6 +36,51 @@ EV = 1.602176634e-19
 C4_NKS = (64, 128, 256, 512, 1024)
 C4_PROBS = (0.3, 0.3, 0.2, 0.15, 0.05)
 
+# Cost model of the split-form scheduler: time of one CTA for one 50-step
+# launch (ms, one CTA per SM, full waves), measured on a B200, by grid size
+# and wires per CTA.  8 wires double the width of every MMA at the same
+# issue count, so a CTA of 8 takes only 1.2-1.6x as long as a CTA of 4:
+# more throughput, more latency.  Other grid sizes scale from the nearest
+# entry by Nk^2 (the exchange work per wire).
+SPLIT_CTA_MS = {(64, 4): 0.49, (64, 8): 0.73, (128, 4): 0.58, (128, 8): 0.84,
+                (256, 4): 0.90, (256, 8): 1.37, (512, 4): 2.53, (512, 8): 3.96,
+                (1024, 4): 8.15, (1024, 8): 9.71}
+
+
+def split_cta_cost(nk, w):
+    ref = min((k for k, ww in SPLIT_CTA_MS if ww == w), key=lambda k: abs(math.log(k / nk)))
+    return SPLIT_CTA_MS[(ref, w)] * (nk / ref) ** 2
+
+
+def choose_wires_per_cta(counts, sms, w8_ok=lambda nk: True):
+    """Wires per CTA (4 or 8) of each grid size for one tick.
+
+    counts: {nk: solves of that size in the tick}.  A tick lasts about
+    max(longest CTA, total CTA time / SMs): with few solves the longest CTA
+    sets it and 4 wires per CTA give the shorter tick (lower latency); once
+    the SMs are full the total sets it and 8 wires per CTA give more
+    throughput.  Starting from 4 everywhere, each size (largest first)
+    moves to 8 if that shortens the estimated tick, or keeps it and frees
+    SM time."""
+    w = {nk: 4 for nk, c in counts.items() if c}
+
+    def tick(wm):
+        total = sum(-(-counts[nk] // wm[nk]) * split_cta_cost(nk, wm[nk]) for nk in wm)
+        return (max(max(split_cta_cost(nk, wm[nk]) for nk in wm), total / sms), total)
+
+    if not w:
+        return w
+    best = tick(w)
+    for nk in sorted(w, reverse=True):
+        if not w8_ok(nk):
+            continue
+        trial = dict(w)
+        trial[nk] = 8
+        t = tick(trial)
+        if t < best:
+            w, best = trial, t
+    return w
+
 
 @dataclass
 class SolveRequest:
@@ -180,9 +225,10 @@ class Server:
         if form == "split":
             self.ws = torch.empty(int(lib.psb_split_ws_bytes(self.n_state)), dtype=torch.uint8,
                                   device="cuda")
-            # 8 wires per CTA wherever that group fits (twice the MMA width
-            # at the same issue cost), else 4
-            self.wg = {nk: (8 if nk <= int(lib.psb_split_max_nk(8)) else 4) for nk in self.nks}
+            # wires per CTA are chosen per tick (choose_wires_per_cta); 8
+            # only where that group fits in shared memory
+            self.w8_max = int(lib.psb_split_max_nk(8))
+            self.sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
         self.model = abi.model_array(hbar)
         self.streams = [torch.cuda.Stream() for _ in self.nks]
         self.copy_stream = torch.cuda.Stream()
@@ -299,6 +345,9 @@ class Server:
         else:
             self._fin = None
         tables = self.h_wires["table"][slots]
+        if self.form == "split":
+            counts = {nk: int((tables == ti).sum()) for ti, nk in enumerate(self.nks)}
+            self.wg = choose_wires_per_cta(counts, self.sms, lambda nk: nk <= self.w8_max)
         plan = []
         # largest grids first: their CTAs run longest, so they start before
         # the short ones fill the SMs

@@ -38,3 +38,22 @@ def test_slot_pool_budget_and_reuse():
 def test_request_bytes():
     assert serve.request_bytes(256, 1000, "plain") == 32 * 256 + 16 * 1000
     assert serve.request_bytes(256, 1000, "split") == 96 * 256 + 16 * 1000
+
+
+def test_wires_per_cta_choice():
+    # few solves: the longest CTA sets the tick, 4 wires per CTA keep it short
+    assert serve.choose_wires_per_cta({1024: 10}, 148) == {1024: 4}
+    # saturated: the total CTA time sets the tick, 8 wires per CTA lower it
+    assert serve.choose_wires_per_cta({1024: 2000}, 148) == {1024: 8}
+    sat = {64: 1800, 128: 1800, 256: 1200, 512: 900, 1024: 300}
+    assert set(serve.choose_wires_per_cta(sat, 148).values()) == {8}
+    # a Poisson-load mix: the largest grid keeps 4 (its CTA is the tick),
+    # smaller grids take 8 where that frees SM time without lengthening it
+    mix = {64: 300, 128: 300, 256: 200, 512: 150, 1024: 50}
+    w = serve.choose_wires_per_cta(mix, 148)
+    assert w[1024] == 4 and w[64] == 8
+    # sizes where 8 wires do not fit stay at 4; empty sizes are left out
+    assert serve.choose_wires_per_cta({1024: 2000, 64: 0}, 148, lambda nk: nk < 1024) == {1024: 4}
+    assert serve.choose_wires_per_cta({}, 148) == {}
+    # the cost model scales unlisted sizes by Nk^2 from the nearest entry
+    assert abs(serve.split_cta_cost(2048, 4) - 4 * serve.SPLIT_CTA_MS[(1024, 4)]) < 1e-12
