@@ -2,13 +2,16 @@
 
 Requests are single-wire SBE solves (own Nk, pulse, dephasing and
 duration) arriving over time.  The server keeps every admitted solve's state
-resident on the device in a slot pool, and each tick advances all resident
-solves by ``chunk`` RK4 steps with one launch per size class of the fused
-step kernel (split int8-digit tensor-core form or plain FP64 form).
-Between ticks it retires finished solves (their P(t) records and final
-state are copied to pinned host memory asynchronously) and admits waiting
-requests as slots and the HBM budget free up, so new work joins the
-running batch without waiting for the batch to drain.
+resident on the device in a slot pool.  Each size class (Nk) is a lane
+with its own CUDA stream: a tick of a lane advances all of that class's
+resident solves by ``chunk`` RK4 steps with one launch of the fused step
+kernel (split int8-digit tensor-core form or plain FP64 form), retires the
+solves that finish (their P(t) records and final state are copied to
+pinned host memory asynchronously) and admits waiting requests of the class
+as slots and the HBM budget free up, so new work joins the running batch
+without waiting for it to drain.  The lanes tick independently and their
+launches run concurrently, so a small solve is not held to the pace of the
+largest grid.
 
     srv = Server(form="split")
     results = srv.run(stream_of_requests)      # list of Result
@@ -230,22 +233,37 @@ class Server:
             self.w8_max = int(lib.psb_split_max_nk(8))
             self.sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
         self.model = abi.model_array(hbar)
-        self.streams = [torch.cuda.Stream() for _ in self.nks]
         self.copy_stream = torch.cuda.Stream()
         self.isz = abi.WIRE_DTYPE.itemsize
         self._wires_rows = self.d_wires.view(self.nslots, self.isz)
-        # per-tick metadata goes through a ring of pinned staging buffers and
-        # one asynchronous copy per tick (the ring depth exceeds the number
-        # of ticks allowed in flight, so a buffer is never rewritten while
-        # its copy may still be pending)
+        # one lane per size class: its own stream, its own ticks, its own
+        # queue and pinned staging ring (per-tick metadata goes through one
+        # asynchronous copy; the ring is deeper than the ticks allowed in
+        # flight, so a buffer is never rewritten while its copy may pend)
         self.ring = 3
-        nb = max(1 << 20, 64 * self.nslots + 8 * self.nslots * abi.SPLIT_GROUP_DTYPE.itemsize)
-        self.stage_h = [torch.empty(nb, dtype=torch.uint8, pin_memory=True) for _ in range(self.ring)]
-        self.stage_d = [torch.empty(nb, dtype=torch.uint8, device="cuda") for _ in range(self.ring)]
-        self.tick = 0
+        self.lanes = []
+        for ti, nk in enumerate(self.nks):
+            nb = max(1 << 16, 64 * cap[nk] + 8 * cap[nk] * abi.SPLIT_GROUP_DTYPE.itemsize)
+            self.lanes.append(Server._Lane(
+                ti, nk, torch.cuda.Stream(),
+                [torch.empty(nb, dtype=torch.uint8, pin_memory=True) for _ in range(self.ring)],
+                [torch.empty(nb, dtype=torch.uint8, device="cuda") for _ in range(self.ring)]))
+        self.tick = 0     # lane ticks issued, all lanes
         self.active = {}  # global slot -> [request, steps_done, admitted_time, nbytes]
         self.pending = []  # retiring batches: (event, entries, host buffers)
         self.results = []
+
+    class _Lane:
+        """One size class: stream, tick count, waiting requests, active
+        slots, events of its ticks in flight, staging ring."""
+
+        def __init__(self, ti, nk, stream, stage_h, stage_d):
+            self.ti, self.nk, self.stream = ti, nk, stream
+            self.stage_h, self.stage_d = stage_h, stage_d
+            self.tick = 0
+            self.waiting = []
+            self.slots = set()
+            self.inflight = []
 
     # -- staging -------------------------------------------------------------------
     class _Stage:
@@ -253,7 +271,7 @@ class Server:
         device copies are views of the device buffer at the same offsets."""
 
         def __init__(self, h, d):
-            self.h, self.d, self.n, self.items = h, d, 0, []
+            self.h, self.d, self.n = h, d, 0
 
         def add(self, arr):
             arr = np.ascontiguousarray(arr)
@@ -269,14 +287,10 @@ class Server:
             o, n = ref
             return self.d[o:o + n].view(dtype)
 
-    def _stage(self):
-        i = self.tick % self.ring
-        return Server._Stage(self.stage_h[i], self.stage_d[i])
-
-    def _push(self, st):
-        if st.n:
-            self.stage_d[self.tick % self.ring][:st.n].copy_(
-                self.stage_h[self.tick % self.ring][:st.n], non_blocking=True)
+        def push(self):
+            """Copy to the device on the current stream."""
+            if self.n:
+                self.d[:self.n].copy_(self.h[:self.n], non_blocking=True)
 
     def _rows(self, offs, nks, total):
         """Device row indices of the state ranges [off, off + nk) (total =
@@ -286,159 +300,143 @@ class Server:
         base = torch.repeat_interleave(torch.cumsum(nks, 0) - nks, nks, output_size=total)
         return starts + (torch.arange(total, device="cuda") - base)
 
-    # -- admission / launch / retirement ---------------------------------------------
-    def _admit_batch(self, reqs, now, st):
-        """Admit as many of ``reqs`` as slots and budget allow; returns the
-        ones left waiting.  Their wire descriptors and zeroed state reach the
-        device with this tick's staged copy."""
+    # -- one tick of one lane ------------------------------------------------------------
+    def _admit(self, lane, now, st):
+        """Admit as many of the lane's waiting requests as slots and budget
+        allow; returns the staged admission or None.  Their wire descriptors
+        and zeroed state reach the device with this tick's staged copy."""
         recs, slots, left = [], [], []
-        for req in reqs:
-            if req.nsteps > self.max_steps:
-                raise ValueError(f"request {req.rid}: {req.nsteps} steps > max_steps")
+        for req in lane.waiting:
             nbytes = request_bytes(req.nk, req.nsteps, self.form)
-            s = self.pool.try_take(req.nk, nbytes)
-            if s is None:
-                left.append(req)
+            sl = self.pool.try_take(req.nk, nbytes) if not left else None
+            if sl is None:
+                left.append(req)  # first come, first served within the class
                 continue
-            g = self.cls_base[req.nk] + s
-            ti = self.nks.index(req.nk)
-            rec = wire_record(req, self.grids[ti], table=ti, off=self.slot_off[g],
+            g = self.cls_base[req.nk] + sl
+            rec = wire_record(req, self.grids[lane.ti], table=lane.ti, off=self.slot_off[g],
                               p_off=g * self.max_steps)
             self.h_wires[g] = rec[0]
             recs.append(rec)
             slots.append(g)
             self.active[g] = [req, 0, now, nbytes]
-        if slots:
-            sl = np.asarray(slots, dtype=np.int64)
-            nk_adm = np.asarray([self.active[g][0].nk for g in slots], dtype=np.int64)
-            self._adm = (st.add(np.concatenate(recs)), st.add(sl),
-                         st.add(np.asarray([self.slot_off[g] for g in slots], dtype=np.int64)),
-                         st.add(nk_adm), len(slots), int(nk_adm.sum()))
-        else:
-            self._adm = None
-        return left
+            lane.slots.add(g)
+        lane.waiting = left
+        if not slots:
+            return None
+        return (st.add(np.concatenate(recs)), st.add(np.asarray(slots, dtype=np.int64)),
+                st.add(np.asarray([self.slot_off[g] for g in slots], dtype=np.int64)),
+                len(slots), len(slots) * lane.nk)
 
-    def _apply_admissions(self, st):
-        if self._adm is None:
-            return
+    def _tick(self, lane, now):
+        """Admit, advance and retire one size class by ``chunk`` steps, all
+        on the lane's stream.  Returns False when the lane has nothing to do."""
         torch = self.torch
-        r_rec, r_sl, r_off, r_nk, k, total = self._adm
-        idx = st.view(r_sl, torch.int64)
-        self._wires_rows[idx] = st.view(r_rec, torch.uint8).view(k, self.isz)
-        rows = self._rows(st.view(r_off, torch.int64), st.view(r_nk, torch.int64), total)
-        self.y.index_fill_(0, rows, 0.0)
-
-    def _launch(self, st):
-        torch = self.torch
-        if not self.active:
-            return
-        slots = np.fromiter(self.active.keys(), dtype=np.int64)
+        i = lane.tick % self.ring
+        st = Server._Stage(lane.stage_h[i], lane.stage_d[i])
+        adm = self._admit(lane, now, st)
+        if not lane.slots:
+            return False
+        slots = np.fromiter(sorted(lane.slots), dtype=np.int64)
         done = np.array([self.active[g][1] for g in slots], dtype=np.int64)
         r_idx = st.add(slots)
         r_val = st.add(slots * self.max_steps + done)  # P(t) records append
-        # solves that finish with this tick: their slots and state ranges
+        # solves that finish with this tick
         fin = slots[done + self.chunk >= np.array([self.active[g][0].nsteps for g in slots])]
+        r_fin = r_foff = None
         if fin.size:
-            self._fin = (fin, st.add(fin),
-                         st.add(np.asarray([self.slot_off[g] for g in fin], dtype=np.int64)),
-                         st.add(np.asarray([self.active[g][0].nk for g in fin], dtype=np.int64)))
-        else:
-            self._fin = None
-        tables = self.h_wires["table"][slots]
+            r_fin = st.add(fin)
+            r_foff = st.add(np.asarray([self.slot_off[g] for g in fin], dtype=np.int64))
+        nk, ti = lane.nk, lane.ti
         if self.form == "split":
-            counts = {nk: int((tables == ti).sum()) for ti, nk in enumerate(self.nks)}
-            self.wg = choose_wires_per_cta(counts, self.sms, lambda nk: nk <= self.w8_max)
-        plan = []
-        # largest grids first: their CTAs run longest, so they start before
-        # the short ones fill the SMs
-        for ti, nk in sorted(enumerate(self.nks), key=lambda t: -t[1]):
-            sel = slots[tables == ti]
-            if sel.size == 0:
-                continue
-            if self.form == "split":
-                wg = self.wg[nk]
-                ng = (sel.size + wg - 1) // wg
-                grp = np.zeros(ng, dtype=abi.SPLIT_GROUP_DTYPE)
-                grp["table"] = ti
-                grp["wire"] = -1
-                padded = np.full(ng * wg, -1, dtype=np.int32)
-                padded[:sel.size] = sel
-                grp["wire"][:, :wg] = padded.reshape(ng, wg)
-                grp["nw"] = wg
-                grp["nw"][-1] = sel.size - (ng - 1) * wg
-                plan.append((ti, nk, st.add(grp), ng, wg))
-            else:
-                plan.append((ti, nk, st.add(sel.astype(np.int32)), sel.size, 0))
-        self._push(st)
-        self._apply_admissions(st)
-        self._wires_i64[st.view(r_idx, torch.int64), self._p_off_col] = st.view(r_val, torch.int64)
-        main = torch.cuda.current_stream()
-        fork = torch.cuda.Event()
-        fork.record(main)
-        joins = []
+            # the classes share the SMs, so the choice sees every lane's load
+            counts = {ln.nk: len(ln.slots) for ln in self.lanes}
+            wg = choose_wires_per_cta(counts, self.sms, lambda n: n <= self.w8_max)[nk]
+            ng = (slots.size + wg - 1) // wg
+            grp = np.zeros(ng, dtype=abi.SPLIT_GROUP_DTYPE)
+            grp["table"] = ti
+            grp["wire"] = -1
+            padded = np.full(ng * wg, -1, dtype=np.int32)
+            padded[:slots.size] = slots
+            grp["wire"][:, :wg] = padded.reshape(ng, wg)
+            grp["nw"] = wg
+            grp["nw"][-1] = slots.size - (ng - 1) * wg
+            r_grp, n_launch = st.add(grp), ng
+        else:
+            wg = 0
+            r_grp, n_launch = st.add(slots.astype(np.int32)), slots.size
         common = (self.device.ptr(self.d_tables), len(self.h_tables), self.device.ptr(self.tabdata),
                   self.tabdata.numel(), self.device.ptr(self.d_wires), self.nslots)
-        dt = float(next(iter(self.active.values()))[0].dt)
-        for ti, nk, ref, n, wg in plan:
-            sm = self.streams[ti]
-            sm.wait_event(fork)
-            ptr = self.device.ptr(st.view(ref, torch.uint8))
+        dt = float(self.active[int(slots[0])][0].dt)
+        sm = lane.stream
+        with torch.cuda.stream(sm):
+            st.push()
+            if adm is not None:
+                r_rec, r_sl, r_off, k, total = adm
+                idx = st.view(r_sl, torch.int64)
+                self._wires_rows[idx] = st.view(r_rec, torch.uint8).view(k, self.isz)
+                nks_t = torch.full((k,), nk, dtype=torch.int64, device="cuda")
+                self.y.index_fill_(0, self._rows(st.view(r_off, torch.int64), nks_t, total), 0.0)
+            self._wires_i64[st.view(r_idx, torch.int64), self._p_off_col] = st.view(r_val, torch.int64)
+            ptr = self.device.ptr(st.view(r_grp, torch.uint8))
             if self.form == "split":
-                self._lib.call("psb_rk4_split", *common, ptr, n, wg, nk, self.device.ptr(self.y),
-                               self.n_state, self.device.ptr(self.ws), self.ws.numel(), self.chunk,
-                               dt, self.device.ptr(self.P), self.P.shape[0], 1, self.max_steps,
-                               abi.as_ptr(self.model), self.device.stream_ptr(sm))
+                self._lib.call("psb_rk4_split", *common, ptr, n_launch, wg, nk,
+                               self.device.ptr(self.y), self.n_state, self.device.ptr(self.ws),
+                               self.ws.numel(), self.chunk, dt, self.device.ptr(self.P),
+                               self.P.shape[0], 1, self.max_steps, abi.as_ptr(self.model),
+                               self.device.stream_ptr(sm))
             else:
                 flags = abi.PSB_TAB_SHARED_V if (self.h_tables["flags"][ti] & abi.PSB_TAB_SHARED_V) else 0
-                self._lib.call("psb_rk4_f64", *common, ptr, n, self.device.ptr(self.y), self.n_state,
-                               nk, flags, self.chunk, dt, self.device.ptr(self.P), self.P.shape[0],
-                               1, self.max_steps, abi.as_ptr(self.model), self.device.stream_ptr(sm))
+                self._lib.call("psb_rk4_f64", *common, ptr, n_launch, self.device.ptr(self.y),
+                               self.n_state, nk, flags, self.chunk, dt, self.device.ptr(self.P),
+                               self.P.shape[0], 1, self.max_steps, abi.as_ptr(self.model),
+                               self.device.stream_ptr(sm))
+            for g in slots:
+                self.active[int(g)][1] += self.chunk
+            if fin.size:
+                self._retire(lane, fin, st.view(r_fin, torch.int64), st.view(r_foff, torch.int64))
             ev = torch.cuda.Event()
             ev.record(sm)
-            joins.append(ev)
-        for ev in joins:
-            main.wait_event(ev)
-        for g in slots:
-            self.active[int(g)][1] += self.chunk
+        lane.inflight.append(ev)
+        lane.tick += 1
+        self.tick += 1
+        return True
 
-    def _retire(self, st):
+    def _retire(self, lane, fin, fin_t, foff_t):
+        """Gather the finished solves' records, state and descriptors on the
+        lane's stream (the current stream), then copy them to pinned host
+        memory on the copy stream."""
         torch = self.torch
-        if getattr(self, "_fin", None) is None:
-            return
-        fin, r_fin, r_off, r_nk = self._fin
-        self._fin = None
         entries = [(int(g), *self.active.pop(int(g))) for g in fin]
-        nks = np.asarray([e[1].nk for e in entries], dtype=np.int64)
-        fin_t = st.view(r_fin, torch.int64)
-        main = torch.cuda.current_stream()
-        rows = self._rows(st.view(r_off, torch.int64), st.view(r_nk, torch.int64), int(nks.sum()))
-        # gather on the main stream (ordered after this tick's launches) ...
+        for g in fin:
+            lane.slots.discard(int(g))
+        total = len(entries) * lane.nk
+        nks_t = torch.full((len(entries),), lane.nk, dtype=torch.int64, device="cuda")
+        rows = self._rows(foff_t, nks_t, total)
         Pg = self.P.view(self.nslots, self.max_steps, 2).index_select(0, fin_t)
         yg = self.y.index_select(0, rows)
-        wg = self._wires_rows.index_select(0, fin_t)
+        wgr = self._wires_rows.index_select(0, fin_t)
         ev0 = torch.cuda.Event()
-        ev0.record(main)
+        ev0.record(torch.cuda.current_stream())
         cs = self.copy_stream
         cs.wait_event(ev0)
-        # ... and copy to pinned host memory on the copy stream
         with torch.cuda.stream(cs):
             hP = torch.empty(Pg.shape, dtype=torch.float64, pin_memory=True)
             hy = torch.empty(yg.shape, dtype=torch.float64, pin_memory=True)
-            hw = torch.empty(wg.shape, dtype=torch.uint8, pin_memory=True)
+            hw = torch.empty(wgr.shape, dtype=torch.uint8, pin_memory=True)
             hP.copy_(Pg, non_blocking=True)
             hy.copy_(yg, non_blocking=True)
-            hw.copy_(wg, non_blocking=True)
+            hw.copy_(wgr, non_blocking=True)
             Pg.record_stream(cs)
             yg.record_stream(cs)
-            wg.record_stream(cs)
+            wgr.record_stream(cs)
             ev = torch.cuda.Event()
             ev.record(cs)
-        self.pending.append((ev, entries, nks, hP, hy, hw))
+        self.pending.append((ev, entries, hP, hy, hw))
 
     def _collect(self, block=False):
         keep = []
         for item in self.pending:
-            ev, entries, nks, hP, hy, hw = item
+            ev, entries, hP, hy, hw = item
             if block:
                 ev.synchronize()
             elif not ev.query():
@@ -460,37 +458,47 @@ class Server:
     def run(self, requests, realtime=True, max_inflight_ticks=2):
         """Serve ``requests``.  realtime: arrivals are honoured on the wall
         clock (the Poisson stream), else every request is available from the
-        start (throughput / capacity runs)."""
-        torch = self.torch
+        start (throughput / capacity runs).
+
+        Each size class ticks on its own stream as soon as its previous
+        ticks allow (at most ``max_inflight_ticks`` queued), so a small
+        solve advances at its own kernel's pace instead of waiting each tick
+        for the largest grid; the classes' launches run concurrently on the
+        GPU.  Largest grids are served first in each round."""
         assert max_inflight_ticks < self.ring
         queue = sorted(requests, key=lambda r: r.arrival)
+        for req in queue:
+            if req.nsteps > self.max_steps:
+                raise ValueError(f"request {req.rid}: {req.nsteps} steps > max_steps")
+            if req.nk not in self.cls_base:
+                raise ValueError(f"request {req.rid}: Nk {req.nk} is not served")
+        by_nk = {lane.nk: lane for lane in self.lanes}
+        order = sorted(self.lanes, key=lambda ln: -ln.nk)
         qi, n = 0, len(queue)
-        waiting = []
         self.results = []
         self.t_start = time.perf_counter()
-        tick_events = []
         while len(self.results) < n:
             now = time.perf_counter() - self.t_start
             while qi < n and (not realtime or queue[qi].arrival <= now):
-                waiting.append(queue[qi])
+                by_nk[queue[qi].nk].waiting.append(queue[qi])
                 qi += 1
             self._collect()
-            st = self._stage()
-            waiting = self._admit_batch(waiting, now, st)
-            if self.active:
-                self._launch(st)
-                self._retire(st)
-                ev = torch.cuda.Event()
-                ev.record(torch.cuda.current_stream())
-                tick_events.append(ev)
-                self.tick += 1
-                while len(tick_events) > max_inflight_ticks:
-                    tick_events.pop(0).synchronize()
-            elif self.pending:
+            issued = False
+            for lane in order:
+                while lane.inflight and lane.inflight[0].query():
+                    lane.inflight.pop(0)
+                if len(lane.inflight) < max_inflight_ticks and (lane.slots or lane.waiting):
+                    issued |= self._tick(lane, now)
+            if issued:
+                continue
+            busy = [ln.inflight[0] for ln in order if ln.inflight]
+            if self.pending and not busy:
                 self._collect(block=True)
+            elif busy:
+                time.sleep(5e-5)
             elif qi < n and realtime:
                 time.sleep(max(0.0, min(1e-3, queue[qi].arrival - now)))
-        torch.cuda.synchronize()
+        self.torch.cuda.synchronize()
         self._collect(block=True)
         self.elapsed = time.perf_counter() - self.t_start
         return sorted(self.results, key=lambda r: r.rid)
