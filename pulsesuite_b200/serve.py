@@ -26,6 +26,7 @@ Host-side logic (request stream, slot allocation, HBM accounting) is plain
 Python and tested without a GPU; the device path needs the sm_100a library.
 """
 
+import functools
 import math
 import time
 from dataclasses import dataclass, field
@@ -50,6 +51,7 @@ SPLIT_CTA_MS = {(64, 4): 0.49, (64, 8): 0.73, (128, 4): 0.58, (128, 8): 0.84,
                 (1024, 4): 8.15, (1024, 8): 9.71}
 
 
+@functools.lru_cache(maxsize=None)
 def split_cta_cost(nk, w):
     ref = min((k for k, ww in SPLIT_CTA_MS if ww == w), key=lambda k: abs(math.log(k / nk)))
     return SPLIT_CTA_MS[(ref, w)] * (nk / ref) ** 2
@@ -240,16 +242,25 @@ class Server:
         # queue and pinned staging ring (per-tick metadata goes through one
         # asynchronous copy; the ring is deeper than the ticks allowed in
         # flight, so a buffer is never rewritten while its copy may pend)
+        # The lanes' streams get priorities by grid size, the largest grid
+        # highest: its CTAs run longest and set the tail (and the p99), so
+        # when SMs free up the CTA scheduler gives them to it first.
         self.ring = 3
         self.lanes = []
+        least, greatest = torch.cuda.Stream.priority_range()
+        rank = {nk: r for r, nk in enumerate(sorted(self.nks, reverse=True))}
         for ti, nk in enumerate(self.nks):
             nb = max(1 << 16, 64 * cap[nk] + 8 * cap[nk] * abi.SPLIT_GROUP_DTYPE.itemsize)
+            prio = min(least, greatest + rank[nk])
             self.lanes.append(Server._Lane(
-                ti, nk, torch.cuda.Stream(),
+                ti, nk, torch.cuda.Stream(priority=prio),
                 [torch.empty(nb, dtype=torch.uint8, pin_memory=True) for _ in range(self.ring)],
                 [torch.empty(nb, dtype=torch.uint8, device="cuda") for _ in range(self.ring)]))
         self.tick = 0     # lane ticks issued, all lanes
         self.active = {}  # global slot -> [request, steps_done, admitted_time, nbytes]
+        self.steps_done = np.zeros(self.nslots, dtype=np.int64)  # per slot, of its solve
+        self.steps_req = np.zeros(self.nslots, dtype=np.int64)
+        self._ar = {nk: torch.arange(nk, dtype=torch.int64, device="cuda") for nk in self.nks}
         self.pending = []  # retiring batches: (event, entries, host buffers)
         self.results = []
 
@@ -292,13 +303,10 @@ class Server:
             if self.n:
                 self.d[:self.n].copy_(self.h[:self.n], non_blocking=True)
 
-    def _rows(self, offs, nks, total):
-        """Device row indices of the state ranges [off, off + nk) (total =
-        sum of nk, known on the host, so nothing synchronises)."""
-        torch = self.torch
-        starts = torch.repeat_interleave(offs, nks, output_size=total)
-        base = torch.repeat_interleave(torch.cumsum(nks, 0) - nks, nks, output_size=total)
-        return starts + (torch.arange(total, device="cuda") - base)
+    def _rows(self, offs, nk):
+        """Device row indices of the state ranges [off, off + nk) of one
+        size class, as one broadcast add (nothing synchronises)."""
+        return (offs.view(-1, 1) + self._ar[nk].view(1, -1)).view(-1)
 
     # -- one tick of one lane ------------------------------------------------------------
     def _admit(self, lane, now, st):
@@ -319,13 +327,15 @@ class Server:
             recs.append(rec)
             slots.append(g)
             self.active[g] = [req, 0, now, nbytes]
+            self.steps_done[g] = 0
+            self.steps_req[g] = req.nsteps
             lane.slots.add(g)
         lane.waiting = left
         if not slots:
             return None
         return (st.add(np.concatenate(recs)), st.add(np.asarray(slots, dtype=np.int64)),
                 st.add(np.asarray([self.slot_off[g] for g in slots], dtype=np.int64)),
-                len(slots), len(slots) * lane.nk)
+                len(slots))
 
     def _tick(self, lane, now):
         """Admit, advance and retire one size class by ``chunk`` steps, all
@@ -337,11 +347,11 @@ class Server:
         if not lane.slots:
             return False
         slots = np.fromiter(sorted(lane.slots), dtype=np.int64)
-        done = np.array([self.active[g][1] for g in slots], dtype=np.int64)
+        done = self.steps_done[slots]
         r_idx = st.add(slots)
         r_val = st.add(slots * self.max_steps + done)  # P(t) records append
         # solves that finish with this tick
-        fin = slots[done + self.chunk >= np.array([self.active[g][0].nsteps for g in slots])]
+        fin = slots[done + self.chunk >= self.steps_req[slots]]
         r_fin = r_foff = None
         if fin.size:
             r_fin = st.add(fin)
@@ -371,11 +381,10 @@ class Server:
         with torch.cuda.stream(sm):
             st.push()
             if adm is not None:
-                r_rec, r_sl, r_off, k, total = adm
+                r_rec, r_sl, r_off, k = adm
                 idx = st.view(r_sl, torch.int64)
                 self._wires_rows[idx] = st.view(r_rec, torch.uint8).view(k, self.isz)
-                nks_t = torch.full((k,), nk, dtype=torch.int64, device="cuda")
-                self.y.index_fill_(0, self._rows(st.view(r_off, torch.int64), nks_t, total), 0.0)
+                self.y.index_fill_(0, self._rows(st.view(r_off, torch.int64), nk), 0.0)
             self._wires_i64[st.view(r_idx, torch.int64), self._p_off_col] = st.view(r_val, torch.int64)
             ptr = self.device.ptr(st.view(r_grp, torch.uint8))
             if self.form == "split":
@@ -390,8 +399,7 @@ class Server:
                                self.n_state, nk, flags, self.chunk, dt, self.device.ptr(self.P),
                                self.P.shape[0], 1, self.max_steps, abi.as_ptr(self.model),
                                self.device.stream_ptr(sm))
-            for g in slots:
-                self.active[int(g)][1] += self.chunk
+            self.steps_done[slots] += self.chunk
             if fin.size:
                 self._retire(lane, fin, st.view(r_fin, torch.int64), st.view(r_foff, torch.int64))
             ev = torch.cuda.Event()
@@ -409,9 +417,7 @@ class Server:
         entries = [(int(g), *self.active.pop(int(g))) for g in fin]
         for g in fin:
             lane.slots.discard(int(g))
-        total = len(entries) * lane.nk
-        nks_t = torch.full((len(entries),), lane.nk, dtype=torch.int64, device="cuda")
-        rows = self._rows(foff_t, nks_t, total)
+        rows = self._rows(foff_t, lane.nk)
         Pg = self.P.view(self.nslots, self.max_steps, 2).index_select(0, fin_t)
         yg = self.y.index_select(0, rows)
         wgr = self._wires_rows.index_select(0, fin_t)
