@@ -137,7 +137,11 @@ class WireBatch:
             self.split_launches.append((key[0], device.to_device(ga), len(ga), nkmax))
         # the class with the largest grid first: its CTAs run longest
         self.split_launches.sort(key=lambda l: -l[3])
-        self.side_streams = [torch.cuda.Stream() for _ in self.split_launches[1:]]
+        # one stream per class, priorities by grid size (the largest grid's
+        # CTAs run longest, so the CTA scheduler serves them first)
+        least, greatest = torch.cuda.Stream.priority_range()
+        self.side_streams = [torch.cuda.Stream(priority=min(least, greatest + r))
+                             for r in range(len(self.split_launches))]
         self.ws = torch.zeros(int(lib.psb_split_ws_bytes(self.n_state)), dtype=torch.uint8,
                               device="cuda")
 
@@ -187,19 +191,18 @@ class WireBatch:
     def rk4(self, nsteps, dt, p_stride=1, stream=None):
         if self.form == "split":
             main = stream if stream is not None else torch.cuda.current_stream()
-            streams = [main] + self.side_streams
-            if len(streams) > 1:
-                fork = torch.cuda.Event()
-                fork.record(main)
-                for s in streams[1:]:
-                    s.wait_event(fork)
+            streams = self.side_streams
+            fork = torch.cuda.Event()
+            fork.record(main)
+            for s in streams:
+                s.wait_event(fork)
             for (wg, groups, ng, nkmax), s in zip(self.split_launches, streams):
                 _lib.call("psb_rk4_split", *self._common(), device.ptr(groups), ng, wg, nkmax,
                           device.ptr(self.y), self.n_state, device.ptr(self.ws), self.ws.numel(),
                           int(nsteps), float(dt), device.ptr(self.P), self.P.shape[0],
                           int(p_stride), self.p_cap, abi.as_ptr(self.model),
                           device.stream_ptr(s))
-            for s in streams[1:]:
+            for s in streams:
                 join = torch.cuda.Event()
                 join.record(s)
                 main.wait_event(join)
