@@ -672,10 +672,15 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
               for (int kj = 0; kj < nK; ++kj, a1 -= kTileCols, bd += 32) slice(a1, bd, kj != 0);
             }
           } else {
-            // streamed: slices k0 .. k0 + gn - 1 sit in slots gb G .. gb G + gn - 1
+            // streamed: slices k0 .. k0 + gn - 1 sit in slots gb G .. gb G + gn - 1.
+            // Every lane polls the group and the warp reconverges after it
+            // (so no lane can fall a buffer cycle behind and test a parity
+            // that has come round again), but it votes on the outcome only
+            // once per row tile: a vote costs the issuing lane about as much
+            // as the poll.
             for (int k0 = 0; k0 < nK; k0 += G) {
               const int gn = min(G, nK - k0);
-              if (!warp_wait(&afull[gb], gph)) {
+              if (!mbar_wait(&afull[gb], gph, abort)) {
                 ok = false;
                 break;
               }
@@ -685,13 +690,14 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
                 for (int j = 0; j < gn; ++j, a1 += kTileCols, bd += 32) slice(a1, bd, k0 + j != 0);
                 umma_commit(&afree[gb]);  // the group's slots are reusable once these finish
               }
+              __syncwarp();
               if (++gb == 2) {
                 gb = 0;
                 gph ^= 1u;
               }
             }
           }
-          __syncwarp();
+          ok = __all_sync(0xffffffffu, ok);
           if (!ok) break;
           if (issuer) umma_commit(&dfull[b]);  // the row tile is ready to drain
           __syncwarp();
