@@ -201,6 +201,20 @@ __device__ __forceinline__ void digits3(float v, int& d1, int& d2, int& d3) {
   d3 = (int)f3;
 }
 
+// One step of a halving max-butterfly over a warp: each lane holds C
+// values, sends half of them to the lane `o` apart and keeps the maxima of
+// the other half (the lane with bit o set keeps the upper half).
+template <int C>
+__device__ __forceinline__ void colmax_halve(float* v, int o, int lane) {
+  const bool up = (lane & o) != 0;
+#pragma unroll
+  for (int i = 0; i < C / 2; ++i) {
+    const float send = up ? v[i] : v[i + C / 2];
+    const float keep = up ? v[i + C / 2] : v[i];
+    v[i] = fmaxf(keep, __shfl_xor_sync(0xffffffffu, send, o));
+  }
+}
+
 // Shared-memory matrix descriptor, no swizzle (canonical layout of 8-row x
 // 16-byte core matrices): start address, leading-dimension (K) byte offset,
 // stride-dimension (M/N) byte offset, descriptor version 1.
@@ -482,13 +496,29 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   const int w0 = hh * WH;
   double4* g_y = reinterpret_cast<double4*>(a.y);
   // Largest |value| of each of this warp's X columns, per lane quarter q.
+  // Halving butterfly (colmax_halve): the 4 WH columns need 4 WH shuffles
+  // in all, not 5 per column; afterwards lane L holds column
+  // (L >> (5 - m)) & (4 WH - 1), m = log2(4 WH).
   auto publish_colmax = [&](const float* cm) {
+    constexpr int C = 4 * WH;  // 8 or 16
+    static_assert(C == 8 || C == 16, "column count of a drain warp");
+    float v[C];
 #pragma unroll
-    for (int c = 0; c < 4 * WH; ++c) {
-      float m = cm[c];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-      if (lane == 0) colmax[q * N + 4 * w0 + c] = m;
+    for (int c = 0; c < C; ++c) v[c] = cm[c];
+    if constexpr (C == 16) {
+      colmax_halve<16>(v, 16, lane);
+      colmax_halve<8>(v, 8, lane);
+      colmax_halve<4>(v, 4, lane);
+      colmax_halve<2>(v, 2, lane);
+      v[0] = fmaxf(v[0], __shfl_xor_sync(0xffffffffu, v[0], 1));
+      if ((lane & 1) == 0) colmax[q * N + 4 * w0 + ((lane >> 1) & 15)] = v[0];
+    } else {
+      colmax_halve<8>(v, 16, lane);
+      colmax_halve<4>(v, 8, lane);
+      colmax_halve<2>(v, 4, lane);
+      v[0] = fmaxf(v[0], __shfl_xor_sync(0xffffffffu, v[0], 2));
+      v[0] = fmaxf(v[0], __shfl_xor_sync(0xffffffffu, v[0], 1));
+      if ((lane & 3) == 0) colmax[q * N + 4 * w0 + ((lane >> 2) & 7)] = v[0];
     }
   };
   auto track = [&](float* cm, int j, float4 v) {
@@ -636,9 +666,10 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
       const bool got = mbar_wait(bar, parity, abort);
       return __all_sync(0xffffffffu, got);
     };
+    // (an abort is seen through the stage-end snapshot and inside every
+    // wait, so the stage start needs no vote of its own)
     for (int s = 0; s < total_stages; ++s) {
-      const bool run = __all_sync(0xffffffffu, !*abort);
-      if (run) {
+      {
         bool ok = !(s == 0 && persist) || warp_wait(&afull[0], 0);
         tc_fence_after();
         // B descriptor of X[s & 1] at k' = 0; +32 per 64-wide slice, +16 per
@@ -646,10 +677,8 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
         const uint64_t bdesc0 = smem_desc(smem_u32(xbase + (s & 1) * L.xbuf), 128, xsbo);
         for (int mi = 0; ok && mi < nM; ++mi, ++it) {
           const int b = it & 1;
-          if (it >= 2 && !warp_wait(&dfree[b], ((it >> 1) - 1) & 1)) {
-            ok = false;
-            break;
-          }
+          // every lane polls; the vote on the outcome comes at the tile end
+          if (it >= 2 && !mbar_wait(&dfree[b], ((it >> 1) - 1) & 1, abort)) ok = false;
           tc_fence_after();
           const uint32_t d2 = tmem + (uint32_t)(3 * N * b);
           const uint32_t d3 = d2 + (uint32_t)N;
@@ -667,7 +696,7 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
           uint64_t bd = bdesc0;
           if (persist) {
             // persistent slot of slice kj is 2 mi - kj + nK - 1
-            if (issuer) {
+            if (issuer && ok) {
               uint32_t a1 = tmem + acol0 + (uint32_t)((2 * mi + nK - 1) * kTileCols);
               for (int kj = 0; kj < nK; ++kj, a1 -= kTileCols, bd += 32) slice(a1, bd, kj != 0);
             }
@@ -678,7 +707,7 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
             // that has come round again), but it votes on the outcome only
             // once per row tile: a vote costs the issuing lane about as much
             // as the poll.
-            for (int k0 = 0; k0 < nK; k0 += G) {
+            for (int k0 = 0; ok && k0 < nK; k0 += G) {
               const int gn = min(G, nK - k0);
               if (!mbar_wait(&afull[gb], gph, abort)) {
                 ok = false;
