@@ -829,10 +829,13 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
       for (int mi = 0; mi < nM; ++mi, ++it) {
         const int k = mi * kTileRows + 32 * q + lane;
         const int b = it & 1;
+        // band energies of this row: loaded before the wait, which hides them
+        const double ekh = k < nk ? (Ee[k] + Eh[k]) * inv_hbar : 0.0;
         bool got = mbar_wait(&dfull[b], (it >> 1) & 1, abort);
         got = __all_sync(0xffffffffu, got);
         if (got) tc_fence_after();
-        const double ekh = k < nk ? (Ee[k] + Eh[k]) * inv_hbar : 0.0;
+        // this lane's row takes part in this tile (abort read once per tile)
+        const bool live = got && k < nk && !*abort;
         const uint32_t kofs = (uint32_t)(k >> 4) * 128 + (uint32_t)(k & 15);
 #pragma unroll
         for (int jp = 0; jp < WH; jp += 2) {
@@ -851,7 +854,7 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
             const int w = w0 + j;
             const float Mjr = __shfl_sync(0xffffffffu, Mr, j);
             const float Mji = __shfl_sync(0xffffffffu, Mi, j);
-            if (!got || k >= nk || w >= grp.nw || *abort) continue;
+            if (!live || w >= grp.nw) continue;
             // exchange sums / hbar (SBEs.py:896-921) from the exact digit
             // products, rounded once to FP32
             float exh[4];
