@@ -57,6 +57,9 @@ def parse():
     ap.add_argument("--capacity-requests", type=int, default=6000,
                     help="c4: requests of the saturated capacity run of each form")
     ap.add_argument("--nwires", type=int, default=0, help="override the workload's wire count")
+    ap.add_argument("--acc-steps", type=int, default=3000,
+                    help="split form: time steps of the accuracy check against the plain form "
+                         "(the workload's duration, at most this; 0 skips it)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -201,6 +204,50 @@ def measured_bf16_peak():
         return 1590.0, "fallback 1.59 PFLOP/s (no MEASURED_PEAKS.json)"
 
 
+def split_accuracy(wl, nsteps, stream):
+    """Per-wire error of the split form against the plain FP64 form (which
+    matches the FP64 oracle to <= 1e-10) on the same workload from the same
+    zero state, max and median over wires:
+    P: max_t |P - P_ref| / max_t |P_ref|;
+    n: max_k |n - n_ref| / max_k |n_ref| of the final n_e and n_h;
+    p: max_k |p - p_ref| of the final state over the wire's peak p scale
+    max_t |P_ref| / (|pscale| Nk) (p itself may have dephased to ~1e-20 by
+    the end, below the rounding floor of its peak, so it is not a scale)."""
+    import torch
+
+    from pulsesuite_b200.batch import WireBatch
+
+    out = {}
+    for form in ("split", "plain"):
+        bb = WireBatch(wl.grids, wl.wires, screened=wl.screened, p_cap=nsteps, form=form)
+        bb.rk4(nsteps, wl.dt, p_stride=1, stream=stream)
+        torch.cuda.synchronize()
+        out[form] = (bb.P[:bb.nw * nsteps].view(bb.nw, nsteps, 2).clone(), bb.y.clone(),
+                     [bb.wire_slice(i) for i in range(bb.nw)])
+        del bb
+    Ps, ys, sl = out["split"]
+    Pp, yp, _ = out["plain"]
+    dP = torch.linalg.vector_norm(Ps - Pp, dim=2).amax(dim=1)
+    refP = torch.linalg.vector_norm(Pp, dim=2).amax(dim=1)
+    errP = (dP / refP.clamp_min(1e-300)).cpu().numpy()
+    refP = refP.cpu().numpy()
+    d = ys - yp
+    dpk = torch.sqrt(d[:, 0] ** 2 + d[:, 1] ** 2).cpu().numpy()
+    dn, rn = d[:, 2:].abs().cpu().numpy(), yp[:, 2:].abs().cpu().numpy()
+    errN = np.zeros(len(sl))
+    errp = np.zeros(len(sl))
+    nks = wl.nks
+    for i, r in enumerate(sl):
+        errN[i] = max(dn[r, c].max() / max(rn[r, c].max(), 1e-300) for c in range(2))
+        pk = refP[i] / max(abs(float(wl.wires["pscale"][i])) * nks[i], 1e-300)
+        errp[i] = dpk[r].max() / max(pk, 1e-300)
+    return {"vs": "plain FP64 form (<= 1e-10 from the FP64 oracle)", "time_steps": nsteps,
+            "P_rel_err_max": float(errP.max()), "P_rel_err_median": float(np.median(errP)),
+            "n_rel_err_max": float(errN.max()), "n_rel_err_median": float(np.median(errN)),
+            "p_err_vs_peak_max": float(errp.max()),
+            "p_err_vs_peak_median": float(np.median(errp))}
+
+
 def run_ours(a):
     import torch
     import torch.distributed as dist
@@ -280,6 +327,12 @@ def run_ours(a):
         plain = {"value": pval, "ms_per_step": pms / a.steps, "split_over_plain": value / pval,
                  "gpu_launches": a.steps * bp.launches_per_call}
         del bp
+    accuracy = None
+    if a.form == "split" and not a.no_plain and a.acc_steps > 0:
+        # the workload's own duration, bounded (at most ~1e10 wire*k*steps)
+        # so the check stays a few seconds
+        n_acc = min(wl.nsteps, a.acc_steps, max(50, int(1e10 // wl.units_per_step)))
+        accuracy = split_accuracy(wl, n_acc, stream)
 
     # -- end to end through the public API: pinned host state in, P + state out
     y_host = torch.zeros((b.n_state, 4), dtype=torch.float64).pin_memory()
@@ -345,6 +398,7 @@ def run_ours(a):
                      "flops_per_launch": flops_launch},
         "gpu_launches": a.steps * b.launches_per_call,
         "plain": plain,
+        "accuracy": accuracy,
         "clocks": clk.summary(),
         "wire_status_ok": bool((status == 0).all()),
     }
