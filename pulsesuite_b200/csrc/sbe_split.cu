@@ -9,7 +9,7 @@
 // tensor cores):
 //     t = V / VS  (|t| < 1/2),    254 t  ~ a1 + a2/254 + a3/254^2
 //     x' = x * sc (|x'| < 1/2),   254 x' ~ b1 + b2/254 + b3/254^2
-// with int8 digits in [-127, 127], VS a power of two and sc a power of two
+// with int8 digits in [-127, 127], VS just above twice the largest |V| and sc a power of two
 // per X column (wire, variable) chosen each stage from the column's largest
 // value.  The products of digit weight i + j <= 4,
 //     D2 = sum a1 b1,  D3 = sum a1 b2 + a2 b1,  D4 = sum a1 b3 + a2 b2 + a3 b1,
@@ -387,7 +387,7 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   const double* Eh = blk + 4 * nk;
 
   // ---- set-up ---------------------------------------------------------------
-  // VS: the power of two with max V < VS / 2, so |t| < 1/2.
+  // VS: just above 2 max V, so |t| < 1/2.
   __shared__ double vmax_w[kThreadsS / 32];
   double vm = 0.0;
   for (int qq = 1 + tid; qq < nk; qq += kThreadsS) vm = fmax(vm, fabs(blk[qq]));
@@ -458,10 +458,12 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   double vmax = 0.0;
 #pragma unroll
   for (int i = 0; i < kThreadsS / 32; ++i) vmax = fmax(vmax, vmax_w[i]);
-  int ex = 0;
-  frexp(vmax > 0.0 ? vmax : 1.0, &ex);  // vmax < 2^ex
-  const double VS = ldexp(1.0, ex + 1);
-  const double inv_VS = ldexp(1.0, -ex - 1);
+  // V is static, so its scale needs no headroom: VS = 2 vmax (1 + 2^-20)
+  // puts the largest |t| just below 1/2 and uses the full digit range (a
+  // power-of-two scale would leave up to a factor 2 of the precision
+  // unused; the static representation error of V drifts the phase of p)
+  const double VS = vmax > 0.0 ? 2.0 * vmax * (1.0 + 0x1p-20) : 1.0;
+  const double inv_VS = 1.0 / VS;
   // Digit-quad tables: word(d) = bytes (a(d), a(d-1), a(d-2), a(d-3)) of one
   // digit plane for d in [dlo, dlo + ntab_words), a(d) = digit of
   // V(|d|)/VS (0 at d = 0 and outside the grid).
