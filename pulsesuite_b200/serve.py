@@ -241,7 +241,8 @@ class Server:
         # one lane per size class: its own stream, its own ticks, its own
         # queue and pinned staging ring (per-tick metadata goes through one
         # asynchronous copy; the ring is deeper than the ticks allowed in
-        # flight, so a buffer is never rewritten while its copy may pend)
+        # flight, so a buffer is never rewritten while its copy may pend).
+        #
         # The lanes' streams get priorities by grid size, the largest grid
         # highest: its CTAs run longest and set the tail (and the p99), so
         # when SMs free up the CTA scheduler gives them to it first.
