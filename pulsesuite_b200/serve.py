@@ -257,7 +257,6 @@ class Server:
                 ti, nk, torch.cuda.Stream(priority=prio),
                 [torch.empty(nb, dtype=torch.uint8, pin_memory=True) for _ in range(self.ring)],
                 [torch.empty(nb, dtype=torch.uint8, device="cuda") for _ in range(self.ring)]))
-        self._w_now = {}  # split form: wires per CTA of each class, this round
         self.tick = 0     # lane ticks issued, all lanes
         self.active = {}  # global slot -> [request, steps_done, admitted_time, nbytes]
         self.steps_done = np.zeros(self.nslots, dtype=np.int64)  # per slot, of its solve
@@ -277,8 +276,6 @@ class Server:
             self.waiting = []
             self.slots = set()
             self.inflight = []
-            self.fin = []         # finished solves not gathered yet
-            self.last_gather = 0  # lane tick of the last gather
 
     # -- staging -------------------------------------------------------------------
     class _Stage:
@@ -343,48 +340,44 @@ class Server:
 
     def _tick(self, lane, now):
         """Admit, advance and retire one size class by ``chunk`` steps, all
-        on the lane's stream.  Returns False when the lane has nothing to do.
-
-        Finished solves leave the launches at once (their state and records
-        stay as they are) and are gathered in batches: every few ticks, when
-        many are waiting, or when the lane runs empty; a slot returns to the
-        pool only after its solve has been collected."""
+        on the lane's stream.  Returns False when the lane has nothing to do."""
         torch = self.torch
         i = lane.tick % self.ring
         st = Server._Stage(lane.stage_h[i], lane.stage_d[i])
         adm = self._admit(lane, now, st)
-        if not lane.slots and not lane.fin:
+        if not lane.slots:
             return False
-        nk, ti = lane.nk, lane.ti
         slots = np.fromiter(sorted(lane.slots), dtype=np.int64)
-        fin = slots[:0]
-        if slots.size:
-            done = self.steps_done[slots]
-            r_idx = st.add(slots)
-            r_val = st.add(slots * self.max_steps + done)  # P(t) records append
-            # solves that finish with this tick
-            fin = slots[done + self.chunk >= self.steps_req[slots]]
-            if self.form == "split":
-                wg = self._w_now.get(nk, 4)
-                ng = (slots.size + wg - 1) // wg
-                grp = np.zeros(ng, dtype=abi.SPLIT_GROUP_DTYPE)
-                grp["table"] = ti
-                grp["wire"] = -1
-                padded = np.full(ng * wg, -1, dtype=np.int32)
-                padded[:slots.size] = slots
-                grp["wire"][:, :wg] = padded.reshape(ng, wg)
-                grp["nw"] = wg
-                grp["nw"][-1] = slots.size - (ng - 1) * wg
-                r_grp, n_launch = st.add(grp), ng
-            else:
-                wg = 0
-                r_grp, n_launch = st.add(slots.astype(np.int32)), slots.size
-        pending = lane.fin + [int(g) for g in fin]
-        gather = bool(pending) and (len(pending) >= 32 or lane.tick - lane.last_gather >= 3
-                                    or slots.size == fin.size)
-        if gather:
-            r_fin = st.add(np.asarray(pending, dtype=np.int64))
-            r_foff = st.add(np.asarray([self.slot_off[g] for g in pending], dtype=np.int64))
+        done = self.steps_done[slots]
+        r_idx = st.add(slots)
+        r_val = st.add(slots * self.max_steps + done)  # P(t) records append
+        # solves that finish with this tick
+        fin = slots[done + self.chunk >= self.steps_req[slots]]
+        r_fin = r_foff = None
+        if fin.size:
+            r_fin = st.add(fin)
+            r_foff = st.add(np.asarray([self.slot_off[g] for g in fin], dtype=np.int64))
+        nk, ti = lane.nk, lane.ti
+        if self.form == "split":
+            # the classes share the SMs, so the choice sees every lane's load
+            counts = {ln.nk: len(ln.slots) for ln in self.lanes}
+            wg = choose_wires_per_cta(counts, self.sms, lambda n: n <= self.w8_max)[nk]
+            ng = (slots.size + wg - 1) // wg
+            grp = np.zeros(ng, dtype=abi.SPLIT_GROUP_DTYPE)
+            grp["table"] = ti
+            grp["wire"] = -1
+            padded = np.full(ng * wg, -1, dtype=np.int32)
+            padded[:slots.size] = slots
+            grp["wire"][:, :wg] = padded.reshape(ng, wg)
+            grp["nw"] = wg
+            grp["nw"][-1] = slots.size - (ng - 1) * wg
+            r_grp, n_launch = st.add(grp), ng
+        else:
+            wg = 0
+            r_grp, n_launch = st.add(slots.astype(np.int32)), slots.size
+        common = (self.device.ptr(self.d_tables), len(self.h_tables), self.device.ptr(self.tabdata),
+                  self.tabdata.numel(), self.device.ptr(self.d_wires), self.nslots)
+        dt = float(self.active[int(slots[0])][0].dt)
         sm = lane.stream
         with torch.cuda.stream(sm):
             st.push()
@@ -393,34 +386,23 @@ class Server:
                 idx = st.view(r_sl, torch.int64)
                 self._wires_rows[idx] = st.view(r_rec, torch.uint8).view(k, self.isz)
                 self.y.index_fill_(0, self._rows(st.view(r_off, torch.int64), nk), 0.0)
-            if slots.size:
-                self._wires_i64[st.view(r_idx, torch.int64), self._p_off_col] = st.view(r_val, torch.int64)
-                common = (self.device.ptr(self.d_tables), len(self.h_tables),
-                          self.device.ptr(self.tabdata), self.tabdata.numel(),
-                          self.device.ptr(self.d_wires), self.nslots)
-                dt = float(self.active[int(slots[0])][0].dt)
-                ptr = self.device.ptr(st.view(r_grp, torch.uint8))
-                if self.form == "split":
-                    self._lib.call("psb_rk4_split", *common, ptr, n_launch, wg, nk,
-                                   self.device.ptr(self.y), self.n_state, self.device.ptr(self.ws),
-                                   self.ws.numel(), self.chunk, dt, self.device.ptr(self.P),
-                                   self.P.shape[0], 1, self.max_steps, abi.as_ptr(self.model),
-                                   self.device.stream_ptr(sm))
-                else:
-                    flags = abi.PSB_TAB_SHARED_V if (self.h_tables["flags"][ti] & abi.PSB_TAB_SHARED_V) else 0
-                    self._lib.call("psb_rk4_f64", *common, ptr, n_launch, self.device.ptr(self.y),
-                                   self.n_state, nk, flags, self.chunk, dt, self.device.ptr(self.P),
-                                   self.P.shape[0], 1, self.max_steps, abi.as_ptr(self.model),
-                                   self.device.stream_ptr(sm))
-                self.steps_done[slots] += self.chunk
-            for g in fin:
-                lane.slots.discard(int(g))
-            if gather:
-                self._retire(lane, pending, st.view(r_fin, torch.int64), st.view(r_foff, torch.int64))
-                lane.fin = []
-                lane.last_gather = lane.tick
+            self._wires_i64[st.view(r_idx, torch.int64), self._p_off_col] = st.view(r_val, torch.int64)
+            ptr = self.device.ptr(st.view(r_grp, torch.uint8))
+            if self.form == "split":
+                self._lib.call("psb_rk4_split", *common, ptr, n_launch, wg, nk,
+                               self.device.ptr(self.y), self.n_state, self.device.ptr(self.ws),
+                               self.ws.numel(), self.chunk, dt, self.device.ptr(self.P),
+                               self.P.shape[0], 1, self.max_steps, abi.as_ptr(self.model),
+                               self.device.stream_ptr(sm))
             else:
-                lane.fin = pending
+                flags = abi.PSB_TAB_SHARED_V if (self.h_tables["flags"][ti] & abi.PSB_TAB_SHARED_V) else 0
+                self._lib.call("psb_rk4_f64", *common, ptr, n_launch, self.device.ptr(self.y),
+                               self.n_state, nk, flags, self.chunk, dt, self.device.ptr(self.P),
+                               self.P.shape[0], 1, self.max_steps, abi.as_ptr(self.model),
+                               self.device.stream_ptr(sm))
+            self.steps_done[slots] += self.chunk
+            if fin.size:
+                self._retire(lane, fin, st.view(r_fin, torch.int64), st.view(r_foff, torch.int64))
             ev = torch.cuda.Event()
             ev.record(sm)
         lane.inflight.append(ev)
@@ -434,6 +416,8 @@ class Server:
         memory on the copy stream."""
         torch = self.torch
         entries = [(int(g), *self.active.pop(int(g))) for g in fin]
+        for g in fin:
+            lane.slots.discard(int(g))
         rows = self._rows(foff_t, lane.nk)
         Pg = self.P.view(self.nslots, self.max_steps, 2).index_select(0, fin_t)
         yg = self.y.index_select(0, rows)
@@ -506,17 +490,11 @@ class Server:
                 by_nk[queue[qi].nk].waiting.append(queue[qi])
                 qi += 1
             self._collect()
-            if self.form == "split":
-                # wires per CTA for this round's ticks (the classes share the
-                # SMs, so the choice sees every lane's load)
-                self._w_now = choose_wires_per_cta(
-                    {ln.nk: len(ln.slots) + len(ln.waiting) for ln in self.lanes}, self.sms,
-                    lambda nk: nk <= self.w8_max)
             issued = False
             for lane in order:
                 while lane.inflight and lane.inflight[0].query():
                     lane.inflight.pop(0)
-                if len(lane.inflight) < max_inflight_ticks and (lane.slots or lane.waiting or lane.fin):
+                if len(lane.inflight) < max_inflight_ticks and (lane.slots or lane.waiting):
                     issued |= self._tick(lane, now)
             if issued:
                 continue
