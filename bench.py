@@ -475,12 +475,20 @@ def run_serve(a):
     # saturated capacity of both forms on the same mix (all requests queued)
     cap = {}
     sat = serve.poisson_stream(rate=1e6, seconds=a.capacity_requests / 1e6, seed=5, chunk=chunk)
+    # (one saturated run lasts about a second and varies by up to ~20 % from
+    # run to run, so each form reports the median of three)
+    cap_runs = {}
     for form in ("split", "plain"):
-        s2 = serve.Server(form=form, chunk=chunk)
-        s2.run(warm, realtime=False)
-        s2.run(sat, realtime=False)
-        cap[form] = s2.throughput()
-        del s2
+        vals = []
+        for _ in range(3):
+            s2 = serve.Server(form=form, chunk=chunk)
+            s2.run(warm, realtime=False)
+            s2.run(sat, realtime=False)
+            vals.append(s2.throughput())
+            del s2
+            torch.cuda.synchronize()
+        cap[form] = float(np.median(vals))
+        cap_runs[form] = vals
     h2d = 136 * len(res)
     d2h = sum(16 * r.nsteps + 32 * r.nk for r in res)
     line = {
@@ -504,7 +512,7 @@ def run_serve(a):
         "latency_p99_s": lat.get(99),
         "capacity": {"split": cap["split"], "plain": cap["plain"],
                      "split_over_plain": cap["split"] / cap["plain"],
-                     "requests": len(sat)},
+                     "requests": len(sat), "runs": cap_runs, "statistic": "median of 3"},
         "e2e": {"value": thr, "unit": "wire*k*steps/s", "h2d_bytes_per_step": h2d / max(1, len(res)),
                 "d2h_bytes_per_step": d2h / max(1, len(res))},
         "roofline": None,
