@@ -37,6 +37,13 @@ REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
 L2_FLUSH_BYTES = 256 << 20
+# DRAM bytes per state element and launch, from one ncu capture of each step
+# kernel on a small configuration-3 case (dram__bytes_read.sum +
+# dram__bytes_write.sum over 1184 x 256 elements; traffic grows with the
+# elements a launch advances, not with its time steps)
+DRAM_BYTES_PER_ELEMENT = {"split": 9.99e6 / (1184 * 256), "plain": 9.91e6 / (1184 * 256)}
+TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + write.sum of the step kernels on 1184 wires x "
+                  "Nk 256, per element, times the elements of this step's launches")
 METRIC = "SBE wire*k*steps/s at <=1e-6 rel err vs FP64 (batched vs plain); p50/p99 latency"
 
 
@@ -373,6 +380,10 @@ def run_ours(a):
         peak, peak_source = 2.0 * peak, "2 x " + peak_source
         bound = "tensor"
     achieved = flops_launch / (avg_launch_ms * 1e-3) / 1e12
+    # DRAM bytes of one bench step's launches, scaled by elements from the
+    # ncu captures of a small c3 case (split 9.99 MB, plain 9.91 MB for
+    # 1184 x 256 elements: the FP64 state read once per launch)
+    traffic = (DRAM_BYTES_PER_ELEMENT[a.form] * b.n_state) if b.n_state else None
 
     line = {
         "metric": METRIC,
@@ -394,8 +405,8 @@ def run_ours(a):
         "e2e": {"value": units * a.steps * world / (e2e_ms * 1e-3), "unit": "wire*k*steps/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "roofline": {"bound": bound, "achieved": achieved, "peak": peak, "unit": "TFLOP/s" if a.form == "plain" else "TOP/s",
-                     "frac": achieved / peak, "traffic": None, "peak_source": peak_source,
-                     "flops_per_launch": flops_launch},
+                     "frac": achieved / peak, "traffic": traffic, "traffic_source": TRAFFIC_SOURCE,
+                     "peak_source": peak_source, "flops_per_launch": flops_launch},
         "gpu_launches": a.steps * b.launches_per_call,
         "plain": plain,
         "accuracy": accuracy,
