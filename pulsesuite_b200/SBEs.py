@@ -2,7 +2,7 @@
 
 Drop-in for the kernel-level signatures of pulsesuite's ``SBEs`` module when
 the states p, C, D and the drive are diagonal in k (a k-independent field
-along the wire, the case the north-star configurations run):
+along the wire, the case of the batched configurations):
 
     configure(Ee, Eh, gap, excitons=True, lf=False, freepot=False)  # module state
     CalcH(Meh, Wee, Whh, C, D, p, VC, Heh, Hee, Hhh)   # in place (SBEs.py:669)

@@ -233,7 +233,7 @@ def rwa_case(nk, nsteps, theta=0.5 * np.pi, fwhm=50e-15, T2=100e-15, det_meV=0.0
 
 
 def make_rk4(R, out, name, case):
-    """Oracle A: reference RHS kernels + reference rk4_dpc (SURVEY harness)."""
+    """Oracle A: reference RHS kernels + reference rk4_dpc (the diagonal-drive harness)."""
     g = case["g"]
     nk = g.nk
     S = R.SBEs

@@ -41,7 +41,7 @@ def test_ctypes_signatures_cover_header():
     assert set(declared()) <= set(_lib._SIGNATURES)
 
 
-def test_struct_layouts_match_c():
+def test_struct_layouts_match_c(tmp_path):
     prog = r'''
 #include <stdio.h>
 #include <stddef.h>
@@ -55,8 +55,7 @@ int main(void) {
   return 0;
 }
 '''
-    tmp = os.path.join(REPO, "_work", "abi_layout")
-    os.makedirs(os.path.dirname(tmp), exist_ok=True)
+    tmp = str(tmp_path / "abi_layout")
     with open(tmp + ".c", "w") as f:
         f.write(prog)
     r = subprocess.run(["gcc", "-I", os.path.join(REPO, "include"), "-o", tmp, tmp + ".c"],
