@@ -191,14 +191,19 @@ __device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t* r) {
 // (Values outside the range give meaningless digits; the callers detect
 // them and re-digitise the column with a wider scale.)
 __device__ __forceinline__ void digits3(float v, int& d1, int& d2, int& d3) {
-  const float f1 = rintf(v * 254.f);
-  const float r1 = fmaf(v, 254.f, -f1);
-  const float f2 = rintf(r1 * 254.f);
-  const float r2 = fmaf(r1, 254.f, -f2);
-  const float f3 = rintf(r2 * 254.f);
-  d1 = (int)f1;
-  d2 = (int)f2;
-  d3 = (int)f3;
+  // x + 1.5 * 2^23 rounds x (|x| < 2^22) to the nearest integer in one FMA
+  // rounding, and that integer is the sum's bit pattern less the constant's:
+  // plain FP32 and integer arithmetic instead of a conversion per digit.
+  constexpr float kMagic = 12582912.f;
+  constexpr int kMagicBits = 0x4B400000;
+  const float t1 = fmaf(v, 254.f, kMagic);
+  const float r1 = fmaf(v, 254.f, -(t1 - kMagic));
+  const float t2 = fmaf(r1, 254.f, kMagic);
+  const float r2 = fmaf(r1, 254.f, -(t2 - kMagic));
+  const float t3 = fmaf(r2, 254.f, kMagic);
+  d1 = __float_as_int(t1) - kMagicBits;
+  d2 = __float_as_int(t2) - kMagicBits;
+  d3 = __float_as_int(t3) - kMagicBits;
 }
 
 // One step of a halving max-butterfly over a warp: each lane holds C
