@@ -179,10 +179,14 @@ def default_capacity(nks=C4_NKS):
 
 
 class Server:
-    """Device slot pool + tick loop (see module docstring)."""
+    """Device slot pool + tick loop (see module docstring).
+
+    max_inflight_ticks: ticks a lane may have queued on its stream before
+    the host waits for the oldest (2: lower latency; 3 measured the same
+    saturated capacity within the run-to-run spread)."""
 
     def __init__(self, form="split", chunk=50, max_steps=4000, capacity=None,
-                 hbm_budget=150e9, nks=C4_NKS):
+                 hbm_budget=150e9, nks=C4_NKS, max_inflight_ticks=2):
         import torch
         from scipy.constants import hbar
 
@@ -246,7 +250,8 @@ class Server:
         # The lanes' streams get priorities by grid size, the largest grid
         # highest: its CTAs run longest and set the tail (and the p99), so
         # when SMs free up the CTA scheduler gives them to it first.
-        self.ring = 3
+        self.max_inflight = int(max_inflight_ticks)  # queued ticks per lane
+        self.ring = self.max_inflight + 1
         self.lanes = []
         least, greatest = torch.cuda.Stream.priority_range()
         rank = {nk: r for r, nk in enumerate(sorted(self.nks, reverse=True))}
@@ -462,7 +467,7 @@ class Server:
                 self.pool.give_back(req.nk, g - self.cls_base[req.nk], nbytes)
         self.pending = keep
 
-    def run(self, requests, realtime=True, max_inflight_ticks=2):
+    def run(self, requests, realtime=True, max_inflight_ticks=None):
         """Serve ``requests``.  realtime: arrivals are honoured on the wall
         clock (the Poisson stream), else every request is available from the
         start (throughput / capacity runs).
@@ -472,6 +477,8 @@ class Server:
         solve advances at its own kernel's pace instead of waiting each tick
         for the largest grid; the classes' launches run concurrently on the
         GPU.  Largest grids are served first in each round."""
+        if max_inflight_ticks is None:
+            max_inflight_ticks = self.max_inflight
         assert max_inflight_ticks < self.ring
         queue = sorted(requests, key=lambda r: r.arrival)
         for req in queue:
