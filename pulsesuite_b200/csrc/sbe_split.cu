@@ -78,7 +78,6 @@ constexpr int kThreadsS = 32 * 13;
 constexpr int kEpiThreads = 32 * kEpiWarps;
 constexpr int kTileRows = 128;  // M of one MMA
 constexpr int kTileK = 64;      // k' per A tile
-constexpr int kKStep = 32;      // K of one kind::i8 MMA
 constexpr int kDigits = 3;
 constexpr int kPlaneCols = kTileK / 4;            // TMEM columns of one digit plane of a tile
 constexpr int kTileCols = kDigits * kPlaneCols;   // 48
