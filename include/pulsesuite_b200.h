@@ -6,7 +6,7 @@
  * each entry point below names the reference interface it replaces
  * (file:line, paths relative to the reference project's src/pulsesuite).
  * The Python facade (pulsesuite_b200/SBEs.py, coulomb.py) binds these with
- * ctypes, as a maintainer of the reference would.
+ * ctypes, the way a maintainer of the reference would bind them.
  *
  * Conventions
  *   - Every function returns PSB_OK (0) or a negative PSB_ERR_* code and never
@@ -253,7 +253,8 @@ int psb_f64_smem_bytes(int nk, int tab_flags);
  */
 #define PSB_SPLIT_WMAX 16
 /* One CTA's work: 1..wgroup wires of one table (same k grid); wire slots
- * past nw are ignored. */
+ * past nw are ignored.  wgroup is 4, 8 or 16 (wider groups make every MMA
+ * wider at the same issue cost; 16 needs nk <= psb_split_max_nk(16)). */
 typedef struct PsbSplitGroup {
   int32_t table;
   int32_t nw;
@@ -262,10 +263,10 @@ typedef struct PsbSplitGroup {
 
 /* Workspace bytes psb_rk4_split needs for n_state elements. */
 int64_t psb_split_ws_bytes(int64_t n_state);
-/* Dynamic shared memory (bytes) of one CTA for a grid of nk, wgroup 4 or 8
- * (the layout psb_rk4_split picks for nkmax = nk). */
+/* Dynamic shared memory (bytes) of one CTA for a grid of nk, wgroup 4, 8
+ * or 16 (the layout psb_rk4_split picks for nkmax = nk). */
 int psb_split_smem_bytes(int nk, int wgroup);
-/* Largest nk a group of wgroup (4 or 8) wires supports. */
+/* Largest nk a group of wgroup (4, 8 or 16) wires supports. */
 int psb_split_max_nk(int wgroup);
 /* Largest nk for which the stage state of a group stays resident in shared
  * memory for the whole call (faster; larger grids keep it in the workspace). */
@@ -273,7 +274,7 @@ int psb_split_max_nk_resident(int wgroup);
 /*
  * nsteps RK4 steps of every group (one CTA each), same contract as
  * psb_rk4_f64 (state, t, steps, status, P(t) records) for the wires of
- * d_groups[0..ngroups).  wgroup (4 or 8) is the group capacity compiled
+ * d_groups[0..ngroups).  wgroup (4, 8 or 16) is the group capacity compiled
  * for; nkmax the largest grid among the groups (<= psb_split_max_nk(wgroup)).
  * d_ws: caller-allocated workspace of psb_split_ws_bytes(n_state) bytes,
  * 32-byte aligned (stage state and RK accumulator per element).  On
@@ -303,7 +304,10 @@ int psb_rk4_split(const PsbTable* d_tables, int ntab, const double* d_tabdata, i
  * no cudaMalloc, cudaFree or allocating library call.
  * - The first call on a device looks up the array's device address
  *   (cudaGetSymbolAddress) with that device current; make that first call
- *   before any stream capture.
+ *   before any stream capture.  The address is cached per device and looked
+ *   up again when the calling context changes; resetting the device
+ *   (cudaDeviceReset) between calls is not supported, since a new primary
+ *   context may reuse the old handle and leave the cached address stale.
  * - All calls share the array, and it keeps what the last call wrote.  The
  *   kernel writes every workspace element before reading it, so nothing
  *   needs to start at zero.  Calls whose kernels overlap on the GPU (other

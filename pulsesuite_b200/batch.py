@@ -30,7 +30,7 @@ class WireBatch:
         if form not in ("plain", "split"):
             raise ValueError("form must be 'plain' or 'split'")
         self.form = form
-        # split form: wires per CTA group by grid size, {nk: 4 or 8}; grids
+        # split form: wires per CTA group by grid size, {nk: 4, 8 or 16}; grids
         # not listed use the built-in rule (see _setup_split)
         self.split_w = dict(split_w or {})
         self.grids = list(grids)
@@ -88,11 +88,11 @@ class WireBatch:
     def _setup_split(self):
         """Wire groups (one CTA each) and the workspace of the split form.
 
-        A group holds up to W in {4, 8} wires of one grid.  The exchange work
-        of a group per step is ~W Nk^2, so W is chosen per grid to give
+        A group holds up to W in {4, 8, 16} wires of one grid.  The exchange
+        work of a group per step is ~W Nk^2, so W is chosen per grid to give
         roughly two waves of equal CTAs over the SMs (W = 4 for large grids,
-        W = 8 once a grid has enough wires: the MMAs are twice as wide at the
-        same issue cost).  Groups are launched in classes of (W, state
+        wider groups once a grid has enough wires: the MMAs are twice as wide
+        at the same issue cost).  Groups are launched in classes of (W, state
         resident in shared memory or not) so that a large grid does not push
         the small ones out of the resident layout; the classes run
         concurrently on side streams, the one with the largest grid first."""
@@ -101,8 +101,8 @@ class WireBatch:
         if ((f & need) != need).any() or (f & abi.PSB_TAB_SCREENED).any():
             raise _lib.PsbError("split form needs unscreened tables with Veh == Vee == Vhh")
         lib = _lib.load()
-        maxnk = {wg: int(lib.psb_split_max_nk(wg)) for wg in (4, 8)}
-        resnk = {wg: int(lib.psb_split_max_nk_resident(wg)) for wg in (4, 8)}
+        maxnk = {wg: int(lib.psb_split_max_nk(wg)) for wg in (4, 8, 16)}
+        resnk = {wg: int(lib.psb_split_max_nk_resident(wg)) for wg in (4, 8, 16)}
         nks = self.h_tables["nk"].astype(np.int64)
         counts = np.bincount(self.h_wires["table"], minlength=len(nks))
         sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
@@ -113,12 +113,14 @@ class WireBatch:
             if counts[t] == 0:
                 continue
             wg = 4
-            if nk <= maxnk[8] and 8 * nk * nk <= max(target, 4 * nk * nk):
-                wg = 8
+            for cand in (16, 8):
+                if nk <= maxnk[cand] and cand * nk * nk <= max(target, 4 * nk * nk):
+                    wg = cand
+                    break
             if nk in self.split_w:
                 wg = int(self.split_w[nk])
-                if wg not in (4, 8):
-                    raise ValueError("split_w values must be 4 or 8")
+                if wg not in (4, 8, 16):
+                    raise ValueError("split_w values must be 4, 8 or 16")
             if nk > maxnk[wg]:
                 raise _lib.PsbError(f"split form: nk {nk} exceeds the supported maximum")
             key = (wg, nk <= resnk[wg])

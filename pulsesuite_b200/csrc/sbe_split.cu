@@ -32,7 +32,7 @@
 // stage point, the RK accumulator and an FP32 copy of y in FP32, the state y
 // and the P(t) sums in FP64.
 //
-// One CTA owns a group of W (4 or 8) wires for all `nsteps` RK4 steps,
+// One CTA owns a group of W (4, 8 or 16) wires for all `nsteps` RK4 steps,
 // 128-row tiles of k at a time:
 //   * X (the MMA B operand: three int8 digit planes, K-major, N = 4W
 //     columns) lives in shared memory, double buffered: stage s reads
@@ -323,7 +323,7 @@ struct Layout {
 // The kernel.
 // ---------------------------------------------------------------------------
 template <int W, bool RES>
-__global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
+__global__ void __maxnreg__(152) split_rk4_kernel(Args a) {
   constexpr int N = 4 * W;
   constexpr int WH = W / 2;  // wires per drain/epilogue warp
   extern __shared__ __align__(1024) uint8_t smem[];
@@ -506,12 +506,20 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   // in all, not 5 per column; afterwards lane L holds column
   // (L >> (5 - m)) & (4 WH - 1), m = log2(4 WH).
   auto publish_colmax = [&](const float* cm) {
-    constexpr int C = 4 * WH;  // 8 or 16
-    static_assert(C == 8 || C == 16, "column count of a drain warp");
+    constexpr int C = 4 * WH;  // 8, 16 or 32
+    static_assert(C == 8 || C == 16 || C == 32, "column count of a drain warp");
     float v[C];
 #pragma unroll
     for (int c = 0; c < C; ++c) v[c] = cm[c];
-    if constexpr (C == 16) {
+    if constexpr (C == 32) {
+      // five halvings leave lane L with column L
+      colmax_halve<32>(v, 16, lane);
+      colmax_halve<16>(v, 8, lane);
+      colmax_halve<8>(v, 4, lane);
+      colmax_halve<4>(v, 2, lane);
+      colmax_halve<2>(v, 1, lane);
+      colmax[q * N + 4 * w0 + lane] = v[0];
+    } else if constexpr (C == 16) {
       colmax_halve<16>(v, 16, lane);
       colmax_halve<8>(v, 8, lane);
       colmax_halve<4>(v, 4, lane);
@@ -1015,8 +1023,11 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   if (warp == kMmaWarp && lane == 0) {
     // every MMA this thread issued has completed before TMEM is released
     umma_commit(final_bar);
-    for (uint32_t i = 0; i < kSpinLimit; ++i)
-      if (mbar_try_wait(final_bar, 0)) break;
+    bool done = false;
+    for (uint32_t i = 0; i < kSpinLimit && !done; ++i) done = mbar_try_wait(final_bar, 0);
+    // MMAs still in flight after the bounded wait: the wires' results are
+    // not trustworthy, so they report PSB_ERR_TIMEOUT
+    if (!done) *abort = 1;
   }
   __syncwarp();
   tc_fence_before();
@@ -1082,26 +1093,34 @@ extern "C" int64_t psb_split_ws_bytes(int64_t n_state) {
 }
 
 extern "C" int psb_split_max_nk(int wgroup) {
+  if (wgroup == 16) return split::max_nk<16, false>();
   if (wgroup == 8) return split::max_nk<8, false>();
   if (wgroup == 4) return split::max_nk<4, false>();
-  return set_error(PSB_ERR_INVALID, "wgroup must be 4 or 8");
+  return set_error(PSB_ERR_INVALID, "wgroup must be 4, 8 or 16");
 }
 
 extern "C" int psb_split_max_nk_resident(int wgroup) {
+  if (wgroup == 16) return split::max_nk<16, true>();
   if (wgroup == 8) return split::max_nk<8, true>();
   if (wgroup == 4) return split::max_nk<4, true>();
-  return set_error(PSB_ERR_INVALID, "wgroup must be 4 or 8");
+  return set_error(PSB_ERR_INVALID, "wgroup must be 4, 8 or 16");
 }
+
+namespace psb {
+namespace split {
+template <int W>
+int smem_bytes(int nk) {
+  return (int)(nk <= max_nk<W, true>() ? Layout<W, true>(nk).total : Layout<W, false>(nk).total);
+}
+}  // namespace split
+}  // namespace psb
 
 extern "C" int psb_split_smem_bytes(int nk, int wgroup) {
   if (nk < 2 || nk > PSB_MAX_NK) return set_error(PSB_ERR_SIZE, "nk %d out of range", nk);
-  if (wgroup == 8)
-    return (int)(nk <= split::max_nk<8, true>() ? split::Layout<8, true>(nk).total
-                                                 : split::Layout<8, false>(nk).total);
-  if (wgroup == 4)
-    return (int)(nk <= split::max_nk<4, true>() ? split::Layout<4, true>(nk).total
-                                                 : split::Layout<4, false>(nk).total);
-  return set_error(PSB_ERR_INVALID, "wgroup must be 4 or 8");
+  if (wgroup == 16) return split::smem_bytes<16>(nk);
+  if (wgroup == 8) return split::smem_bytes<8>(nk);
+  if (wgroup == 4) return split::smem_bytes<4>(nk);
+  return set_error(PSB_ERR_INVALID, "wgroup must be 4, 8 or 16");
 }
 
 extern "C" int psb_rk4_split(const PsbTable* d_tables, int ntab, const double* d_tabdata,
@@ -1113,8 +1132,8 @@ extern "C" int psb_rk4_split(const PsbTable* d_tables, int ntab, const double* d
   if (!d_tables || !d_tabdata || !d_wires || !d_groups || !d_y || !d_ws || !model || ntab <= 0 ||
       nw < 0 || ngroups < 0)
     return set_error(PSB_ERR_INVALID, "psb_rk4_split: null pointer or bad count");
-  if (wgroup != 4 && wgroup != 8)
-    return set_error(PSB_ERR_INVALID, "psb_rk4_split: wgroup must be 4 or 8");
+  if (wgroup != 4 && wgroup != 8 && wgroup != 16)
+    return set_error(PSB_ERR_INVALID, "psb_rk4_split: wgroup must be 4, 8 or 16");
   if (nkmax < 2 || nkmax > psb_split_max_nk(wgroup))
     return set_error(PSB_ERR_SIZE, "psb_rk4_split: nkmax %d too large for wgroup %d", nkmax,
                      wgroup);
@@ -1147,6 +1166,7 @@ extern "C" int psb_rk4_split(const PsbTable* d_tables, int ntab, const double* d
   a.p_cap = p_cap;
   a.hbar = model->hbar;
   cudaStream_t st = (cudaStream_t)stream;
+  if (wgroup == 16) return split::launch<16>(a, nkmax, st);
   return wgroup == 8 ? split::launch<8>(a, nkmax, st) : split::launch<4>(a, nkmax, st);
 }
 
@@ -1154,7 +1174,11 @@ extern "C" int psb_rk4_split(const PsbTable* d_tables, int ntab, const double* d
 // psb_rk4_split without a caller workspace: the workspace is one file-scope
 // device array (held by every GPU that loads the library).  Host code only
 // sees a host-side stand-in under the array's name, so its device address
-// is looked up once per device with cudaGetSymbolAddress and cached.
+// is looked up once per device with cudaGetSymbolAddress and cached,
+// together with the context it was looked up in: a call from another
+// context of that device looks it up again.  (A device reset that gives the
+// new primary context the old handle is not detected: resetting a device
+// between calls is not supported.)
 // ---------------------------------------------------------------------------
 #include <mutex>
 
@@ -1163,7 +1187,28 @@ namespace split {
 static __device__ __align__(256) uint8_t g_noalloc_ws[PSB_SPLIT_NOALLOC_SCRATCH_BYTES];
 constexpr int kMaxDevices = 64;
 static void* g_noalloc_ptr[kMaxDevices] = {};
+static void* g_noalloc_ctx[kMaxDevices] = {};
 static std::mutex g_noalloc_mu;
+
+// The current driver context (CUcontext as void*), or null when the driver
+// entry point is unavailable; fetched through the runtime, so the library
+// does not link the driver library.  Called with g_noalloc_mu held.
+static void* current_context() {
+  typedef int (*CtxGetCurrent)(void**);
+  static CtxGetCurrent fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<CtxGetCurrent>(p);
+  }
+  void* ctx = nullptr;
+  if (fn && fn(&ctx) != 0) ctx = nullptr;
+  return ctx;
+}
 
 // Device address of g_noalloc_ws on the current device (set-up on first use).
 static int noalloc_scratch(void** out) {
@@ -1174,13 +1219,15 @@ static int noalloc_scratch(void** out) {
   if (dev < 0 || dev >= kMaxDevices)
     return set_error(PSB_ERR_UNSUPPORTED, "device ordinal %d beyond %d", dev, kMaxDevices);
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
+  const void* ctx = current_context();
+  if (!g_noalloc_ptr[dev] || ctx != g_noalloc_ctx[dev]) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_ws);
     if (e != cudaSuccess || !p)
       return set_error(PSB_ERR_CUDA, "cudaGetSymbolAddress(workspace): %s",
                        cudaGetErrorString(e));
     g_noalloc_ptr[dev] = p;
+    g_noalloc_ctx[dev] = current_context();  // the lookup may have created the context
   }
   *out = g_noalloc_ptr[dev];
   return PSB_OK;
