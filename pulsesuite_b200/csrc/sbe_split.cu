@@ -323,7 +323,7 @@ struct Layout {
 // The kernel.
 // ---------------------------------------------------------------------------
 template <int W, bool RES>
-__global__ void __maxnreg__(152) split_rk4_kernel(Args a) {
+__global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   constexpr int N = 4 * W;
   constexpr int WH = W / 2;  // wires per drain/epilogue warp
   extern __shared__ __align__(1024) uint8_t smem[];
