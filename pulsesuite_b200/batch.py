@@ -91,8 +91,9 @@ class WireBatch:
         A group holds up to W in {4, 8, 16} wires of one grid.  The exchange
         work of a group per step is ~W Nk^2, so W is chosen per grid to give
         roughly two waves of equal CTAs over the SMs (W = 4 for large grids,
-        wider groups once a grid has enough wires: the MMAs are twice as wide
-        at the same issue cost).  Groups are launched in classes of (W, state
+        W = 8 once a grid has enough wires: the MMAs are twice as wide at the
+        same issue cost; W = 16 only where ``split_w`` asks for it, since its
+        epilogue runs from the workspace).  Groups are launched in classes of (W, state
         resident in shared memory or not) so that a large grid does not push
         the small ones out of the resident layout; the classes run
         concurrently on side streams, the one with the largest grid first."""
@@ -113,10 +114,8 @@ class WireBatch:
             if counts[t] == 0:
                 continue
             wg = 4
-            for cand in (16, 8):
-                if nk <= maxnk[cand] and cand * nk * nk <= max(target, 4 * nk * nk):
-                    wg = cand
-                    break
+            if nk <= maxnk[8] and 8 * nk * nk <= max(target, 4 * nk * nk):
+                wg = 8
             if nk in self.split_w:
                 wg = int(self.split_w[nk])
                 if wg not in (4, 8, 16):

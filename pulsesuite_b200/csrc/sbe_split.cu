@@ -70,12 +70,23 @@
 namespace psb {
 namespace split {
 
-constexpr int kEpiWarps = 8;    // warps 0..7: drain + epilogue
-constexpr int kGenWarp0 = 8;    // warps 8..11: A-tile generators
+constexpr int kEpiWarps = 8;    // warps 0..7: drain + epilogue (warpgroups 0, 1)
+constexpr int kGenWarp0 = 8;    // warps 8..11: A-tile generators (warpgroup 2)
 constexpr int kGenWarps = 4;
-constexpr int kMmaWarp = 12;    // warp 12: TMEM owner + MMA issuer
-constexpr int kThreadsS = 32 * 13;
+constexpr int kMmaWarp = 12;    // warp 12: TMEM owner + MMA issuer (warpgroup 3;
+                                // warps 13..15 only complete that warpgroup)
+constexpr int kThreadsS = 32 * 16;
 constexpr int kEpiThreads = 32 * kEpiWarps;
+// Registers per thread: 128 at launch (65536 / 512 threads); after the
+// set-up the generator and MMA warpgroups give theirs down to kRegsLow and
+// the two epilogue warpgroups take them: 256 kRegsHigh + 256 kRegsLow =
+// 512 * kRegsLaunch, so the increase always finds its registers.
+constexpr int kRegsLaunch = 128;
+constexpr int kRegsLow = 64;
+constexpr int kRegsHigh = 2 * kRegsLaunch - kRegsLow;  // 192
+static_assert(kEpiWarps * 32 * kRegsHigh + (kThreadsS - kEpiWarps * 32) * kRegsLow <=
+                  kThreadsS * kRegsLaunch,
+              "register split exceeds the launch allocation");
 constexpr int kTileRows = 128;  // M of one MMA
 constexpr int kTileK = 64;      // k' per A tile
 constexpr int kDigits = 3;
@@ -661,7 +672,12 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   const int total_stages = a.nsteps * 4;
   const double h = a.dt;
 
-  if (warp == kMmaWarp) {
+  // Roles.  Each warpgroup changes its register allocation once, at the top
+  // of its branch (all four warps at the same instruction): warpgroups 2
+  // and 3 down to kRegsLow, the epilogue warpgroups 0 and 1 up to kRegsHigh.
+  if (warp >= kMmaWarp) {
+    asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(kRegsLow));
+    if (warp == kMmaWarp) {
     // ---- MMA issuer -----------------------------------------------------------
     // The whole warp polls the barriers (uniform control flow) and lane 0
     // alone issues the MMAs and commits.  One thread issues every MMA, and
@@ -751,7 +767,9 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
       named_sync(1, kEpiThreads + 32);
       if (snap[s & 1]) break;
     }
+    }
   } else if (warp >= kGenWarp0) {
+    asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(kRegsLow));
     // ---- A-tile generators ------------------------------------------------------
     // Row r = 32 gq + lane of the tile for 2 mi - kj = dl is a(d0 - c),
     // c = 0..63, d0 = 64 dl + r; TMEM column j of a digit plane holds
@@ -805,6 +823,7 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
       }
     }
   } else {
+    asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(kRegsHigh));
     // ---- drain / epilogue warps -----------------------------------------------------
     uint32_t it = 0;
     const uint32_t lrow = tmem + ((uint32_t)(32 * q) << 16);
@@ -845,6 +864,29 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
         const int b = it & 1;
         // band energies of this row: loaded before the wait, which hides them
         const double ekh = k < nk ? (Ee[k] + Eh[k]) * inv_hbar : 0.0;
+        // the state inputs of this row's elements do not depend on the
+        // accumulators either: for up to four wires per warp they are all
+        // loaded here, so their latency (shared memory, or L2 for the
+        // workspace) overlaps the MMAs and each other
+        constexpr bool kPre = WH <= 4;
+        float4 in_ys[kPre ? WH : 1], in_acc[kPre ? WH : 1], in_yf[kPre ? WH : 1];
+        double4 in_y[kPre ? WH : 1];
+        if constexpr (kPre) {
+#pragma unroll
+          for (int j = 0; j < WH; ++j) {
+            const int w = w0 + j;
+            in_ys[j] = in_acc[j] = in_yf[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+            in_y[j] = make_double4(0.0, 0.0, 0.0, 0.0);
+            if (k < nk && w < grp.nw) {
+              float4* ysp; float4* accp; float4* yfp;
+              ws_ptrs(w, k, ysp, accp, yfp);
+              in_ys[j] = *ysp;
+              if (stg != 0) in_acc[j] = *accp;
+              if (stg == 1 || stg == 2) in_yf[j] = *yfp;
+              if (stg == 3) in_y[j] = RES ? s_y[w * kpad + k] : g_y[woff[w] + k];
+            }
+          }
+        }
         bool got = mbar_wait(&dfull[b], (it >> 1) & 1, abort);
         got = __all_sync(0xffffffffu, got);
         if (got) tc_fence_after();
@@ -881,7 +923,8 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
             }
             float4* ysp; float4* accp; float4* yfp;
             ws_ptrs(w, k, ysp, accp, yfp);
-            const float4 ysf = *ysp;
+            float4 ysf;
+            if constexpr (kPre) ysf = in_ys[j]; else ysf = *ysp;
             // diagonal RHS (SBEs.py:1962-1975, 2325-2337, 2623-2636) / hbar:
             // phase and dephasing terms in FP64, Rabi terms in FP32
             const float omr = Mjr + exh[0];
@@ -896,15 +939,24 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
             // RK4 stage combination (integrator.py:143-157): acc = k1 + 2 k2
             // + 2 k3 and the stage points in FP32, y += h/6 (acc + k4) in FP64
             float4 nxt;
+            float4 af, yf;
+            double4 yv;
+            if constexpr (kPre) {
+              af = in_acc[j];
+              yf = in_yf[j];
+              yv = in_y[j];
+            } else {
+              if (stg != 0) af = *accp;
+              if (stg == 1 || stg == 2) yf = *yfp;
+              if (stg == 3) yv = RES ? s_y[w * kpad + k] : g_y[woff[w] + k];
+            }
             if (stg == 0) {
               *accp = make_float4(f0, f1, f2, f2);
               // the stage-0 point is the FP32 copy of y
               nxt = make_float4(ysf.x + h2f * f0, ysf.y + h2f * f1, ysf.z + h2f * f2,
                                 ysf.w + h2f * f2);
             } else if (stg == 3) {
-              const float4 af = *accp;
               double4* yp = RES ? s_y + (w * kpad + k) : g_y + (woff[w] + k);
-              double4 yv = *yp;
               yv.x += (double)(h6f * (af.x + f0));
               yv.y += (double)(h6f * (af.y + f1));
               yv.z += (double)(h6f * (af.z + f2));
@@ -915,10 +967,8 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
               pr[j] += yv.x;
               pim[j] += yv.y;
             } else {
-              const float4 af = *accp;
               *accp = make_float4(af.x + 2.f * f0, af.y + 2.f * f1, af.z + 2.f * f2,
                                   af.w + 2.f * f2);
-              const float4 yf = *yfp;
               const float c2 = stg == 1 ? h2f : hf;
               nxt = make_float4(yf.x + c2 * f0, yf.y + c2 * f1, yf.z + c2 * f2, yf.w + c2 * f2);
             }
@@ -1067,8 +1117,20 @@ int launch_res(Args a, int nkmax, cudaStream_t s) {
   if (smem > kMaxDynSmem)
     return set_error(PSB_ERR_SIZE, "split form: nk %d does not fit a group of %d wires", nkmax,
                      W);
-  cudaError_t e = cudaFuncSetAttribute(split_rk4_kernel<W, RES>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  // the register reallocation inside the kernel assumes exactly kRegsLaunch
+  // registers per thread at launch (an increase beyond what the warpgroups
+  // gave down would never complete), so a build that differs is refused
+  cudaFuncAttributes fa{};
+  cudaError_t e = cudaFuncGetAttributes(&fa, split_rk4_kernel<W, RES>);
+  if (e != cudaSuccess)
+    return set_error(PSB_ERR_CUDA, "cudaFuncGetAttributes: %s", cudaGetErrorString(e));
+  if (fa.numRegs != kRegsLaunch || fa.maxThreadsPerBlock < kThreadsS)
+    return set_error(PSB_ERR_UNSUPPORTED,
+                     "split_rk4_kernel built with %d registers per thread (needs %d) and at "
+                     "most %d threads (needs %d)",
+                     fa.numRegs, kRegsLaunch, fa.maxThreadsPerBlock, kThreadsS);
+  e = cudaFuncSetAttribute(split_rk4_kernel<W, RES>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess)
     return set_error(PSB_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
   a.smem_bytes = smem;

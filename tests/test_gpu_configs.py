@@ -1,0 +1,111 @@
+"""GPU parity on the shapes of the benchmark configurations, against the
+CPU oracle (FP64 restatement of the reference path, pinned to the
+reference's own goldens), through the C ABI.
+
+  c2  screened exchange (eps(q; n1D) recomputed every right-hand side,
+      coulomb.py:1195-1230) at Nk 512, plain FP64 form;
+  c3  per-wire pump + probe drive (two Gaussian pulses, the probe with its
+      own delay and carrier phase), Nk 256, dt = 0.5 fs: plain FP64 form
+      over the pulses, split form over the whole 4000-step duration;
+  c4  the worst draws of the serving stream for the split form: the
+      largest grids (Nk 1024 and 512), the longest solves (4000 steps of
+      1 fs), pulse area near 2 pi, T2 near 300 fs and |detuning| near
+      50 meV (the split form's error is a slow phase drift that grows with
+      time, excitation and T2).
+
+Tolerances (normwise relative, max|x - ref| / max|ref|): plain FP64
+<= 1e-10 in P(t), p_k, n_e,k, n_h,k; split form <= 1e-6 in P(t) and
+<= 1e-5 in the final state.
+"""
+
+import numpy as np
+import pytest
+from helpers import relerr
+from test_gpu_parity import oracle_run
+
+from pulsesuite_b200 import abi, workloads
+from pulsesuite_b200 import grid as pgrid
+from pulsesuite_b200.batch import WireBatch
+
+pytestmark = pytest.mark.gpu
+
+TOL_PLAIN = 1e-10
+TOL_P = 1e-6
+TOL_STATE = 1e-5
+
+
+def _errors(b, grids, w, n, dt, screened=False):
+    """Per-wire errors [P, p, n_e, n_h] of batch b against the oracle."""
+    yo, Po, _ = oracle_run(grids, w, n, dt, screened=screened)
+    y = b.state()
+    errs = []
+    for i in range(len(w)):
+        s = b.wire_slice(i)
+        errs.append([relerr(b.records(i), Po[i]),
+                     relerr(y[s, 0] + 1j * y[s, 1], yo[s, 0] + 1j * yo[s, 1]),
+                     relerr(y[s, 2], yo[s, 2]), relerr(y[s, 3], yo[s, 3])])
+    return np.array(errs)
+
+
+def test_c3_pump_probe_plain_vs_oracle(cuda):
+    wl = workloads.config3(seed=33, nwires=24)
+    assert (wl.wires["npulse"] == 2).all()
+    n = 1200  # 600 fs: pump at 90 fs, probes up to 290 fs, then free dephasing
+    b = WireBatch(wl.grids, wl.wires, p_cap=n)
+    b.rk4(n, wl.dt)
+    assert (b.wires()["status"] == 0).all()
+    e = _errors(b, wl.grids, wl.wires, n, wl.dt)
+    print(f"c3 plain: max P err {e[:, 0].max():.2e}, max state err {e[:, 1:].max():.2e}")
+    assert e.max() < TOL_PLAIN, e
+
+
+def test_c3_pump_probe_split_full_duration(cuda):
+    wl = workloads.config3(seed=34, nwires=8)
+    n = wl.nsteps  # 4000 steps of 0.5 fs
+    b = WireBatch(wl.grids, wl.wires, p_cap=n, form="split")
+    b.rk4(n, wl.dt)
+    assert (b.wires()["status"] == 0).all()
+    e = _errors(b, wl.grids, wl.wires, n, wl.dt)
+    print(f"c3 split: max P err {e[:, 0].max():.2e}, max state err {e[:, 1:].max():.2e}")
+    assert e[:, 0].max() < TOL_P and e[:, 1:].max() < TOL_STATE, e
+
+
+def c4_worst_case():
+    """Four solves at the edges of the serving stream's parameter ranges."""
+    nks = [1024, 1024, 512, 512]
+    draws = [  # (theta / pi, detuning meV, FWHM fs, T2 fs)
+        (1.98, +49.0, 20.0, 298.0),
+        (1.95, -49.0, 200.0, 295.0),
+        (1.98, -49.0, 20.0, 299.0),
+        (1.90, +48.0, 120.0, 297.0),
+    ]
+    grids = [pgrid.wire_grid(1024), pgrid.wire_grid(512)]
+    w = np.zeros(len(nks), dtype=abi.WIRE_DTYPE)
+    for i, (nk, (th, det, fwhm, t2)) in enumerate(zip(nks, draws)):
+        workloads._fill(w, i, grids[0 if nk == 1024 else 1], 0 if nk == 1024 else 1,
+                        th * np.pi, fwhm * 1e-15, 3.0 * fwhm * 1e-15, det * 1e-3, t2 * 1e-15)
+    return grids, w
+
+
+def test_c4_worst_draws_split_4000_steps(cuda):
+    grids, w = c4_worst_case()
+    n, dt = 4000, 1e-15
+    b = WireBatch(grids, w, p_cap=n, form="split")
+    b.rk4(n, dt)
+    assert (b.wires()["status"] == 0).all()
+    e = _errors(b, grids, w, n, dt)
+    print("c4 worst draws, split, 4000 steps: P err " + " ".join(f"{x:.2e}" for x in e[:, 0])
+          + f"; max state err {e[:, 1:].max():.2e}")
+    assert e[:, 0].max() < TOL_P and e[:, 1:].max() < TOL_STATE, e
+
+
+def test_c2_screened_nk512_plain_vs_oracle(cuda):
+    wl = workloads.config2(seed=35, nwires=4, nsteps=300)
+    assert wl.screened
+    n = wl.nsteps
+    b = WireBatch(wl.grids, wl.wires, screened=True, p_cap=n)
+    b.rk4(n, wl.dt)
+    assert (b.wires()["status"] == 0).all()
+    e = _errors(b, wl.grids, wl.wires, n, wl.dt, screened=True)
+    print(f"c2 screened plain: max P err {e[:, 0].max():.2e}, max state err {e[:, 1:].max():.2e}")
+    assert e.max() < TOL_PLAIN, e
