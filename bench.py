@@ -2,26 +2,43 @@
 """Benchmark of the quantum-wire SBE step on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload c1] [--chunk S]
+                    [--workload c4|c1|c2|c3] [--chunk S]
 
-A bench step advances every wire of the workload by S time steps (one launch
-of the fused step kernel per size class); the metric counts wire*k*steps,
-i.e. sum_w Nk_w * S per bench step.  Default workload: configuration 1 (1024
-wires, Nk ~ U[64,512] rounded to 32, RK4 with dt = 1 fs) in the batched
-split form (exchange sums as exact int8-digit products on the tensor cores,
-<= 1e-6 in P(t) against FP64); the plain FP64 form of the same workload is
-timed in the same run and reported beside it ("plain").  --workload c4 runs
-the continuous-batching server on the Poisson request stream of
-configuration 4 and reports p50/p99 solve latency with the throughput.
+Default workload: configuration 4, the serving stream (Poisson 2000
+requests/s for 60 s; Nk in {64, 128, 256, 512, 1024} with p = {.3, .3, .2,
+.15, .05}; 1-4 ps at dt = 1 fs; pulse area, detuning, FWHM and T2 as
+configuration 1).  The line reports:
+
+  value     the batched split form (exchange sums as exact int8-digit
+            products on the tensor cores) on the stream's request mix as a
+            resident batch (the first 4096 requests of the stream, inputs in
+            HBM): a bench step advances every resident solve by S time steps
+            (one launch per size class); wire*k*steps/s = sum Nk * S / time.
+  plain     the plain FP64 form of the same batch, same timing rules, and
+            split_over_plain.
+  accuracy  per-solve error of the split form against the plain FP64 form
+            (which matches the FP64 oracle to <= 1e-10) over 4000 steps:
+            P(t), final p, n_e, n_h.
+  e2e       the serving API (pulsesuite_b200.serve.Server.run): requests in
+            from the host, continuous batching on the device, P(t) records
+            and final states copied back to host memory; the saturated
+            capacity of the split form on a backlog of the stream.
+  serving   saturated capacity of both forms on the same backlog, and p50 /
+            p99 solve latency of the Poisson stream served in real time (the
+            split form on the whole 60 s; the plain form on a shorter slice).
+  cpu_baseline            the CPU oracle (an OpenMP C restatement of the
+                          reference's path) on a sample of the same mix, all
+                          host cores;
+  cpu_baseline_reference  the reference's own Numba path (imported from
+                          baseline/_ref), full-matrix RHS + rk4_dpc, timed
+                          per Nk and weighted by the mix (large Nk
+                          extrapolated).
 
 Timing: W untimed bench steps, then K bench steps each bracketed by CUDA
 events on the launching stream, with a 256 MiB write between them (L2 is
 126 MB) outside the events; barrier + synchronize around the whole loop;
-max over ranks.  `e2e` repeats the measurement through the public API with
-each step's state copied in from pinned host memory and its P(t) + state
-copied back inside the timed region (copies on their own streams,
-overlapping the neighbouring steps' compute).  `--impl reference` times the CPU oracle (the
-restatement of the reference's Numba path) on the host cores instead.
+max over ranks.  `--impl reference` times the CPU oracle on the host cores
+on the same workload and prints the same line shape.
 """
 
 import argparse
@@ -39,9 +56,9 @@ sys.path.insert(0, REPO)
 
 L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes per state element and launch, from one ncu capture of each step
-# kernel on a small configuration-3 case (dram__bytes_read.sum +
-# dram__bytes_write.sum over 1184 x 256 elements; traffic grows with the
-# elements a launch advances, not with its time steps)
+# kernel (dram__bytes_read.sum + dram__bytes_write.sum over the elements of
+# the captured launch; traffic grows with the elements a launch advances,
+# not with its time steps)
 DRAM_BYTES_PER_ELEMENT = {"split": 9.99e6 / (1184 * 256), "plain": 9.91e6 / (1184 * 256)}
 TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + write.sum of the step kernels on 1184 wires x "
                   "Nk 256, per element, times the elements of this step's launches")
@@ -54,44 +71,86 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c1", choices=["c1", "c2", "c3", "c4"])
+    ap.add_argument("--workload", default="c4", choices=["c1", "c2", "c3", "c4"])
     ap.add_argument("--chunk", type=int, default=100, help="time steps per bench step")
     ap.add_argument("--form", default="split", choices=["plain", "split"],
                     help="split int8-digit tensor-core kernel or plain FP64 kernel")
     ap.add_argument("--no-plain", action="store_true",
                     help="skip the plain-form comparison of the split run")
-    ap.add_argument("--rate", type=float, default=2000.0, help="c4: requests per second")
-    ap.add_argument("--serve-seconds", type=float, default=60.0, help="c4: stream length")
-    ap.add_argument("--capacity-requests", type=int, default=6000,
-                    help="c4: requests of the saturated capacity run of each form")
     ap.add_argument("--nwires", type=int, default=0, help="override the workload's wire count")
-    ap.add_argument("--acc-steps", type=int, default=3000,
-                    help="split form: time steps of the accuracy check against the plain form "
-                         "(the workload's duration, at most this; 0 skips it)")
+    ap.add_argument("--acc-steps", type=int, default=4000,
+                    help="time steps of the accuracy check (the workload's duration, at most "
+                         "this; 0 skips it)")
+    ap.add_argument("--rate", type=float, default=2000.0, help="c4: requests per second")
+    ap.add_argument("--serve-seconds", type=float, default=60.0,
+                    help="c4: stream length served in real time by the split form")
+    ap.add_argument("--plain-serve-seconds", type=float, default=15.0,
+                    help="c4: stream length served in real time by the plain form")
+    ap.add_argument("--capacity-requests", type=int, default=24000,
+                    help="c4: backlog of the saturated capacity runs (both forms)")
+    ap.add_argument("--no-serve", action="store_true", help="c4: skip the serving runs")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-baseline", action="store_true",
+                    help="skip timing the reference's own Numba path")
     return ap.parse_args()
+
+
+def c4_stream(rank, seconds, rate=2000.0, chunk=50):
+    """The configuration-4 request stream of one rank (seeded Poisson arrivals)."""
+    from pulsesuite_b200 import serve
+
+    return serve.poisson_stream(rate=rate, seconds=seconds, seed=4 + 1000 * rank, chunk=chunk)
 
 
 def make_workload(name, rank, nwires):
     from pulsesuite_b200 import workloads
 
     if name == "c4":
-        # the request mix of the serving stream as a fixed batch of wires
-        from pulsesuite_b200 import grid as pgrid
+        # the request mix of the serving stream as a resident batch of wires:
+        # the first `nwires` requests of the rank's stream, each its own Nk,
+        # pulse, detuning, FWHM and T2
         from pulsesuite_b200 import abi, serve
+        from pulsesuite_b200 import grid as pgrid
 
-        reqs = serve.poisson_stream(rate=2000.0, seconds=(nwires or 256) / 2000.0,
-                                    seed=4 + 1000 * rank)
+        n = nwires or 4096
+        reqs = c4_stream(rank, seconds=1.2 * n / 2000.0 + 1.0)[:n]
         grids = [pgrid.wire_grid(nk) for nk in serve.C4_NKS]
         w = np.concatenate([serve.wire_record(r, grids[serve.C4_NKS.index(r.nk)],
                                               table=serve.C4_NKS.index(r.nk)) for r in reqs])
         assert w.dtype == abi.WIRE_DTYPE
-        return workloads.Workload(f"c4 request mix: {len(w)} wires", grids, w, 2500, 1e-15)
+        return workloads.Workload(f"c4 request mix: {len(w)} resident solves", grids, w, 4000,
+                                  1e-15)
     kw = {"seed": 1 + 1000 * rank + {"c1": 0, "c2": 1, "c3": 2}[name]}
     if nwires:
         kw["nwires"] = nwires
     return workloads.CONFIGS[name](**kw)
+
+
+def config_for(a, wl, world):
+    """The line's `config`, identical in both arms (ours and --impl reference)."""
+    cfg = {"workload": WORKLOAD_NAMES[a.workload], "resident_batch": wl.name,
+           "wires_per_gpu": int(len(wl.wires)), "wire_k_per_time_step": int(wl.units_per_step),
+           "time_steps_per_bench_step": int(a.chunk),
+           "l2": "256 MiB write between timed steps (outside the events)",
+           "parallelism": f"wires sharded, {world} independent GPU(s)"}
+    if a.workload == "c4":
+        cfg["serving"] = {"rate_per_s": a.rate, "seconds": a.serve_seconds,
+                          "capacity_requests": a.capacity_requests, "tick_steps": 50,
+                          "hbm_budget_GB": 150}
+    return cfg
+
+
+WORKLOAD_NAMES = {
+    "c1": "c1: 1024 wires, Nk U[64,512] rounded to 32, pulse area U[0.1pi,2pi], detuning "
+          "U[-50,50] meV, FWHM U[20,200] fs, T2 U[50,300] fs, 3000 x 1 fs RK4",
+    "c2": "c2: 16384 wires, Nk 512, statically screened (eps(q; n1D) every RHS), pulse area "
+          "U[0.2pi,1.5pi], 2000 x 1 fs RK4",
+    "c3": "c3: 65536 wires (256x256 sites), Nk 256, pump 30 fs + probe 15 fs (delay U[0,200] "
+          "fs, phase U[0,2pi)), T2 100 fs, 4000 x 0.5 fs RK4",
+    "c4": "c4: Poisson 2000 requests/s for 60 s, Nk in {64,128,256,512,1024} "
+          "p={.3,.3,.2,.15,.05}, 1-4 ps at 1 fs, parameters as c1, 150 GB HBM budget",
+}
 
 
 # ---------------------------------------------------------------------------
@@ -150,9 +209,12 @@ class Clocks:
 
 
 # ---------------------------------------------------------------------------
-# CPU baseline: the oracle (restatement of the reference's Numba path).
+# CPU baselines.
 # ---------------------------------------------------------------------------
 def cpu_baseline(wl, seconds, threads):
+    """The oracle (OpenMP C restatement of the reference's path, the same
+    O(Nk^2) diagonal arithmetic as the GPU kernels) on a sample of the
+    workload's wires, all host threads."""
     from scipy.constants import hbar
 
     from oracle import oracle as orc
@@ -183,6 +245,65 @@ def cpu_baseline(wl, seconds, threads):
     return {"value": rate, "unit": "wire*k*steps/s", "cores": threads, "kind": "port",
             "sample": f"{nw} wires drawn from the workload x {nsteps} RK4 steps "
                       f"({el:.1f} s, OpenMP over wires)"}
+
+
+def cpu_baseline_reference(wl, threads, measure_nks=(64, 128, 256)):
+    """The reference's own Numba CPU path (baseline/_ref; full Nk x Nk
+    CalcH + dpdt/dCdt/dDdt integrated by rk4_dpc, Numba threads inside the
+    kernels), timed for one RK4 step of one wire at each measured Nk and
+    weighted by the workload's wires: wire*k*steps/s = sum Nk / sum t(Nk).
+    Grids above the largest measured one are extrapolated with the power
+    law through the two largest measurements (the reference is O(Nk^3) per
+    right-hand side).  Screening (c2) is not included in the timed RHS and
+    the two-pulse drive (c3) is timed as one pulse (same cost)."""
+    from oracle import numba_ref
+
+    if not numba_ref.available():
+        return {"unavailable": "reference not installed under baseline/_ref"}
+    import platform
+
+    t0 = time.perf_counter()
+    R = numba_ref.load(threads=threads)
+    load_s = time.perf_counter() - t0
+    from pulsesuite_b200 import abi
+    from pulsesuite_b200 import grid as pgrid
+
+    nks_all = wl.nks
+    present = sorted(set(int(n) for n in nks_all))
+    meas = sorted(set([n for n in present if n <= max(measure_nks)] +
+                      [n for n in measure_nks if n <= max(present)]))
+    per = {}
+    for nk in meas:
+        g = pgrid.wire_grid(nk)
+        w = np.zeros(1, dtype=abi.WIRE_DTYPE)
+        src = wl.wires[int(np.argmin(np.abs(nks_all - nk)))]
+        w[0] = src
+        w["npulse"] = 1
+        per[nk] = numba_ref.seconds_per_step(R, g, w[0], wl.dt, nsteps=1)
+    ms = sorted(per)
+    if len(ms) >= 2:
+        n1, n2 = ms[-2], ms[-1]
+        expo = float(np.log(per[n2] / per[n1]) / np.log(n2 / n1))
+    else:
+        expo = 3.0
+
+    def t_of(nk):
+        if nk in per:
+            return per[nk]
+        ref = min(ms, key=lambda m: abs(np.log(m / nk)))
+        return per[ref] * (nk / ref) ** expo
+
+    total_t = float(sum(t_of(int(n)) for n in nks_all))
+    value = float(nks_all.sum()) / total_t
+    extrap = sorted(set(int(n) for n in nks_all) - set(per))
+    return {"value": value, "unit": "wire*k*steps/s", "cores": int(R.threads),
+            "kind": "reference", "cpu": platform.processor() or platform.machine(),
+            "sample": "reference SBEs._CalcH_jit (recompiled serial, parallel build wrong "
+                      "under numba 0.65) + _dpdt/_dCdt/_dDdt_jit + integrator.rk4_dpc, one "
+                      "RK4 step of one wire per measured Nk "
+                      + ", ".join(f"{k}: {v * 1e3:.1f} ms" for k, v in sorted(per.items()))
+                      + (f"; Nk {extrap} extrapolated as Nk^{expo:.2f}" if extrap else ""),
+            "extrapolated": bool(extrap), "import_and_jit_s": load_s}
 
 
 # ---------------------------------------------------------------------------
@@ -256,102 +377,93 @@ def split_accuracy(wl, nsteps, stream):
             "p_err_vs_peak_median": float(np.median(errp))}
 
 
-def run_ours(a):
+def oracle_accuracy(wl, nsteps, stream, nsample=16):
+    """Plain-form error against the FP64 oracle on a sample of wires over
+    `nsteps` (the check used where the split form does not apply)."""
+    import torch
+    from scipy.constants import hbar
+
+    from oracle import oracle as orc
+    from pulsesuite_b200 import grid as pgrid
+    from pulsesuite_b200.batch import WireBatch
+
+    rng = np.random.default_rng(11)
+    idx = np.sort(rng.choice(len(wl.wires), size=min(nsample, len(wl.wires)), replace=False))
+    w = wl.wires[idx].copy()
+    b = WireBatch(wl.grids, w, screened=wl.screened, p_cap=nsteps, form="plain")
+    b.rk4(nsteps, wl.dt, stream=stream)
+    torch.cuda.synchronize()
+    blocks = [orc.grid_tables(g, screened=wl.screened) for g in wl.grids]
+    tables, tabdata = pgrid.pack_tables(wl.grids, blocks, screened=wl.screened)
+    ww = w.copy()
+    nks = tables["nk"][ww["table"]].astype(np.int64)
+    ww["off"] = np.concatenate([[0], np.cumsum(nks)[:-1]])
+    ww["p_off"] = np.arange(len(ww)) * nsteps
+    yo = np.zeros(4 * int(nks.sum()))
+    Po = orc.rk4(tables, tabdata, ww, yo, nsteps, wl.dt, hbar, p_stride=1, p_cap=nsteps,
+                 nthreads=os.cpu_count() or 1).reshape(len(ww), nsteps)
+    yo = yo.reshape(-1, 4)
+    y = b.state()
+    eP, ep, en = [], [], []
+    for i in range(len(ww)):
+        sl = b.wire_slice(i)
+        rP = b.records(i)
+        eP.append(np.max(np.abs(rP - Po[i])) / max(np.max(np.abs(Po[i])), 1e-300))
+        pr, po = y[sl, 0] + 1j * y[sl, 1], yo[sl, 0] + 1j * yo[sl, 1]
+        ep.append(np.max(np.abs(pr - po)) / max(np.max(np.abs(po)), 1e-300))
+        en.append(max(np.max(np.abs(y[sl, c] - yo[sl, c])) / max(np.max(np.abs(yo[sl, c])), 1e-300)
+                      for c in (2, 3)))
+    return {"vs": "FP64 oracle (CPU restatement pinned to the reference's goldens)",
+            "form": "plain", "time_steps": nsteps, "wires": int(len(ww)),
+            "P_rel_err_max": float(np.max(eP)), "p_rel_err_max": float(np.max(ep)),
+            "n_rel_err_max": float(np.max(en))}
+
+
+def timed_steps(b, S, dt, K, W, stream, flush, world):
+    """W warm-up bench steps, then K bench steps of S time steps each, every
+    one bracketed by CUDA events on `stream` with an L2 flush between them
+    (outside the events); total device ms, max over ranks."""
     import torch
     import torch.distributed as dist
 
-    from pulsesuite_b200 import _lib, device
-    from pulsesuite_b200.batch import WireBatch
-
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-
-    wl = make_workload(a.workload, rank, a.nwires)
-    if wl.screened and a.form == "split":
-        a.form = "plain"  # the split form has no screened exchange
-    S = a.chunk
-    b = WireBatch(wl.grids, wl.wires, screened=wl.screened, p_cap=S, form=a.form)
-    stream = torch.cuda.current_stream()
-    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
-    units = wl.units_per_step * S
-    flops_launch = wl.flops_per_step() * S
-
-    def step(p_stride=1):
-        b.rk4(S, wl.dt, p_stride=p_stride, stream=stream)
-
-    for _ in range(a.warmup):
-        step()
+    for _ in range(W):
+        b.rk4(S, dt, stream=stream)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-
-    # -- device-resident timing --------------------------------------------
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in range(a.steps)]
-    with Clocks(local) as clk:
-        torch.cuda.synchronize()
-        for i in range(a.steps):
-            flush.fill_(float(i))
-            evs[i][0].record(stream)
-            b.rk4(S, wl.dt, p_stride=1, stream=stream)
-            evs[i][1].record(stream)
-        torch.cuda.synchronize()
-    times = [e0.elapsed_time(e1) for e0, e1 in evs]
-    total_ms = float(sum(times))
+           for _ in range(K)]
+    torch.cuda.synchronize()
+    for i in range(K):
+        flush.fill_(float(i))
+        evs[i][0].record(stream)
+        b.rk4(S, dt, p_stride=1, stream=stream)
+        evs[i][1].record(stream)
+    torch.cuda.synchronize()
+    total_ms = float(sum(e0.elapsed_time(e1) for e0, e1 in evs))
     if world > 1:
         t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
         dist.barrier()
-    value = units * a.steps * world / (total_ms * 1e-3)
-    status = b.wires()["status"]
-    plain = None
-    if a.form == "split" and not a.no_plain:
-        # the plain FP64 form of the same workload, same timing rules
-        bp = WireBatch(wl.grids, wl.wires, screened=wl.screened, p_cap=S, form="plain")
-        for _ in range(a.warmup):
-            bp.rk4(S, wl.dt, stream=stream)
-        pev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-               for _ in range(a.steps)]
-        torch.cuda.synchronize()
-        for i in range(a.steps):
-            flush.fill_(float(i))
-            pev[i][0].record(stream)
-            bp.rk4(S, wl.dt, p_stride=1, stream=stream)
-            pev[i][1].record(stream)
-        torch.cuda.synchronize()
-        pms = float(sum(e0.elapsed_time(e1) for e0, e1 in pev))
-        if world > 1:
-            t = torch.tensor([pms], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            pms = float(t.item())
-        pval = units * a.steps * world / (pms * 1e-3)
-        plain = {"value": pval, "ms_per_step": pms / a.steps, "split_over_plain": value / pval,
-                 "gpu_launches": a.steps * bp.launches_per_call}
-        del bp
-    accuracy = None
-    if a.form == "split" and not a.no_plain and a.acc_steps > 0:
-        # the workload's own duration, bounded (at most ~1e10 wire*k*steps)
-        # so the check stays a few seconds
-        n_acc = min(wl.nsteps, a.acc_steps, max(50, int(1e10 // wl.units_per_step)))
-        accuracy = split_accuracy(wl, n_acc, stream)
+    return total_ms
 
-    # -- end to end through the public API: pinned host state in, P + state out.
-    # Every step copies its input state from pinned host memory and reads its
-    # P(t) records and final state back to pinned host memory; the copies run
-    # on their own stream and overlap the neighbouring steps' compute, as a
-    # caller streaming independent batches through the API would run them:
-    #   upload stream:    H2D input(i+1) -> staging
-    #   download stream:  D2H snapshot(i) -> host(i % 2)
-    #   compute:      staging -> y, rk4, y/P -> snapshot(i % 2)
-    # The timed region spans all K steps, from before the first upload to
-    # after the last download.
+
+def pipelined_e2e(b, wl, S, K, stream, world):
+    """End to end through the public API: every bench step copies its input
+    state from pinned host memory and reads its P(t) records and final state
+    back to pinned host memory; the copies run on their own streams and
+    overlap the neighbouring steps' compute, as a caller streaming
+    independent batches through the API would run them:
+      upload stream:    H2D input(i+1) -> staging
+      download stream:  D2H snapshot(i) -> host(i % 2)
+      compute:      staging -> y, rk4, y/P -> snapshot(i % 2)
+    The timed region spans all K steps, from before the first upload to after
+    the last download; it includes two device-to-device staging copies per
+    step (not counted in the host<->device bytes) and no L2 flush."""
+    import torch
+    import torch.distributed as dist
+
     y_host = torch.zeros((b.n_state, 4), dtype=torch.float64).pin_memory()
     y_out = [torch.empty_like(y_host).pin_memory() for _ in range(2)]
     P_out = [torch.empty(tuple(b.P.shape), dtype=torch.float64).pin_memory() for _ in range(2)]
@@ -370,9 +482,8 @@ def run_ours(a):
         y_stage.copy_(y_host, non_blocking=True)
     staged.record(cs_up)
     out_done = [None, None]
-    for i in range(a.steps):
+    for i in range(K):
         stream.wait_event(staged)
-        flush.fill_(float(i))
         b.y.copy_(y_stage)
         consumed = ev()
         consumed.record(stream)
@@ -384,7 +495,7 @@ def run_ours(a):
         P_snap[j].copy_(b.P)
         snapped = ev()
         snapped.record(stream)
-        if i + 1 < a.steps:
+        if i + 1 < K:
             with torch.cuda.stream(cs_up):
                 cs_up.wait_event(consumed)
                 y_stage.copy_(y_host, non_blocking=True)
@@ -406,14 +517,137 @@ def run_ours(a):
         t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
-    h2d = y_host.numel() * 8
-    d2h = (P_out[0].numel() + y_out[0].numel()) * 8
+    return e2e_ms, y_host.numel() * 8, (P_out[0].numel() + y_out[0].numel()) * 8
+
+
+def serve_section(a, rank, world):
+    """Configuration 4 through the serving API: saturated capacity of both
+    forms on the same backlog (the first `capacity_requests` requests of the
+    rank's stream, all queued at once), and the Poisson stream served in real
+    time (split form: `serve_seconds`; plain form: `plain_serve_seconds`)."""
+    import torch
+    import torch.distributed as dist
+
+    from pulsesuite_b200 import serve
+
+    chunk = 50
+    warm = serve.poisson_stream(rate=200.0, seconds=0.1, seed=99, chunk=chunk)
+    sat = c4_stream(rank, seconds=1.1 * a.capacity_requests / a.rate + 1.0, rate=a.rate,
+                    chunk=chunk)[:a.capacity_requests]
+    out = {"capacity": {}, "realtime": {}}
+    for form in ("split", "plain"):
+        srv = serve.Server(form=form, chunk=chunk)
+        srv.run(warm, realtime=False)
+        srv.reset_counters()
+        res = srv.run(sat, realtime=False)
+        ok = all(r.status == 0 for r in res)
+        out["capacity"][form] = {"value": srv.throughput(), "seconds": srv.elapsed,
+                                 "requests": len(res), "ticks": srv.tick_count,
+                                 "h2d_bytes": srv.h2d_bytes, "d2h_bytes": srv.d2h_bytes,
+                                 "status_ok": ok}
+        del srv
+        torch.cuda.synchronize()
+    for form, secs in (("split", a.serve_seconds), ("plain", a.plain_serve_seconds)):
+        if secs <= 0:
+            continue
+        reqs = c4_stream(rank, seconds=secs, rate=a.rate, chunk=chunk)
+        srv = serve.Server(form=form, chunk=chunk)
+        srv.run(warm, realtime=False)
+        res = srv.run(reqs, realtime=True)
+        lat = srv.latency_percentiles((50, 99))
+        out["realtime"][form] = {"seconds_of_stream": secs, "requests": len(res),
+                                 "throughput": srv.throughput(), "p50_s": lat.get(50),
+                                 "p99_s": lat.get(99),
+                                 "status_ok": all(r.status == 0 for r in res)}
+        del srv
+        torch.cuda.synchronize()
+    if world > 1:
+        for form in ("split", "plain"):
+            t = torch.tensor([out["capacity"][form]["value"]], device="cuda",
+                             dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.SUM)
+            out["capacity"][form]["value"] = float(t.item())
+    c = out["capacity"]
+    c["split_over_plain"] = c["split"]["value"] / c["plain"]["value"]
+    return out
+
+
+def run_ours(a):
+    import torch
+    import torch.distributed as dist
+
+    from pulsesuite_b200 import _lib, device
+    from pulsesuite_b200.batch import WireBatch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    wl = make_workload(a.workload, rank, a.nwires)
+    form, form_note = a.form, None
+    if wl.screened and form == "split":
+        form = "plain"
+        form_note = ("the split form has no screened exchange (per-wire screened tables); "
+                     "this screened workload runs in the plain FP64 form")
+    S = a.chunk
+    b = WireBatch(wl.grids, wl.wires, screened=wl.screened, p_cap=S, form=form)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    units = wl.units_per_step * S
+
+    with Clocks(local) as clk:
+        total_ms = timed_steps(b, S, wl.dt, a.steps, a.warmup, stream, flush, world)
+    value = units * a.steps * world / (total_ms * 1e-3)
+    status = b.wires()["status"]
+    plain = None
+    if form == "split" and not a.no_plain:
+        bp = WireBatch(wl.grids, wl.wires, screened=wl.screened, p_cap=S, form="plain")
+        pms = timed_steps(bp, S, wl.dt, a.steps, a.warmup, stream, flush, world)
+        pval = units * a.steps * world / (pms * 1e-3)
+        fp64 = fp64_peak_tflops(torch, _lib, device)
+        pach = wl.flops_per_step() * S / (pms / a.steps * 1e-3) / 1e12
+        plain = {"value": pval, "ms_per_step": pms / a.steps, "split_over_plain": value / pval,
+                 "gpu_launches": a.steps * bp.launches_per_call,
+                 "roofline": {"bound": "fp64", "achieved": pach, "peak": fp64,
+                              "unit": "TFLOP/s", "frac": pach / fp64,
+                              "peak_source": "measured in this run: psb_probe_fp64_fma"}}
+        del bp
+    accuracy = None
+    if a.acc_steps > 0:
+        if form == "split" and not a.no_plain:
+            # the workload's own duration, bounded (at most ~2e10 wire*k*steps)
+            n_acc = min(wl.nsteps, a.acc_steps, max(50, int(2e10 // wl.units_per_step)))
+            accuracy = split_accuracy(wl, n_acc, stream)
+        elif form == "plain" and rank == 0:
+            accuracy = oracle_accuracy(wl, min(wl.nsteps, a.acc_steps, 300), stream)
+
+    serving = None
+    if a.workload == "c4" and not a.no_serve:
+        serving = serve_section(a, rank, world)
+        cs = serving["capacity"]["split" if form == "split" else "plain"]
+        e2e = {"value": cs["value"], "unit": "wire*k*steps/s",
+               "h2d_bytes_per_step": cs["h2d_bytes"] / max(1, cs["ticks"]),
+               "d2h_bytes_per_step": cs["d2h_bytes"] / max(1, cs["ticks"]),
+               "api": "pulsesuite_b200.serve.Server.run (saturated backlog)",
+               "step": "one server tick (one launch of one size class)",
+               "requests": cs["requests"]}
+    else:
+        e2e_ms, h2d, d2h = pipelined_e2e(b, wl, S, a.steps, stream, world)
+        e2e = {"value": units * a.steps * world / (e2e_ms * 1e-3), "unit": "wire*k*steps/s",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "api": "WireBatch.rk4 with pinned host state in and P(t) + state out"}
 
     avg_launch_ms = total_ms / a.steps
-    if a.form == "plain":
+    if form == "plain":
         peak = fp64_peak_tflops(torch, _lib, device)
         peak_source = "measured in this run: psb_probe_fp64_fma (FMA loop)"
-        bound = "fp64"
+        bound, unit = "fp64", "TFLOP/s"
+        flops_launch = wl.flops_per_step() * S
     else:
         # the split algorithm's tensor-core work: 6 int8 digit products x 4
         # columns x Nk MACs (2 ops) per element and stage, 4 stages per step
@@ -422,12 +656,9 @@ def run_ours(a):
         peak, peak_source = measured_bf16_peak()
         # dense int8 tensor rate is twice the bf16 rate on B200
         peak, peak_source = 2.0 * peak, "2 x " + peak_source
-        bound = "tensor"
+        bound, unit = "tensor", "TOP/s"
     achieved = flops_launch / (avg_launch_ms * 1e-3) / 1e12
-    # DRAM bytes of one bench step's launches, scaled by elements from the
-    # ncu captures of a small c3 case (split 9.99 MB, plain 9.91 MB for
-    # 1184 x 256 elements: the FP64 state read once per launch)
-    traffic = (DRAM_BYTES_PER_ELEMENT[a.form] * b.n_state) if b.n_state else None
+    traffic = (DRAM_BYTES_PER_ELEMENT[form] * b.n_state) if b.n_state else None
 
     line = {
         "metric": METRIC,
@@ -440,25 +671,32 @@ def run_ours(a):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64" if a.form == "plain" else "int8x3digits+s32acc+f64",
+        "dtype": "f64" if form == "plain" else "int8x3digits+s32acc+f64",
         "data": "synthetic (seeded configuration draws)",
-        "config": {"workload": wl.name, "wires_per_gpu": len(wl.wires),
-                   "wire_k_per_time_step": wl.units_per_step, "time_steps_per_bench_step": S,
-                   "form": a.form, "l2": "256 MiB write between timed steps",
-                   "parallelism": f"wires sharded, {world} independent GPU(s)"},
-        "e2e": {"value": units * a.steps * world / (e2e_ms * 1e-3), "unit": "wire*k*steps/s",
-                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "roofline": {"bound": bound, "achieved": achieved, "peak": peak, "unit": "TFLOP/s" if a.form == "plain" else "TOP/s",
-                     "frac": achieved / peak, "traffic": traffic, "traffic_source": TRAFFIC_SOURCE,
-                     "peak_source": peak_source, "flops_per_launch": flops_launch},
+        "config": config_for(a, wl, world),
+        "form": form,
+        "e2e": e2e,
+        "roofline": {"bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
+                     "frac": achieved / peak, "traffic": traffic,
+                     "traffic_source": TRAFFIC_SOURCE, "peak_source": peak_source,
+                     "flops_per_launch": flops_launch},
         "gpu_launches": a.steps * b.launches_per_call,
         "plain": plain,
         "accuracy": accuracy,
+        "serving": serving,
         "clocks": clk.summary(),
         "wire_status_ok": bool((status == 0).all()),
     }
+    if form_note:
+        line["form_note"] = form_note
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(wl, a.cpu_seconds, os.cpu_count() or 1)
+        threads = os.cpu_count() or 1
+        line["cpu_baseline"] = cpu_baseline(wl, a.cpu_seconds, threads)
+        if not a.no_reference_baseline:
+            try:
+                line["cpu_baseline_reference"] = cpu_baseline_reference(wl, threads)
+            except Exception as ex:  # reported, not fatal: the baseline is informational
+                line["cpu_baseline_reference"] = {"unavailable": f"{type(ex).__name__}: {ex}"}
     if world > 1:
         dist.destroy_process_group()
     if rank == 0:
@@ -466,6 +704,12 @@ def run_ours(a):
 
 
 def run_reference(a):
+    """The reference arm: the CPU implementation of the path on the host
+    cores, on the same workload and `config` as our arm.  The reference
+    itself is Python/Numba with an O(Nk^3) full-matrix RHS; its timed arm is
+    the oracle port (OpenMP C restatement of the same arithmetic, O(Nk^2)),
+    the stronger CPU line, and the reference's own Numba path is reported
+    beside it (cpu_baseline_reference)."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
@@ -475,8 +719,10 @@ def run_reference(a):
     vals = []
     for _ in range(max(1, a.warmup)):
         cpu_baseline(wl, 1.0, threads)
+    t0 = time.perf_counter()
     for _ in range(a.steps):
         vals.append(cpu_baseline(wl, min(a.cpu_seconds, 60.0 / max(1, a.steps)), threads))
+    wall = time.perf_counter() - t0
     v = float(np.mean([x["value"] for x in vals]))
     cb = dict(vals[-1])
     cb["value"] = v
@@ -488,103 +734,30 @@ def run_reference(a):
         "n_gpus": world,
         "steps": a.steps,
         "warmup": a.warmup,
-        "ms_per_step": None,
+        "ms_per_step": wall * 1e3 / a.steps,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (seeded configuration draws)",
-        "config": {"workload": wl.name, "form": "CPU oracle (restatement of the reference's "
-                   "Numba path), all host threads"},
+        "config": config_for(a, wl, world),
+        "form": "CPU oracle (OpenMP C restatement of the reference's path), all host threads",
         "cpu_baseline": cb,
         "e2e": {"value": v, "unit": "wire*k*steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+    if not a.no_reference_baseline:
+        try:
+            line["cpu_baseline_reference"] = cpu_baseline_reference(wl, threads)
+        except Exception as ex:
+            line["cpu_baseline_reference"] = {"unavailable": f"{type(ex).__name__}: {ex}"}
     print(json.dumps(line), flush=True)
-
-
-def run_serve(a):
-    """Configuration 4: the continuous-batching server on the Poisson stream
-    (split form), plus a saturated capacity run of both forms on the same
-    request mix."""
-    import torch
-
-    from pulsesuite_b200 import serve
-
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    torch.cuda.set_device(local)
-    chunk = 50
-    reqs = serve.poisson_stream(rate=a.rate, seconds=a.serve_seconds, seed=4 + 1000 * rank,
-                                chunk=chunk)
-    # warm-up: a few requests through each form
-    warm = serve.poisson_stream(rate=200.0, seconds=0.1, seed=99, chunk=chunk)
-    srv = serve.Server(form="split", chunk=chunk)
-    srv.run(warm, realtime=False)
-    with Clocks(local) as clk:
-        res = srv.run(reqs, realtime=True)
-    thr = srv.throughput()
-    lat = srv.latency_percentiles((50, 99))
-    ok = all(r.status == 0 for r in res)
-    # saturated capacity of both forms on the same mix (all requests queued)
-    cap = {}
-    sat = serve.poisson_stream(rate=1e6, seconds=a.capacity_requests / 1e6, seed=5, chunk=chunk)
-    # (one saturated run lasts about a second and varies by up to ~20 % from
-    # run to run, so each form reports the median of three)
-    cap_runs = {}
-    for form in ("split", "plain"):
-        vals = []
-        for _ in range(3):
-            s2 = serve.Server(form=form, chunk=chunk)
-            s2.run(warm, realtime=False)
-            s2.run(sat, realtime=False)
-            vals.append(s2.throughput())
-            del s2
-            torch.cuda.synchronize()
-        cap[form] = float(np.median(vals))
-        cap_runs[form] = vals
-    h2d = 136 * len(res)
-    d2h = sum(16 * r.nsteps + 32 * r.nk for r in res)
-    line = {
-        "metric": METRIC,
-        "value": thr,
-        "unit": "wire*k*steps/s",
-        "n_gpus": world,
-        "steps": len(res),
-        "warmup": len(warm),
-        "ms_per_step": None,
-        "higher_is_better": True,
-        "scaling": "weak",
-        "vs_baseline": None,
-        "dtype": "int8x3digits+s32acc+f64",
-        "data": "synthetic Poisson request stream (seeded)",
-        "config": {"workload": f"c4: Poisson {a.rate:g}/s for {a.serve_seconds:g} s, Nk in "
-                               "{64,128,256,512,1024} p={.3,.3,.2,.15,.05}, 1-4 ps at 1 fs, "
-                               "150 GB HBM budget", "requests": len(res), "tick_steps": chunk,
-                   "form": "split, continuous batching"},
-        "latency_p50_s": lat.get(50),
-        "latency_p99_s": lat.get(99),
-        "capacity": {"split": cap["split"], "plain": cap["plain"],
-                     "split_over_plain": cap["split"] / cap["plain"],
-                     "requests": len(sat), "runs": cap_runs, "statistic": "median of 3"},
-        "e2e": {"value": thr, "unit": "wire*k*steps/s", "h2d_bytes_per_step": h2d / max(1, len(res)),
-                "d2h_bytes_per_step": d2h / max(1, len(res))},
-        "roofline": None,
-        "gpu_launches": None,
-        "clocks": clk.summary(),
-        "wire_status_ok": ok,
-    }
-    if rank == 0:
-        print(json.dumps(line), flush=True)
 
 
 def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
-    elif a.workload == "c4":
-        run_serve(a)
     else:
         run_ours(a)
 

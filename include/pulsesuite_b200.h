@@ -201,6 +201,19 @@ int psb_calch_f64(const PsbTable* d_tables, int ntab, const double* d_tabdata, i
                   int64_t n_state, int nkmax, int tab_flags, const PsbModel* model,
                   void* stream);
 /*
+ * Diagonal time derivatives of n k-points from given Hamiltonian diagonals:
+ * the diagonal of dpdt, dCdt and dDdt (SBEs.py:1850-1975, 2221-2337,
+ * 2513-2636) for diagonal states, in the reference's association order,
+ *   i hbar dp = Hhh p + Hee p - Heh C - Heh D + Heh - i hbar g p + Off
+ *   i hbar dC = i hbar dD = Heh conj(p) - conj(Heh) p
+ * d_h[3k..3k+2] = (Heh, Hee, Hhh) and d_state[3k..3k+2] = (p, C, D) as
+ * complex (re, im) pairs; d_gam[k] = GamE_k + GamH_k; d_off[k] = OffP_kk
+ * (complex) or NULL; d_out[3k..3k+2] = (dp, dC, dD) complex.
+ */
+int psb_diag_derivs_f64(const double* d_h, const double* d_state, const double* d_gam,
+                        const double* d_off, double hbar, double* d_out, int64_t n,
+                        void* stream);
+/*
  * nsteps classical RK4 steps of size dt on every wire, in the stage order of
  * the reference integrator (libpulsesuite/integrator.py:143-157, rk4_dpc),
  * the whole step fused in one kernel with the wire's state resident on chip.

@@ -16,8 +16,8 @@ freepot)``); the module-level calls read them from module state, set here by
 ``configure`` (keyword arguments of ``CalcH`` override it per call).
 
 The exchange sums over k' (the O(Nk^2) part) run in the sm_100a FP64 kernel
-through ``psb_calch_f64``; the O(Nk) elementwise derivatives run as device
-tensor arithmetic.  Arrays may be numpy arrays or tensors; results come
+through ``psb_calch_f64``; the O(Nk) elementwise derivatives in one launch of
+``psb_diag_derivs_f64``.  Arrays may be numpy arrays or tensors; results come
 back as numpy (in place for CalcH, as the reference does).  Off-diagonal
 states (a k-dependent field along the wire) need the full-matrix right-hand
 side, which this package does not provide: such inputs raise
@@ -77,16 +77,23 @@ def _v_rows(VC, nk):
     return np.ascontiguousarray(v[:nk].T)
 
 
-def h_diagonals(p, ne, nh, VC, Ee, Eh, gap, excitons=True, stream=None):
-    """Device computation of the renormalised H diagonals for one wire:
-    returns complex Heh exchange part (without the drive) and real Hee, Hhh,
-    each (Nk,) numpy."""
+_TABLE_CACHE = {}
+
+
+def _device_table(v, Ee, Eh, excitons):
+    """Device table descriptor + tabdata for one grid, cached by content (a
+    caller stepping one wire re-uses the same V rows and band energies on
+    every call)."""
+    import hashlib
+
     import torch
 
-    device.require_cuda()
-    p = np.asarray(p, dtype=np.complex128)
-    nk = p.size
-    v = _v_rows(VC, nk)
+    nk = v.shape[1]
+    key = hashlib.sha1(b"".join(np.ascontiguousarray(a, dtype=np.float64).tobytes()
+                                for a in (v, Ee, Eh)) + bytes([bool(excitons)])).hexdigest()
+    hit = _TABLE_CACHE.get(key)
+    if hit is not None:
+        return hit
     blk = np.zeros((abi.TAB_BLOCKS, nk))
     blk[0:3] = v
     blk[abi.TAB_EE] = Ee
@@ -98,11 +105,27 @@ def h_diagonals(p, ne, nh, VC, Ee, Eh, gap, excitons=True, stream=None):
         flags |= abi.PSB_TAB_SHARED_V
     tables["flags"] = flags
     tables["L"] = 1.0
+    if len(_TABLE_CACHE) >= 8:
+        _TABLE_CACHE.pop(next(iter(_TABLE_CACHE)))
+    hit = (device.to_device(tables), torch.as_tensor(blk.reshape(-1), device="cuda"), flags)
+    _TABLE_CACHE[key] = hit
+    return hit
+
+
+def h_diagonals(p, ne, nh, VC, Ee, Eh, gap, excitons=True, stream=None):
+    """Device computation of the renormalised H diagonals for one wire:
+    returns complex Heh exchange part (without the drive) and real Hee, Hhh,
+    each (Nk,) numpy."""
+    import torch
+
+    device.require_cuda()
+    p = np.asarray(p, dtype=np.complex128)
+    nk = p.size
+    v = _v_rows(VC, nk)
+    d_tab, d_td, flags = _device_table(v, Ee, Eh, excitons)
     w = np.zeros(1, dtype=abi.WIRE_DTYPE)
     w["gap"] = gap
     y = np.stack([p.real, p.imag, np.asarray(ne, np.float64), np.asarray(nh, np.float64)], 1)
-    d_tab = device.to_device(tables)
-    d_td = torch.as_tensor(blk.reshape(-1), device="cuda")
     d_w = device.to_device(w)
     d_y = torch.as_tensor(np.ascontiguousarray(y), device="cuda")
     d_h = torch.empty_like(d_y)
@@ -154,40 +177,479 @@ def _gam(g, nk):
     return np.full(nk, float(g)) if g.ndim == 0 else np.asarray(g, dtype=np.float64)
 
 
-def _device_diag(*arrs):
+def _derivs(C, D, p, Heh, Hee, Hhh, GamE, GamH, Off):
+    """(dp, dC, dD) diagonals from one launch of psb_diag_derivs_f64."""
     import torch
 
     device.require_cuda()
-    return [torch.as_tensor(np.array(a, dtype=np.complex128), device="cuda") for a in arrs]
+    pd = _diag_of("p", p)
+    nk = pd.size
+    c, d = _diag_of("C", C), _diag_of("D", D)
+    heh, hee, hhh = (_diag_of(n, m) for n, m in (("Heh", Heh), ("Hee", Hee), ("Hhh", Hhh)))
+    off = _np(Off)
+    off = np.diag(off) if off.ndim == 2 else off
+    g = _gam(GamE, nk) + _gam(GamH, nk)
+    h = np.stack([heh, hee, hhh], 1).astype(np.complex128)
+    st = np.stack([pd, c, d], 1).astype(np.complex128)
+    # one host->device copy of the packed inputs, one kernel, one copy back
+    packed = np.concatenate([h.view(np.float64).reshape(-1), st.view(np.float64).reshape(-1),
+                             g, np.asarray(off, dtype=np.complex128).view(np.float64)])
+    buf = torch.as_tensor(packed, device="cuda")
+    out = torch.empty(6 * nk, dtype=torch.float64, device="cuda")
+    base = buf.data_ptr()
+    _lib.call("psb_diag_derivs_f64", base, base + 8 * 6 * nk, base + 8 * 12 * nk,
+              base + 8 * 13 * nk, float(hbar), device.ptr(out), nk, device.stream_ptr())
+    r = out.cpu().numpy().view(np.complex128).reshape(nk, 3)
+    return r[:, 0].copy(), r[:, 1].copy(), r[:, 2].copy()
 
 
 def dpdt(C, D, p, Heh, Hee, Hhh, GamE, GamH, OffP):
     """d p / dt (SBEs.py:1850-1975) for diagonal states: (Nk, Nk) with the
     diagonal i hbar dp_k/dt = (Hee_k + Hhh_k) p_k - Heh_k (C_k + D_k) + Heh_k
     - i hbar (GamE_k + GamH_k) p_k + OffP_kk."""
-    pd = _diag_of("p", p)
-    nk = pd.size
-    c, d = _diag_of("C", C), _diag_of("D", D)
-    heh, hee, hhh = (_diag_of(n, m) for n, m in (("Heh", Heh), ("Hee", Hee), ("Hhh", Hhh)))
-    off = np.diag(_np(OffP)) if _np(OffP).ndim == 2 else _np(OffP)
-    g = _gam(GamE, nk) + _gam(GamH, nk)
-    tp, tc, td, th, te, tH, to, tg = _device_diag(pd, c, d, heh, hee, hhh, off, g)
-    r = (tH * tp + te * tp - th * tc - th * td + th - ii * hbar * tg * tp + to) / (ii * hbar)
-    return np.diag(r.cpu().numpy())
+    return np.diag(_derivs(C, D, p, Heh, Hee, Hhh, GamE, GamH, OffP)[0])
 
 
 def dCdt(Cee, Dhh, Phe, Heh, Hee, Hhh, GamE, GamH, OffE):
     """d C / dt (SBEs.py:2221-2337) for diagonal states: the diagonal is
     (Heh_k conj(p_k) - conj(Heh_k) p_k) / (i hbar) (the Hee commutator
     vanishes on the diagonal)."""
-    pd = _diag_of("p", Phe)
-    heh = _diag_of("Heh", Heh)
-    tp, th = _device_diag(pd, heh)
-    r = (th * tp.conj() - th.conj() * tp) / (ii * hbar)
-    return np.diag(r.cpu().numpy())
+    return np.diag(_derivs(Cee, Dhh, Phe, Heh, Hee, Hhh, GamE, GamH, 0.0 * _np(Phe))[1])
 
 
 def dDdt(Cee, Dhh, Phe, Heh, Hee, Hhh, GamE, GamH, OffH):
     """d D / dt (SBEs.py:2513-2636) for diagonal states: same diagonal as
     dCdt, (Heh_k conj(p_k) - conj(Heh_k) p_k) / (i hbar)."""
-    return dCdt(Cee, Dhh, Phe, Heh, Hee, Hhh, GamE, GamH, OffH)
+    return np.diag(_derivs(Cee, Dhh, Phe, Heh, Hee, Hhh, GamE, GamH, 0.0 * _np(Phe))[2])
+
+
+# ===========================================================================
+# The solver API of the reference (SBEs.py:4631-6078) for diagonal drives.
+# ===========================================================================
+from scipy.constants import c as _c0  # noqa: E402
+from scipy.constants import e as _e0  # noqa: E402
+from scipy.constants import epsilon_0 as _eps0  # noqa: E402
+from scipy.constants import k as _kB  # noqa: E402
+from scipy.constants import m_e as _me0  # noqa: E402
+
+_twopi = 2.0 * np.pi
+_TEMP_K = 77.0  # lattice temperature of the Fermi occupations (phonons.py:22)
+
+
+def _fftg(F):
+    """FFTG of usefulsubs.py:2278-2304: alternate-sign shift, FFT, shift, -F/N."""
+    F[1::2] = -F[1::2]
+    F[:] = np.fft.fft(F)
+    F[1::2] = -F[1::2]
+    F[:] = -F / float(len(F))
+
+
+def _ifftg(F):
+    """iFFTG of usefulsubs.py:2307-2334."""
+    F[1::2] = -F[1::2]
+    F[:] = np.fft.ifft(F)
+    F[1::2] = -F[1::2]
+    F[:] = -F * float(len(F))
+
+
+def _k_array(n, length):
+    """GetKArray (typespace.py:362-381): wavenumbers in FFT order."""
+    dl = _twopi / length if length > 0 else 1.0
+    return np.array([i * dl if i <= n // 2 else (i - n) * dl for i in range(n)], dtype=np.float64)
+
+
+def _array0_index(x):
+    """GetArray0Index (usefulsubs.py:1028-1060)."""
+    dx = x[2] - x[1]
+    xi = np.round((x + 0.1 * dx) / dx).astype(np.int32)
+    hits = np.nonzero(xi == 0)[0]
+    if hits.size == 0:
+        raise ValueError("Zero index not found in array")
+    return int(hits[0])
+
+
+def _fermi(En):
+    """FermiDistr (phonons.py:317-341) at the module temperature."""
+    return 1.0 / (np.exp(En / _kB / _TEMP_K) + 1.0)
+
+
+def yw(w):
+    """Wire sign factor (-1)^floor((w-1)/2) (qwoptics.py:1099-1112)."""
+    return (-1) ** int(np.floor((w - 1) / 2.0))
+
+
+def QWChi1(lam, dky, Ee, Eh, area, geh, dcv):
+    """Linear susceptibility of the wire (qwoptics.py:1115-1152)."""
+    ww = _twopi * _c0 / lam
+    d1 = Ee + Eh - ii * HBAR * geh - HBAR * ww
+    d2 = Ee + Eh + ii * HBAR * geh + HBAR * ww
+    return 4 * dcv**2 / _eps0 / area * dky / _twopi * np.sum((Ee + Eh) / (d1 * d2))
+
+
+class SBESolver:
+    """The reference's ``SBESolver`` (SBEs.py:4631) on the GPU, for states and
+    drives that are diagonal in k.
+
+    Same constructor and parameter files: ``params/qw.params`` and
+    ``params/mb.params`` are read from the working directory in the
+    reference's line order (SBEs.py:4990-5038), and the k grid, wire-space
+    grid, material constants and initial Fermi occupations are derived as in
+    SBEs.py:4766-4885.  The Nw wires live in one ``WireBatch`` (plain FP64
+    kernels): the reference's two stored levels (YY2/CC2/DD2 and
+    YY3/CC3/DD3, SBEs.py:5073-5092) are the batch's y1 and y, and each step
+    is one launch of ``psb_leapfrog_f64`` for the wire (the reference's
+    integrator, SBEs.py:5685-5718), with the unscreened or per-step screened
+    Coulomb table (mb.params Screened) of ``psb_coulomb_vint``.
+
+    What is supported is the reference's diagonal sub-case: Optics and
+    Excitons with the field entering only at q = 0 of the wire
+    (``Ey[NQ0]``: a field uniform along the wire, dipole coupling Ycv), in
+    which the reference's full-matrix state stays exactly diagonal.  Flags
+    whose physics is not diagonal-preserving or not provided (EHs, Phonon,
+    DCTrans, DiagDph, OffDiagDph, Recomb) raise NotImplementedError, as do
+    fields with other q components (``QWCalculator`` windows the field
+    along the wire, which gives it every q: that path needs the full-matrix
+    right-hand side).  No data files are written (the reference's
+    diagnostics under dataQW/ are not reproduced).
+    """
+
+    _UNSUPPORTED = ("EHs", "Phonon", "DCTrans", "DiagDph", "OffDiagDph", "Recomb")
+
+    def __init__(self, q, rr, r0, Emaxxx, lam, Nw, QW, backend="auto"):
+        # defaults of SBEs.py:4638-4671, overwritten by the params files
+        self.L, self.Delta0, self.gap = 100e-9, 5e-9, 1.5 * _e0
+        self.me, self.mh, self.HO = 0.07 * _me0, 0.45 * _me0, 100e-3 * _e0
+        self.gam_e = self.gam_h = self.gam_eh = 1.0 / 1e-12
+        self.epsr, self.Edc, self.wL = 9.1, 0.0, 0.0
+        self.Optics = self.Excitons = self.EHs = self.Screened = self.Phonon = True
+        self.DCTrans, self.LF, self.FreePot = False, True, False
+        self.DiagDph = self.OffDiagDph = True
+        self.OBE = self.Recomb = self.ReadDC = self.PLSpec = self.ignorewire = False
+        self.Xqwparams = False
+        self.jmax, self.ntmax = 1000, 100000
+        self.small = 1e-200
+        self.Nw = int(Nw)
+        self.wireoff = True
+        self.xxx = self.jjj = 1
+        self.t = 0.0
+        self.start = False
+        self._backend = backend
+        self.batch = None
+        if not QW:
+            return
+        self._read_qw_params()
+        self._read_mb_params()
+        bad = [f for f in self._UNSUPPORTED if getattr(self, f)]
+        if bad:
+            raise NotImplementedError(
+                "mb.params flags " + ", ".join(bad) + " need physics beyond the diagonal "
+                "Hartree-Fock SBE step (not provided by pulsesuite_b200)")
+        self.Emax0 = float(Emaxxx)
+        kmax = np.sqrt(1.2 * self.gap * 2.0 * self.me / (HBAR**2))
+        self.dkr = _twopi / (2.0 * self.L)
+        nk_odd = int(np.floor(kmax / self.dkr) * 2 + 1)
+        self.Nr = nk_odd * 2
+        self.Nk = nk_odd - 1
+        dnk = (self.Nk - 1) // 2
+        self.NK0 = dnk + 1
+        self.kr = np.array([self.dkr * (-dnk + k - 0.5) for k in range(self.Nk)])
+        self.r = np.linspace(-self.L, self.L, self.Nr)
+        Qr = np.roll(_k_array(self.Nr, 2 * self.L), self.Nr // 2)
+        Qr[0] = -Qr[0]
+        self.Qr = Qr
+        self.NQ0 = _array0_index(Qr)
+        self.dr = (self.r[2] - self.r[1]) * (self.Nr - 1) / float(self.Nr)
+        self.dcv = np.sqrt((_e0 * HBAR) ** 2 / (6.0 * _me0 * self.gap) * (_me0 / self.me - 1.0))
+        self.alphae = np.sqrt(self.me * self.HO) / HBAR
+        self.alphah = np.sqrt(self.mh * self.HO) / HBAR
+        self.ehint = np.sqrt(2.0 * self.alphae * self.alphah /
+                             (self.alphae**2 + self.alphah**2))
+        self.gam_eh = (self.gam_e + self.gam_h) / 2.0
+        self.qc = 2.0 * self.alphae * self.alphah / (self.alphae + self.alphah)
+        self.area = np.sqrt(2.0 * np.pi) / np.sqrt(self.alphae**2 + self.alphah**2) * self.Delta0
+        self.Ee = HBAR**2 * self.kr**2 / (2.0 * self.me)
+        self.Eh = HBAR**2 * self.kr**2 / (2.0 * self.mh)
+        self.window = np.exp(-((self.r / (self.L / 2.0)) ** 150))  # qwoptics.py:636-655
+        self.chiw = QWChi1(lam, self.dkr, self.Ee + self.gap, self.Eh, self.area, self.gam_eh,
+                           self.dcv)
+        self._build_batch()
+        self.start = True
+
+    # -- parameter files (SBEs.py:4990-5038) ---------------------------------
+    def _read_qw_params(self):
+        with open("params/qw.params", "r", encoding="utf-8") as f:
+            vals = [f.readline().split()[0] for _ in range(15)]
+        self.L, self.Delta0 = float(vals[0]), float(vals[1])
+        self.gap = float(vals[2]) * _e0
+        self.me, self.mh = float(vals[3]) * _me0, float(vals[4]) * _me0
+        self.HO = float(vals[5]) * _e0
+        self.gam_e, self.gam_h, self.gam_eh = float(vals[6]), float(vals[7]), float(vals[8])
+        self.epsr = float(vals[9])
+        self.Oph = float(vals[10]) * _e0 / HBAR
+        self.Gph = float(vals[11]) * _e0 / HBAR
+        self.Edc = float(vals[12])
+        self.jmax, self.ntmax = int(vals[13]), int(vals[14])
+
+    def _read_mb_params(self):
+        names = ("Optics", "Excitons", "EHs", "Screened", "Phonon", "DCTrans", "LF", "FreePot",
+                 "DiagDph", "OffDiagDph", "Recomb", "PLSpec", "ignorewire", "Xqwparams",
+                 "LorentzDelta")
+        with open("params/mb.params", "r", encoding="utf-8") as f:
+            for n in names:
+                setattr(self, n, bool(int(f.readline().split()[0])))
+
+    # -- device state ----------------------------------------------------------
+    def _build_batch(self):
+        import torch
+
+        from . import coulomb
+        from . import grid as pgrid
+        from .batch import WireBatch
+
+        g = pgrid.Grid(nk=self.Nk, dk=self.dkr, kr=self.kr, L=self.L, me=self.me, mh=self.mh,
+                       epsr=self.epsr, delta0=self.Delta0, alphae=self.alphae,
+                       alphah=self.alphah, vkind="vint", y=self.r, gap=self.gap, dcv=self.dcv,
+                       ehint=self.ehint, area=self.area)
+        self.grid = g
+        blk = coulomb.table_block(g, screened=self.Screened)
+        host = np.zeros((abi.TAB_BLOCKS, self.Nk))
+        host[0:3] = blk.reshape(abi.TAB_BLOCKS, self.Nk)[0:3].cpu().numpy()
+        tables, _ = pgrid.pack_tables([g], [host.reshape(-1)], screened=self.Screened,
+                                      excitons=self.Excitons)
+        w = np.zeros(self.Nw, dtype=abi.WIRE_DTYPE)
+        w["table"] = 0
+        w["npulse"] = 0
+        w["gap"] = self.gap
+        w["gamma"] = self.gam_e + self.gam_h
+        w["pscale"] = 2.0 * self.ehint / self.area / self.L * self.dcv
+        # M = -ehint Ycv Ey[NQ0] yw(w) (SBEs.py:5165-5175, Ycv = dcv)
+        w["mscale"] = [self.ehint * self.dcv * yw(i + 1) for i in range(self.Nw)]
+        self.batch = WireBatch([g], w, screened=self.Screened, excitons=self.Excitons, p_cap=1,
+                               tables=tables, tabdata=blk.contiguous())
+        # CC = DD = diag FermiDistr(Ee + gap/2) on every level (SBEs.py:4857-4868)
+        f = _fermi(self.Ee + self.gap / 2.0)
+        y = np.zeros((self.Nw, self.Nk, 4))
+        y[:, :, 2] = f
+        y[:, :, 3] = f
+        self.batch.set_state(y.reshape(-1, 4), y.reshape(-1, 4))
+        self.y0 = self.batch.y1.clone()  # level 1 (YY1/CC1/DD1)
+        self._field = torch.zeros((self.Nw, 2), dtype=torch.float64, device="cuda")
+        self._steps_col = abi.WIRE_DTYPE.fields["steps"][1] // 4
+        self._wires_i32 = self.batch.d_wires.view(torch.int32).view(self.Nw, -1)
+
+    def levels(self, w):
+        """Diagonals (p, ne, nh) of the three stored levels of wire w (1-based),
+        numpy, as (YY1, YY2, YY3), (CC1, CC2, CC3), (DD1, DD2, DD3)."""
+        s = self.batch.wire_slice(w - 1)
+        out = []
+        for lv in (self.y0, self.batch.y1, self.batch.y):
+            a = lv[s].cpu().numpy()
+            out.append(a)
+        return ([a[:, 0] + 1j * a[:, 1] for a in out], [a[:, 2] + 0j for a in out],
+                [a[:, 3] + 0j for a in out])
+
+    # -- the step ---------------------------------------------------------------
+    def _drive(self, Ex, Ey, Ez):
+        """E = Ey[NQ0] after checking that no other q component reaches Meh."""
+        if not self.Optics:
+            return 0.0
+        lo, hi = self.NQ0 - (self.Nk - 1), self.NQ0 + self.Nk
+        win = slice(max(lo, 0), hi)
+        ey = np.array(Ey[win], dtype=np.complex128, copy=True)
+        ey[self.NQ0 - win.start] = 0.0
+        if np.any(np.asarray(Ex)[win] != 0) or np.any(np.asarray(Ez)[win] != 0) or np.any(ey != 0):
+            raise NotImplementedError(
+                "the field has components other than Ey at q = 0 of the wire: the SBE state "
+                "becomes non-diagonal, which needs the full-matrix right-hand side (not "
+                "provided by pulsesuite_b200)")
+        return complex(Ey[self.NQ0])
+
+    def _sbe_calculator(self, Ex, Ey, Ez, Vr, dt, Px, Py, Pz, Re, Rh, WriteFields, w):
+        """One leapfrog step of wire w (1-based) driven by the wire-space fields
+        (SBEs.py:5624-5836), with its source terms written in place: Px, Py,
+        Pz = QWPolarization3 of the new p (qwoptics.py:815-946) and, with LF,
+        Re, Rh = QWRho5 of the new C, D (qwoptics.py:948-1078), all in q space."""
+        E = self._drive(Ex, Ey, Ez)
+        for a in (Px, Py, Pz, Re, Rh):
+            a[:] = 0.0
+        b = self.batch
+        i = w - 1
+        s = b.wire_slice(i)
+        self.y0[s].copy_(b.y1[s])  # YY1 <- YY2 (SBEs.py:5082-5092)
+        self._field[i, 0] = E.real
+        self._field[i, 1] = E.imag
+        self._wires_i32[i, self._steps_col] = 0  # the field sample of this step is index 0
+        import torch
+
+        order = torch.tensor([i], dtype=torch.int32, device="cuda")
+        from . import device as _dev
+
+        _lib.call("psb_leapfrog_f64", *b._common(), _dev.ptr(order), 1, _dev.ptr(b.y1),
+                  _dev.ptr(b.y), b.n_state, self.Nk, b.tab_flags, _dev.ptr(self._field), 2,
+                  self._field.numel(), 1, float(dt), _dev.ptr(b.P), b.P.shape[0], 1,
+                  b.p_cap, abi.as_ptr(b.model), _dev.stream_ptr())
+        st = int(b.wires()["status"][i])
+        if st != abi.PSB_OK:
+            raise _lib.PsbError(f"wire {w}: step status {st}")
+        y3 = b.y[s].cpu().numpy()
+        if self.Optics:
+            # diagonal p: P(r) = 2 ehint/(area L) window(r) sum_k Re(p_k X_kk) (qwoptics.py:85-127)
+            pr = y3[:, 0]
+            sgn = np.array([(-1.0) ** (k + 1) for k in range(self.Nk)])
+            scale = 2 * self.ehint / self.area / self.L
+            Px[:] = scale * self.window * np.sum(pr * self.dcv * sgn)
+            Py[:] = scale * self.window * (np.sum(pr * self.dcv) * yw(w))
+            Pz[:] = scale * self.window * (np.sum(-pr * self.dcv) * (-1) ** w)
+            for a in (Px, Py, Pz):
+                _fftg(a)
+        if self.LF:
+            self._rho(y3[:, 2], y3[:, 3], Re, Rh)
+            Re[:] = 2.0 * _e0 * Re / self.area * self.ehint
+            Rh[:] = 2.0 * _e0 * Rh / self.area * self.ehint
+
+    def _rho(self, ne, nh, re, rh):
+        """QWRho5 (qwoptics.py:948-1078) for diagonal C, D: the density along
+        the wire is sum_k n_k window(r) / (2L), then the boundary offset is
+        removed, the totals are restored and the result is transformed."""
+        nr = self.Nr
+        dr = self.r[1] - self.r[0]
+        re[:] = np.sum(ne) * self.window / (2.0 * self.L)
+        rh[:] = np.sum(nh) * self.window / (2.0 * self.L)
+        for a, tot in ((re, np.sum(np.abs(ne)) + 1e-50), (rh, np.sum(np.abs(nh)) + 1e-50)):
+            a[:] = a - np.real(np.sum(a[0:10]) + np.sum(a[nr - 10:nr])) / 20.0
+            a[:] = a * tot / (np.sum(np.abs(a)) * dr + 1e-100)
+            _fftg(a)
+
+    def QWCalculator(self, Exx, Eyy, Ezz, Vrr, rr, q, dt, w, Pxx, Pyy, Pzz, Rho, DoQWP,
+                     DoQWDl):
+        """Per-time-step entry (SBEs.py:5838-6001): bookkeeping of the step
+        counters and the wire-off gate as in the reference, then the step.
+        While the field stays below 1e-3 of Emaxxx the wire is off and the
+        outputs are zero, as in the reference.  A field that switches the
+        wire on reaches the wire through Prop2QW, whose window along the wire
+        gives it every q component: that needs the full-matrix right-hand
+        side, so NotImplementedError is raised."""
+        for a in (Pxx, Pyy, Pzz, Rho):
+            a[:] = 0.0
+        if w == 1:
+            if self.jjj == self.jmax:
+                self.jjj = 0
+            self.xxx += 1
+            self.jjj += 1
+            self.t += dt
+        mag = np.max(np.sqrt(np.abs(Exx) ** 2 + np.abs(Eyy) ** 2 + np.abs(Ezz) ** 2))
+        if self.wireoff and mag < 1e-3 * self.Emax0:
+            return
+        raise NotImplementedError(
+            "QWCalculator: a propagation-space field drives the wire through Prop2QW "
+            "(qwoptics.py:673-721), whose window makes the state non-diagonal; use "
+            "_sbe_calculator with a q = 0 field, or WireBatch")
+
+    # -- small accessors (SBEs.py:5516-5534) ---------------------------------------
+    def chiqw(self):
+        return self.chiw
+
+    def getqc(self):
+        return self.qc
+
+    def QWArea(self):
+        return self.area
+
+    def ShutOffOptics(self):
+        self.Optics = False
+
+    # -- backup files (SBEs.py:5536-5585) -----------------------------------------
+    _KEYS = ("CC1", "CC2", "CC3", "DD1", "DD2", "DD3", "YY1", "YY2", "YY3")
+
+    def _level_arrays(self):
+        """{key: (Nw, Nk) complex diagonals} of the nine stored arrays."""
+        out = {}
+        levels = [lv.view(self.Nw, self.Nk, 4).cpu().numpy()
+                  for lv in (self.y0, self.batch.y1, self.batch.y)]
+        for n, a in enumerate(levels, start=1):
+            out[f"YY{n}"] = a[:, :, 0] + 1j * a[:, :, 1]
+            out[f"CC{n}"] = a[:, :, 2] + 0j
+            out[f"DD{n}"] = a[:, :, 3] + 0j
+        return out
+
+    def write_sbes_data(self, n, directory="dataQW/backup/"):
+        """Write the nine coherence arrays in the reference's backup format:
+        one file per array, per wire then k2 then k1 one line "re im" of
+        arr[k1, k2, w] (full Nk x Nk, zero off the diagonal)."""
+        import os
+
+        os.makedirs(directory, exist_ok=True)
+        arrs = self._level_arrays()
+        for key in self._KEYS:
+            a = arrs[key]
+            lines = []
+            for w in range(self.Nw):
+                for k2 in range(self.Nk):
+                    for k1 in range(self.Nk):
+                        val = complex(a[w, k1]) if k1 == k2 else 0j
+                        lines.append(f"{np.real(val)} {np.imag(val)}\n")
+            with open(os.path.join(directory, f"{key}.{n}.dat"), "w", encoding="utf-8") as f:
+                f.write("".join(lines))
+
+    def read_sbes_data(self, Nt, directory="dataQW/backup/"):
+        """Read backup files written by the reference (or write_sbes_data);
+        the arrays must be diagonal in k."""
+        import os
+
+        import torch
+
+        vals = {}
+        for key in self._KEYS:
+            with open(os.path.join(directory, f"{key}.{Nt}.dat"), "r", encoding="utf-8") as f:
+                raw = np.array([float(x) for x in f.read().split()], dtype=np.float64)
+            m = (raw[0::2] + 1j * raw[1::2]).reshape(self.Nw, self.Nk, self.Nk)  # [w, k2, k1]
+            d = np.einsum("wkk->wk", m)
+            off = m.copy()
+            idx = np.arange(self.Nk)
+            off[:, idx, idx] = 0.0
+            if np.any(off != 0):
+                raise NotImplementedError(f"{key}: off-diagonal coherences need the full-matrix "
+                                          "SBE state (not provided by pulsesuite_b200)")
+            vals[key] = d
+        for n, lv in enumerate((self.y0, self.batch.y1, self.batch.y), start=1):
+            y = np.stack([vals[f"YY{n}"].real, vals[f"YY{n}"].imag, vals[f"CC{n}"].real,
+                          vals[f"DD{n}"].real], -1).reshape(-1, 4)
+            lv.copy_(torch.as_tensor(y))
+
+
+# Module-level shims of the reference (SBEs.py:6019-6078).
+_default_solver = None
+
+
+def InitializeSBE(q, rr, r0, Emaxxx, lam, Nw, QW):
+    global _default_solver
+    _default_solver = SBESolver(q, rr, r0, Emaxxx, lam, Nw, QW)
+
+
+def QWCalculator(Exx, Eyy, Ezz, Vrr, rr, q, dt, w, Pxx, Pyy, Pzz, Rho, DoQWP, DoQWDl):
+    _default_solver.QWCalculator(Exx, Eyy, Ezz, Vrr, rr, q, dt, w, Pxx, Pyy, Pzz, Rho, DoQWP,
+                                 DoQWDl)
+
+
+def chiqw():
+    return _default_solver.chiqw()
+
+
+def getqc():
+    return _default_solver.getqc()
+
+
+def QWArea():
+    return _default_solver.QWArea()
+
+
+def ShutOffOptics():
+    _default_solver.ShutOffOptics()
+
+
+def WriteSBEsData(n):
+    _default_solver.write_sbes_data(n)
+
+
+def ReadSBEsData(Nt):
+    _default_solver.read_sbes_data(Nt)

@@ -31,6 +31,7 @@ _SIGNATURES = {
     "psb_leapfrog_f64": ([vp, i32, vp, i64, vp, i32, vp, i32, vp, vp, i64, i32, i32, vp, i64,
                           i64, i32, f64, vp, i64, i32, i32, vp, vp], i32),
     "psb_f64_smem_bytes": ([i32, i32], i32),
+    "psb_diag_derivs_f64": ([vp, vp, vp, vp, f64, vp, i64, vp], i32),
     "psb_probe_fp64_fma": ([i32, i32, vp, vp, vp], i32),
     "psb_split_ws_bytes": ([i64], i64),
     "psb_split_smem_bytes": ([i32, i32], i32),

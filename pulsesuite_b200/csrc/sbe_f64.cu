@@ -722,3 +722,62 @@ extern "C" int psb_leapfrog_f64(const PsbTable* d_tables, int ntab, const double
   bt.hbar = model->hbar;
   return launch_sbe_f64(bt, kLeapfrog, n_order, nkmax, tab_flags, (cudaStream_t)stream);
 }
+
+// ---------------------------------------------------------------------------
+// Elementwise diagonal derivatives from given Hamiltonian diagonals (the
+// diagonal of dpdt / dCdt / dDdt for diagonal states, SBEs.py:1958-1975,
+// 2325-2337, 2623-2636), in the reference's association order:
+//   i hbar dp = ((((Hhh p + Hee p) - Heh C) - Heh D) + Heh) - (i hbar g) p + Off
+//   i hbar dC = i hbar dD = Heh conj(p) - conj(Heh) p
+// (the Hee / Hhh commutators vanish on the diagonal).
+// ---------------------------------------------------------------------------
+namespace psb {
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) {
+  return make_double2(a.x + b.x, a.y + b.y);
+}
+__device__ __forceinline__ double2 csub(double2 a, double2 b) {
+  return make_double2(a.x - b.x, a.y - b.y);
+}
+// x / (i hbar) = (x.im / hbar, -x.re / hbar)
+__device__ __forceinline__ double2 div_ihbar(double2 x, double hb) {
+  return make_double2(x.y / hb, -x.x / hb);
+}
+
+__global__ void diag_derivs_kernel(const double2* __restrict__ h, const double2* __restrict__ st,
+                                   const double* __restrict__ g, const double2* __restrict__ off,
+                                   double hb, double2* __restrict__ out, int64_t n) {
+  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const double2 heh = h[3 * k], hee = h[3 * k + 1], hhh = h[3 * k + 2];
+  const double2 p = st[3 * k], c = st[3 * k + 1], d = st[3 * k + 2];
+  double2 acc = cadd(cmul(hhh, p), cmul(hee, p));
+  acc = csub(acc, cmul(heh, c));
+  acc = csub(acc, cmul(heh, d));
+  acc = cadd(acc, heh);
+  // (i hbar) g = (0, hbar g) as a complex scalar, times p
+  acc = csub(acc, cmul(make_double2(0.0 * g[k], hb * g[k]), p));
+  if (off) acc = cadd(acc, off[k]);
+  out[3 * k] = div_ihbar(acc, hb);
+  const double2 pc = make_double2(p.x, -p.y), hc = make_double2(heh.x, -heh.y);
+  const double2 dn = div_ihbar(csub(cmul(heh, pc), cmul(hc, p)), hb);
+  out[3 * k + 1] = dn;
+  out[3 * k + 2] = dn;
+}
+}  // namespace psb
+
+extern "C" int psb_diag_derivs_f64(const double* d_h, const double* d_state, const double* d_gam,
+                                   const double* d_off, double hbar, double* d_out, int64_t n,
+                                   void* stream) {
+  if (!d_h || !d_state || !d_gam || !d_out || n < 0 || !(hbar > 0.0))
+    return psb::set_error(PSB_ERR_INVALID, "psb_diag_derivs_f64: null pointer or bad size");
+  if (n == 0) return PSB_OK;
+  const int threads = 256;
+  const int64_t blocks = (n + threads - 1) / threads;
+  psb::diag_derivs_kernel<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(
+      reinterpret_cast<const double2*>(d_h), reinterpret_cast<const double2*>(d_state), d_gam,
+      reinterpret_cast<const double2*>(d_off), hbar, reinterpret_cast<double2*>(d_out), n);
+  return psb::check_cuda("diag_derivs_kernel");
+}

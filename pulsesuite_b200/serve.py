@@ -269,6 +269,15 @@ class Server:
         self._ar = {nk: torch.arange(nk, dtype=torch.int64, device="cuda") for nk in self.nks}
         self.pending = []  # retiring batches: (event, entries, host buffers)
         self.results = []
+        self.reset_counters()
+
+    def reset_counters(self):
+        """Zero the host<->device byte counters and the tick count (bytes of
+        the tensors each tick copies: staged metadata in, records and states
+        out)."""
+        self.h2d_bytes = 0
+        self.d2h_bytes = 0
+        self.tick_count = 0
 
     class _Lane:
         """One size class: stream, tick count, waiting requests, active
@@ -384,6 +393,8 @@ class Server:
                   self.tabdata.numel(), self.device.ptr(self.d_wires), self.nslots)
         dt = float(self.active[int(slots[0])][0].dt)
         sm = lane.stream
+        self.h2d_bytes += st.n
+        self.tick_count += 1
         with torch.cuda.stream(sm):
             st.push()
             if adm is not None:
@@ -443,6 +454,7 @@ class Server:
             wgr.record_stream(cs)
             ev = torch.cuda.Event()
             ev.record(cs)
+        self.d2h_bytes += (hP.numel() + hy.numel()) * 8 + hw.numel()
         self.pending.append((ev, entries, hP, hy, hw))
 
     def _collect(self, block=False):

@@ -25,6 +25,7 @@ Cases (all stored as .npz next to this script):
   rk4_*.npz       reference RHS integrated by libpulsesuite.integrator.rk4_dpc
                   (rotating-frame drive, the benchmark configurations' physics)
   leapfrog_*.npz  SBESolver._sbe_calculator, the reference's own driver
+  solver_*.npz    the SBESolver API with LF on: source terms, levels, backup files
 """
 
 import argparse
@@ -371,6 +372,63 @@ def make_leapfrog(R, out, name, L=2.85e-8, screened=False, nsteps=3000, dt=10e-1
         os.chdir(cwd)
 
 
+MB_PARAMS_LF = "1\n1\n0\n0\n0\n0\n1\n0\n0\n0\n0\n0\n0\n0\n0\n"
+
+
+def make_solver_api(R, out, name="solver_lf_nk32", L=2.85e-8, nsteps=300, dt=10e-18):
+    """The reference's SBESolver as a caller uses it, with LF on (so the
+    charge densities Re, Rh of QWRho5 are computed): the initial levels, the
+    last step's source terms Px, Py, Pz, Re, Rh (q space), the final levels,
+    and the text of the backup files write_sbes_data writes at the end."""
+    cwd = os.getcwd()
+    run = tempfile.mkdtemp(prefix="api_", dir=_TMP)
+    os.makedirs(os.path.join(run, "params"))
+    gam = 5e12
+    with open(os.path.join(run, "params", "qw.params"), "w") as f:
+        f.write(QW_PARAMS.format(L=L, gam=gam))
+    with open(os.path.join(run, "params", "mb.params"), "w") as f:
+        f.write(MB_PARAMS_LF)
+    os.chdir(run)
+    try:
+        rr = np.linspace(-5e-7, 5e-7, 64)
+        qrr = R.SBEs.GetKArray(64, 64 * (rr[1] - rr[0]))
+        s = R.SBEs.SBESolver(qrr, rr, 0.0, 1e7, 800e-9, 1, True)
+        nk, nr = s.Nk, s.Nr
+
+        def levels():
+            return np.stack([np.stack([np.diag(a[:, :, 0]) for a in
+                                       (s.YY1, s.YY2, s.YY3)]),
+                             np.stack([np.diag(a[:, :, 0]) for a in (s.CC1, s.CC2, s.CC3)]),
+                             np.stack([np.diag(a[:, :, 0]) for a in (s.DD1, s.DD2, s.DD3)])])
+
+        init = levels()
+        E0, tw, tp = 2e8, 4e-15, 1.5e-15
+        wl = (s.gap + 0.05 * 1.602176634e-19) / R.SBEs.hbar
+        field = np.zeros(nsteps, dtype=complex)
+        srcs = [np.zeros(nr, complex) for _ in range(5)]
+        for n in range(nsteps):
+            t = n * dt
+            E = E0 * np.exp(-(((t - tp) / tw) ** 2)) * np.cos(wl * (t - tp))
+            field[n] = E
+            Ex, Ey, Ez, Vr = (np.zeros(nr, complex) for _ in range(4))
+            Ey[s.NQ0] = E
+            s._sbe_calculator(Ex, Ey, Ez, Vr, dt, *srcs, False, 1)
+        s.write_sbes_data(7)
+        texts = {}
+        for key in ("CC1", "CC2", "CC3", "DD1", "DD2", "DD3", "YY1", "YY2", "YY3"):
+            with open(os.path.join("dataQW", "backup", f"{key}.7.dat")) as f:
+                texts[key] = np.array(f.read())
+        np.savez_compressed(os.path.join(out, f"{name}.npz"), nk=nk, nr=nr, NQ0=s.NQ0, L=L,
+                            gam=gam, dt=dt, nsteps=nsteps, field=field, init=init,
+                            final=levels(), Px=srcs[0], Py=srcs[1], Pz=srcs[2], Re=srcs[3],
+                            Rh=srcs[4], r=s.r.copy(), Qr=s.Qr.copy(), kr=s.kr.copy(),
+                            chiw=s.chiw, qc=s.qc, area=s.area,
+                            **{f"backup_{k}": v for k, v in texts.items()})
+        print(f"{name}: Nk={nk}, {nsteps} steps, max|Re| = {np.max(np.abs(srcs[3])):.3e}")
+    finally:
+        os.chdir(cwd)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--full-c0", action="store_true")
@@ -396,6 +454,8 @@ def main():
     if want("leapfrog"):
         make_leapfrog(R, out, "leapfrog_nk32", screened=False)
         make_leapfrog(R, out, "leapfrog_screened_nk32", screened=True, nsteps=2000)
+    if want("solver"):
+        make_solver_api(R, out)
     if a.full_c0:
         make_rk4(R, out, "rk4_c0_nk128_full", rwa_case(128, 4000))
 
