@@ -65,8 +65,6 @@
 // returns.
 #include <math.h>
 
-#include <type_traits>
-
 #include "psb_common.cuh"
 
 namespace psb {
@@ -861,47 +859,40 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
       const float* fx = xfach + (s & 1) * N;
       uint8_t* xn = xbase + bn * L.xbuf;
       int* ovn = ovf + bn * N;
-      // per-wire constants of the stage, read once instead of per element
-      constexpr bool kHoist = WH <= 4;
-      float wMr[WH], wMi[WH];
-#pragma unroll
-      for (int j = 0; j < WH; ++j) {
-        wMr[j] = __shfl_sync(0xffffffffu, Mr, j);
-        wMi[j] = __shfl_sync(0xffffffffu, Mi, j);
-      }
-      float4 wfx[kHoist ? WH : 1], wsc[kHoist ? WH : 1];
-      double wgap[kHoist ? WH : 1], wgam[kHoist ? WH : 1];
-      if constexpr (kHoist) {
-#pragma unroll
-        for (int j = 0; j < WH; ++j) {
-          const int w = w0 + j;
-          wfx[j] = *reinterpret_cast<const float4*>(fx + 4 * w);
-          wsc[j] = *reinterpret_cast<const float4*>(scw + 4 * w);
-          wgap[j] = gaph[w];
-          wgam[j] = wpar[w].y;
-        }
-      }
-      // columns (bit 4 j + c) whose next-stage digits outgrew the lagged
-      // scale; published once at the end of the stage
-      uint32_t ovbits = 0;
-      // One row tile of this stage.  The stage is a compile-time constant
-      // here, so the element code has no stage branches, and invalid
-      // elements (rows past nk, empty wire slots) are masked instead of
-      // skipped: the elements of a row form one straight-line block that
-      // the compiler can interleave.
-      auto row_tile = [&](auto stg_c, int mi) {
-        constexpr int STG = decltype(stg_c)::value;
+      for (int mi = 0; mi < nM; ++mi, ++it) {
         const int k = mi * kTileRows + 32 * q + lane;
         const int b = it & 1;
         // band energies of this row: loaded before the wait, which hides them
         const double ekh = k < nk ? (Ee[k] + Eh[k]) * inv_hbar : 0.0;
+        // the state inputs of this row's elements do not depend on the
+        // accumulators either: for up to four wires per warp they are all
+        // loaded here, so their latency (shared memory, or L2 for the
+        // workspace) overlaps the MMAs and each other
+        constexpr bool kPre = WH <= 4;
+        float4 in_ys[kPre ? WH : 1], in_acc[kPre ? WH : 1], in_yf[kPre ? WH : 1];
+        double4 in_y[kPre ? WH : 1];
+        if constexpr (kPre) {
+#pragma unroll
+          for (int j = 0; j < WH; ++j) {
+            const int w = w0 + j;
+            in_ys[j] = in_acc[j] = in_yf[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+            in_y[j] = make_double4(0.0, 0.0, 0.0, 0.0);
+            if (k < nk && w < grp.nw) {
+              float4* ysp; float4* accp; float4* yfp;
+              ws_ptrs(w, k, ysp, accp, yfp);
+              in_ys[j] = *ysp;
+              if (stg != 0) in_acc[j] = *accp;
+              if (stg == 1 || stg == 2) in_yf[j] = *yfp;
+              if (stg == 3) in_y[j] = RES ? s_y[w * kpad + k] : g_y[woff[w] + k];
+            }
+          }
+        }
         bool got = mbar_wait(&dfull[b], (it >> 1) & 1, abort);
         got = __all_sync(0xffffffffu, got);
         if (got) tc_fence_after();
         // this lane's row takes part in this tile (abort read once per tile)
         const bool live = got && k < nk && !*abort;
         const uint32_t kofs = (uint32_t)(k >> 4) * 128 + (uint32_t)(k & 15);
-        const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
         for (int jp = 0; jp < WH; jp += 2) {
           // accumulators of wires w0+jp, w0+jp+1 (8 columns each)
@@ -912,91 +903,79 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
             tmem_ld8(col + N, r3);
             tmem_ld8(col + 2 * N, r4);
             tmem_ld_wait();
-          } else {
-#pragma unroll
-            for (int i = 0; i < 8; ++i) r2[i] = r3[i] = r4[i] = 0u;
           }
 #pragma unroll
           for (int u = 0; u < 2; ++u) {
             const int j = jp + u;
             const int w = w0 + j;
-            const bool ok = live && w < grp.nw;
-            float4* ysp; float4* accp; float4* yfp;
-            ws_ptrs(w, k, ysp, accp, yfp);
-            double4* yp = RES ? s_y + (w * kpad + k) : g_y + (woff[w] + k);
-            float4 ysf = zero4, af = zero4, yf = zero4;
-            double4 yv = make_double4(0.0, 0.0, 0.0, 0.0);
-            if (ok) {
-              ysf = *ysp;
-              if (STG != 0) af = *accp;
-              if (STG == 1 || STG == 2) yf = *yfp;
-              if (STG == 3) yv = *yp;
-            }
+            const float Mjr = __shfl_sync(0xffffffffu, Mr, j);
+            const float Mji = __shfl_sync(0xffffffffu, Mi, j);
+            if (!live || w >= grp.nw) continue;
             // exchange sums / hbar (SBEs.py:896-921) from the exact digit
             // products, rounded once to FP32
-            float4 fxw;
-            if constexpr (kHoist) fxw = wfx[j];
-            else fxw = *reinterpret_cast<const float4*>(fx + 4 * w);
-            const float fxc[4] = {fxw.x, fxw.y, fxw.z, fxw.w};
             float exh[4];
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
               const int cc = 4 * u + c;
               const float e = (float)(int)r2[cc] +
                               ((float)(int)r3[cc] + (float)(int)r4[cc] * inv_base) * inv_base;
-              exh[c] = e * fxc[c];
+              exh[c] = e * fx[4 * w + c];
             }
+            float4* ysp; float4* accp; float4* yfp;
+            ws_ptrs(w, k, ysp, accp, yfp);
+            float4 ysf;
+            if constexpr (kPre) ysf = in_ys[j]; else ysf = *ysp;
             // diagonal RHS (SBEs.py:1962-1975, 2325-2337, 2623-2636) / hbar:
             // phase and dephasing terms in FP64, Rabi terms in FP32
-            double gpw, gw;  // gap / hbar and gamma of the wire
-            if constexpr (kHoist) {
-              gpw = wgap[j];
-              gw = wgam[j];
-            } else {
-              gpw = gaph[w];
-              gw = wpar[w].y;
-            }
-            const float omr = wMr[j] + exh[0];
-            const float omi = wMi[j] + exh[1];
-            const double sumh = (ekh + gpw) - (double)(exh[2] + exh[3]);
+            const float omr = Mjr + exh[0];
+            const float omi = Mji + exh[1];
+            const double sumh = (ekh + gaph[w]) - (double)(exh[2] + exh[3]);
             const float nn = ysf.z + ysf.w - 1.f;
             const double prd = ysf.x, pid = ysf.y;
+            const double gw = wpar[w].y;  // gamma
             const float f0 = (float)(sumh * pid - gw * prd) - omi * nn;
             const float f1 = (float)(-(sumh * prd) - gw * pid) + omr * nn;
             const float f2 = 2.f * (omi * ysf.x - omr * ysf.y);
             // RK4 stage combination (integrator.py:143-157): acc = k1 + 2 k2
             // + 2 k3 and the stage points in FP32, y += h/6 (acc + k4) in FP64
             float4 nxt;
-            if constexpr (STG == 0) {
-              if (ok) *accp = make_float4(f0, f1, f2, f2);
+            float4 af, yf;
+            double4 yv;
+            if constexpr (kPre) {
+              af = in_acc[j];
+              yf = in_yf[j];
+              yv = in_y[j];
+            } else {
+              if (stg != 0) af = *accp;
+              if (stg == 1 || stg == 2) yf = *yfp;
+              if (stg == 3) yv = RES ? s_y[w * kpad + k] : g_y[woff[w] + k];
+            }
+            if (stg == 0) {
+              *accp = make_float4(f0, f1, f2, f2);
               // the stage-0 point is the FP32 copy of y
               nxt = make_float4(ysf.x + h2f * f0, ysf.y + h2f * f1, ysf.z + h2f * f2,
                                 ysf.w + h2f * f2);
-            } else if constexpr (STG == 3) {
+            } else if (stg == 3) {
+              double4* yp = RES ? s_y + (w * kpad + k) : g_y + (woff[w] + k);
               yv.x += (double)(h6f * (af.x + f0));
               yv.y += (double)(h6f * (af.y + f1));
               yv.z += (double)(h6f * (af.z + f2));
               yv.w += (double)(h6f * (af.w + f2));
+              *yp = yv;
               nxt = make_float4((float)yv.x, (float)yv.y, (float)yv.z, (float)yv.w);
-              if (ok) {
-                *yp = yv;
-                *yfp = nxt;
-                pr[j] += yv.x;
-                pim[j] += yv.y;
-              }
+              *yfp = nxt;
+              pr[j] += yv.x;
+              pim[j] += yv.y;
             } else {
-              if (ok)
-                *accp = make_float4(af.x + 2.f * f0, af.y + 2.f * f1, af.z + 2.f * f2,
-                                    af.w + 2.f * f2);
-              const float c2 = STG == 1 ? h2f : hf;
+              *accp = make_float4(af.x + 2.f * f0, af.y + 2.f * f1, af.z + 2.f * f2,
+                                  af.w + 2.f * f2);
+              const float c2 = stg == 1 ? h2f : hf;
               nxt = make_float4(yf.x + c2 * f0, yf.y + c2 * f1, yf.z + c2 * f2, yf.w + c2 * f2);
             }
-            if (ok) *ysp = nxt;
-            track(cm, j, ok ? nxt : zero4);
+            *ysp = nxt;
+            track(cm, j, nxt);
             // digits of the next stage point with the lagged column scales
-            float4 sc;
-            if constexpr (kHoist) sc = wsc[j];
-            else sc = *reinterpret_cast<const float4*>(scw + 4 * w);
+            const float4 sc = *reinterpret_cast<const float4*>(scw + 4 * w);
             const float xv[4] = {nxt.x * sc.x, nxt.y * sc.y, nxt.z * sc.z, nxt.w * sc.w};
             // x_off(k, 4w + c): columns 4w..4w+3 share a core matrix
             const uint32_t obase = (uint32_t)(w >> 1) * xsbo + (uint32_t)(w & 1) * 64 + kofs;
@@ -1005,12 +984,13 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
               int d1, d2, d3;
               digits3(xv[c], d1, d2, d3);
               const uint32_t o = obase + 16 * c;
-              if (ok) {
-                xn[o] = (uint8_t)d1;
-                xn[L.plane + o] = (uint8_t)d2;
-                xn[2 * L.plane + o] = (uint8_t)d3;
+              xn[o] = (uint8_t)d1;
+              xn[L.plane + o] = (uint8_t)d2;
+              xn[2 * L.plane + o] = (uint8_t)d3;
+              if (!(fabsf(xv[c]) < 0.5f)) {
+                ovn[4 * w + c] = 1;
+                ovf_any[bn] = 1;
               }
-              ovbits |= (uint32_t)(ok && !(fabsf(xv[c]) < 0.5f)) << (4 * j + c);
             }
           }
         }
@@ -1018,20 +998,6 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
         tc_fence_before();
         __syncwarp();
         if (lane == 0 && got) mbar_arrive(&dfree[b]);
-      };
-      for (int mi = 0; mi < nM; ++mi, ++it) {
-        switch (stg) {
-          case 0: row_tile(std::integral_constant<int, 0>{}, mi); break;
-          case 1: row_tile(std::integral_constant<int, 1>{}, mi); break;
-          case 2: row_tile(std::integral_constant<int, 2>{}, mi); break;
-          default: row_tile(std::integral_constant<int, 3>{}, mi); break;
-        }
-      }
-      if (ovbits) {
-#pragma unroll
-        for (int i = 0; i < 4 * WH; ++i)
-          if (ovbits & (1u << i)) ovn[4 * w0 + i] = 1;
-        ovf_any[bn] = 1;
       }
       publish_colmax(cm);
       if (stg == 3) {
