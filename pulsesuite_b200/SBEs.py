@@ -192,8 +192,9 @@ def _derivs(C, D, p, Heh, Hee, Hhh, GamE, GamH, Off):
     h = np.stack([heh, hee, hhh], 1).astype(np.complex128)
     st = np.stack([pd, c, d], 1).astype(np.complex128)
     # one host->device copy of the packed inputs, one kernel, one copy back
+    off = np.ascontiguousarray(np.broadcast_to(np.asarray(off, dtype=np.complex128), (nk,)))
     packed = np.concatenate([h.view(np.float64).reshape(-1), st.view(np.float64).reshape(-1),
-                             g, np.asarray(off, dtype=np.complex128).view(np.float64)])
+                             g, off.view(np.float64)])
     buf = torch.as_tensor(packed, device="cuda")
     out = torch.empty(6 * nk, dtype=torch.float64, device="cuda")
     base = buf.data_ptr()
