@@ -864,29 +864,6 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
         const int b = it & 1;
         // band energies of this row: loaded before the wait, which hides them
         const double ekh = k < nk ? (Ee[k] + Eh[k]) * inv_hbar : 0.0;
-        // the state inputs of this row's elements do not depend on the
-        // accumulators either: for up to four wires per warp they are all
-        // loaded here, so their latency (shared memory, or L2 for the
-        // workspace) overlaps the MMAs and each other
-        constexpr bool kPre = WH <= 4;
-        float4 in_ys[kPre ? WH : 1], in_acc[kPre ? WH : 1], in_yf[kPre ? WH : 1];
-        double4 in_y[kPre ? WH : 1];
-        if constexpr (kPre) {
-#pragma unroll
-          for (int j = 0; j < WH; ++j) {
-            const int w = w0 + j;
-            in_ys[j] = in_acc[j] = in_yf[j] = make_float4(0.f, 0.f, 0.f, 0.f);
-            in_y[j] = make_double4(0.0, 0.0, 0.0, 0.0);
-            if (k < nk && w < grp.nw) {
-              float4* ysp; float4* accp; float4* yfp;
-              ws_ptrs(w, k, ysp, accp, yfp);
-              in_ys[j] = *ysp;
-              if (stg != 0) in_acc[j] = *accp;
-              if (stg == 1 || stg == 2) in_yf[j] = *yfp;
-              if (stg == 3) in_y[j] = RES ? s_y[w * kpad + k] : g_y[woff[w] + k];
-            }
-          }
-        }
         bool got = mbar_wait(&dfull[b], (it >> 1) & 1, abort);
         got = __all_sync(0xffffffffu, got);
         if (got) tc_fence_after();
@@ -923,8 +900,7 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
             }
             float4* ysp; float4* accp; float4* yfp;
             ws_ptrs(w, k, ysp, accp, yfp);
-            float4 ysf;
-            if constexpr (kPre) ysf = in_ys[j]; else ysf = *ysp;
+            const float4 ysf = *ysp;
             // diagonal RHS (SBEs.py:1962-1975, 2325-2337, 2623-2636) / hbar:
             // phase and dephasing terms in FP64, Rabi terms in FP32
             const float omr = Mjr + exh[0];
@@ -939,24 +915,15 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
             // RK4 stage combination (integrator.py:143-157): acc = k1 + 2 k2
             // + 2 k3 and the stage points in FP32, y += h/6 (acc + k4) in FP64
             float4 nxt;
-            float4 af, yf;
-            double4 yv;
-            if constexpr (kPre) {
-              af = in_acc[j];
-              yf = in_yf[j];
-              yv = in_y[j];
-            } else {
-              if (stg != 0) af = *accp;
-              if (stg == 1 || stg == 2) yf = *yfp;
-              if (stg == 3) yv = RES ? s_y[w * kpad + k] : g_y[woff[w] + k];
-            }
             if (stg == 0) {
               *accp = make_float4(f0, f1, f2, f2);
               // the stage-0 point is the FP32 copy of y
               nxt = make_float4(ysf.x + h2f * f0, ysf.y + h2f * f1, ysf.z + h2f * f2,
                                 ysf.w + h2f * f2);
             } else if (stg == 3) {
+              const float4 af = *accp;
               double4* yp = RES ? s_y + (w * kpad + k) : g_y + (woff[w] + k);
+              double4 yv = *yp;
               yv.x += (double)(h6f * (af.x + f0));
               yv.y += (double)(h6f * (af.y + f1));
               yv.z += (double)(h6f * (af.z + f2));
@@ -967,8 +934,10 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
               pr[j] += yv.x;
               pim[j] += yv.y;
             } else {
+              const float4 af = *accp;
               *accp = make_float4(af.x + 2.f * f0, af.y + 2.f * f1, af.z + 2.f * f2,
                                   af.w + 2.f * f2);
+              const float4 yf = *yfp;
               const float c2 = stg == 1 ? h2f : hf;
               nxt = make_float4(yf.x + c2 * f0, yf.y + c2 * f1, yf.z + c2 * f2, yf.w + c2 * f2);
             }
