@@ -89,6 +89,8 @@ def parse():
     ap.add_argument("--capacity-requests", type=int, default=24000,
                     help="c4: backlog of the saturated capacity runs (both forms)")
     ap.add_argument("--no-serve", action="store_true", help="c4: skip the serving runs")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="launch each bench step eagerly instead of replaying its CUDA graph")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reference-baseline", action="store_true",
@@ -419,15 +421,24 @@ def oracle_accuracy(wl, nsteps, stream, nsample=16):
             "n_rel_err_max": float(np.max(en))}
 
 
-def timed_steps(b, S, dt, K, W, stream, flush, world):
+def timed_steps(b, S, dt, K, W, stream, flush, world, graph=True):
     """W warm-up bench steps, then K bench steps of S time steps each, every
     one bracketed by CUDA events on `stream` with an L2 flush between them
-    (outside the events); total device ms, max over ranks."""
+    (outside the events); total device ms, max over ranks.  With `graph` a
+    bench step is one replay of the CUDA graph of the batch's rk4 call."""
     import torch
     import torch.distributed as dist
 
+    if graph:
+        g = b.capture(S, dt, p_stride=1)
+
+        def step():
+            g.replay()
+    else:
+        def step():
+            b.rk4(S, dt, p_stride=1, stream=stream)
     for _ in range(W):
-        b.rk4(S, dt, stream=stream)
+        step()
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -437,7 +448,7 @@ def timed_steps(b, S, dt, K, W, stream, flush, world):
     for i in range(K):
         flush.fill_(float(i))
         evs[i][0].record(stream)
-        b.rk4(S, dt, p_stride=1, stream=stream)
+        step()
         evs[i][1].record(stream)
     torch.cuda.synchronize()
     total_ms = float(sum(e0.elapsed_time(e1) for e0, e1 in evs))
@@ -601,13 +612,15 @@ def run_ours(a):
     units = wl.units_per_step * S
 
     with Clocks(local) as clk:
-        total_ms = timed_steps(b, S, wl.dt, a.steps, a.warmup, stream, flush, world)
+        total_ms = timed_steps(b, S, wl.dt, a.steps, a.warmup, stream, flush, world,
+                               graph=not a.no_graph)
     value = units * a.steps * world / (total_ms * 1e-3)
     status = b.wires()["status"]
     plain = None
     if form == "split" and not a.no_plain:
         bp = WireBatch(wl.grids, wl.wires, screened=wl.screened, p_cap=S, form="plain")
-        pms = timed_steps(bp, S, wl.dt, a.steps, a.warmup, stream, flush, world)
+        pms = timed_steps(bp, S, wl.dt, a.steps, a.warmup, stream, flush, world,
+                          graph=not a.no_graph)
         pval = units * a.steps * world / (pms * 1e-3)
         fp64 = fp64_peak_tflops(torch, _lib, device)
         pach = wl.flops_per_step() * S / (pms / a.steps * 1e-3) / 1e12
@@ -681,6 +694,7 @@ def run_ours(a):
                      "traffic_source": TRAFFIC_SOURCE, "peak_source": peak_source,
                      "flops_per_launch": flops_launch},
         "gpu_launches": a.steps * b.launches_per_call,
+        "launch": "eager" if a.no_graph else "CUDA graph replay per bench step",
         "plain": plain,
         "accuracy": accuracy,
         "serving": serving,

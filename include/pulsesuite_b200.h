@@ -274,6 +274,16 @@ typedef struct PsbSplitGroup {
   int32_t wire[PSB_SPLIT_WMAX];
 } PsbSplitGroup;
 
+/*
+ * Polls a bounded on-chip hand-off wait of the split kernel makes before it
+ * gives up (0 restores the default, 2^26).  A wait that runs out makes its
+ * CTA stop: it waits (bounded) for its MMAs in flight, frees its tensor
+ * memory and reports PSB_ERR_TIMEOUT in the status of its wires; the call
+ * and the context stay usable.  Applies to launches issued after the call
+ * (process-wide); a small value makes the waits run out on purpose, which
+ * is how the timeout path is tested.
+ */
+int psb_split_set_wait_limit(uint32_t spins);
 /* Workspace bytes psb_rk4_split needs for n_state elements. */
 int64_t psb_split_ws_bytes(int64_t n_state);
 /* Dynamic shared memory (bytes) of one CTA for a grid of nk, wgroup 4, 8

@@ -25,7 +25,7 @@ class WireBatch:
     psb_rk4_split)."""
 
     def __init__(self, grids, wires, screened=False, excitons=True, p_cap=0, tables=None,
-                 tabdata=None, form="plain", split_w=None):
+                 tabdata=None, form="plain", split_w=None, tune=True):
         device.require_cuda()
         if form not in ("plain", "split"):
             raise ValueError("form must be 'plain' or 'split'")
@@ -33,6 +33,7 @@ class WireBatch:
         # split form: wires per CTA group by grid size, {nk: 4, 8 or 16}; grids
         # not listed use the built-in rule (see _setup_split)
         self.split_w = dict(split_w or {})
+        self.tune = bool(tune)
         self.grids = list(grids)
         self.screened = bool(screened)
         if tables is None:
@@ -88,12 +89,12 @@ class WireBatch:
     def _setup_split(self):
         """Wire groups (one CTA each) and the workspace of the split form.
 
-        A group holds up to W in {4, 8, 16} wires of one grid.  The exchange
-        work of a group per step is ~W Nk^2, so W is chosen per grid to give
-        roughly two waves of equal CTAs over the SMs (W = 4 for large grids,
-        W = 8 once a grid has enough wires: the MMAs are twice as wide at the
-        same issue cost; W = 16 only where ``split_w`` asks for it, since its
-        epilogue runs from the workspace).  Groups are launched in classes of (W, state
+        A group holds up to W in {4, 8, 16} wires of one grid.  W is chosen
+        per grid by the autotuner (tune.SplitTuner: measured per-CTA cost of
+        each W on this device, times the waves of CTAs the grid's wire count
+        needs); with ``tune=False`` by a rule (W = 8 once a grid has enough
+        wires for roughly two waves of CTAs, else 4); ``split_w`` overrides
+        both per grid.  Groups are launched in classes of (W, state
         resident in shared memory or not) so that a large grid does not push
         the small ones out of the resident layout; the classes run
         concurrently on side streams, the one with the largest grid first."""
@@ -114,7 +115,11 @@ class WireBatch:
             if counts[t] == 0:
                 continue
             wg = 4
-            if nk <= maxnk[8] and 8 * nk * nk <= max(target, 4 * nk * nk):
+            if self.tune:
+                from .tune import shared_tuner
+
+                wg = shared_tuner().best_width(nk, int(counts[t]))
+            elif nk <= maxnk[8] and 8 * nk * nk <= max(target, 4 * nk * nk):
                 wg = 8
             if nk in self.split_w:
                 wg = int(self.split_w[nk])
@@ -213,6 +218,26 @@ class WireBatch:
                       device.ptr(self.y), self.n_state, nkmax, flags, int(nsteps), float(dt),
                       device.ptr(self.P), self.P.shape[0], int(p_stride), self.p_cap,
                       abi.as_ptr(self.model), device.stream_ptr(stream))
+
+    def capture(self, nsteps, dt, p_stride=1):
+        """A CUDA graph of one ``rk4(nsteps, dt, p_stride)`` call (every size
+        class's launch, the split form's side streams and their joins), to
+        replay with ``graph.replay()`` on the current stream: one host call
+        per step instead of one launch per class plus the stream
+        synchronisation.  The graph reads and writes this batch's own state,
+        wire descriptors and P(t) buffers, so a caller changes the data
+        between replays (``set_state``, the wire descriptors), not the
+        shapes.  One eager call first sets the kernels' attributes outside
+        the capture (it advances the batch like any rk4 call)."""
+        import torch
+
+        self.rk4(nsteps, dt, p_stride=p_stride)
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self.rk4(nsteps, dt, p_stride=p_stride)
+        torch.cuda.synchronize()
+        return g
 
     def leapfrog(self, field, nsteps, dt, p_stride=1, stream=None):
         """field: device float64 tensor (nw, 2*n_samples) of sampled E(t_n)."""

@@ -65,6 +65,8 @@
 // returns.
 #include <math.h>
 
+#include <atomic>
+
 #include "psb_common.cuh"
 
 namespace psb {
@@ -94,6 +96,9 @@ constexpr int kPlaneCols = kTileK / 4;            // TMEM columns of one digit p
 constexpr int kTileCols = kDigits * kPlaneCols;   // 48
 constexpr int kTmemCols = 512;
 constexpr double kBase = 254.0;
+// Polls of one bounded hand-off wait before it gives up (the default of
+// psb_split_set_wait_limit; the teardown wait for the last MMAs always uses
+// this value).
 constexpr uint32_t kSpinLimit = 1u << 26;
 // dynamic shared memory per CTA (the 227 KiB limit less the static
 // shared memory and alignment padding)
@@ -139,8 +144,9 @@ __device__ __forceinline__ bool mbar_test_wait(uint64_t* bar, uint32_t parity) {
 // abort) or another role aborted.  Spinning with test_wait rather than
 // suspending in try_wait keeps the hand-off latency between the MMA issuer,
 // the generators and the drain warps short.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort) {
-  for (uint32_t i = 0; i < kSpinLimit; ++i) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort,
+                                          uint32_t limit) {
+  for (uint32_t i = 0; i < limit; ++i) {
     if (mbar_test_wait(bar, parity)) return true;
     if (*abort) return false;
   }
@@ -301,6 +307,7 @@ struct Args {
   int p_cap;
   double hbar;
   uint32_t smem_bytes;  // dynamic shared memory of the launch
+  uint32_t spin_limit;  // polls of a bounded hand-off wait (>= 1)
 };
 
 // Shared-memory layout of one CTA.  RES: the element state (y double4,
@@ -693,7 +700,7 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
     uint32_t gph = 0; // parity of that buffer's current fill
     const int G = nslot / 2;
     auto warp_wait = [&](uint64_t* bar, uint32_t parity) -> bool {
-      const bool got = mbar_wait(bar, parity, abort);
+      const bool got = mbar_wait(bar, parity, abort, a.spin_limit);
       return __all_sync(0xffffffffu, got);
     };
     // (an abort is seen through the stage-end snapshot and inside every
@@ -708,7 +715,8 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
         for (int mi = 0; ok && mi < nM; ++mi, ++it) {
           const int b = it & 1;
           // every lane polls; the vote on the outcome comes at the tile end
-          if (it >= 2 && !mbar_wait(&dfree[b], ((it >> 1) - 1) & 1, abort)) ok = false;
+          if (it >= 2 && !mbar_wait(&dfree[b], ((it >> 1) - 1) & 1, abort, a.spin_limit))
+            ok = false;
           tc_fence_after();
           const uint32_t d2 = tmem + (uint32_t)(3 * N * b);
           const uint32_t d3 = d2 + (uint32_t)N;
@@ -739,7 +747,7 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
             // as the poll.
             for (int k0 = 0; ok && k0 < nK; k0 += G) {
               const int gn = min(G, nK - k0);
-              if (!mbar_wait(&afull[gb], gph, abort)) {
+              if (!mbar_wait(&afull[gb], gph, abort, a.spin_limit)) {
                 ok = false;
                 break;
               }
@@ -804,7 +812,7 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
         for (int mi = 0; mi < nM && !*abort; ++mi) {
           for (int k0 = 0; k0 < nK; k0 += G) {
             const int gn = min(G, nK - k0);
-            bool got = first || mbar_wait(&afree[gb], gph ^ 1u, abort);
+            bool got = first || mbar_wait(&afree[gb], gph ^ 1u, abort, a.spin_limit);
             got = __all_sync(0xffffffffu, got);
             if (!got) break;
             tc_fence_after();
@@ -864,7 +872,7 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
         const int b = it & 1;
         // band energies of this row: loaded before the wait, which hides them
         const double ekh = k < nk ? (Ee[k] + Eh[k]) * inv_hbar : 0.0;
-        bool got = mbar_wait(&dfull[b], (it >> 1) & 1, abort);
+        bool got = mbar_wait(&dfull[b], (it >> 1) & 1, abort, a.spin_limit);
         got = __all_sync(0xffffffffu, got);
         if (got) tc_fence_after();
         // this lane's row takes part in this tile (abort read once per tile)
@@ -1118,6 +1126,17 @@ int launch(const Args& a, int nkmax, cudaStream_t s) {
 
 using namespace psb;
 
+namespace psb {
+namespace split {
+static std::atomic<uint32_t> g_spin_limit{kSpinLimit};
+}  // namespace split
+}  // namespace psb
+
+extern "C" int psb_split_set_wait_limit(uint32_t spins) {
+  split::g_spin_limit.store(spins == 0 ? split::kSpinLimit : spins);
+  return PSB_OK;
+}
+
 extern "C" int64_t psb_split_ws_bytes(int64_t n_state) {
   if (n_state < 0) return set_error(PSB_ERR_INVALID, "n_state < 0");
   return 64 * n_state + 32;
@@ -1196,6 +1215,7 @@ extern "C" int psb_rk4_split(const PsbTable* d_tables, int ntab, const double* d
   a.p_stride = p_stride;
   a.p_cap = p_cap;
   a.hbar = model->hbar;
+  a.spin_limit = split::g_spin_limit.load();
   cudaStream_t st = (cudaStream_t)stream;
   if (wgroup == 16) return split::launch<16>(a, nkmax, st);
   return wgroup == 8 ? split::launch<8>(a, nkmax, st) : split::launch<4>(a, nkmax, st);

@@ -36,16 +36,20 @@ import numpy as np
 from . import abi
 
 EV = 1.602176634e-19
+# Result.status of a request cancelled before it finished (host-side status;
+# the kernel statuses are the PSB_* codes, all >= -6)
+STATUS_CANCELLED = -100
 # Nk classes of the serving stream and their probabilities
 C4_NKS = (64, 128, 256, 512, 1024)
 C4_PROBS = (0.3, 0.3, 0.2, 0.15, 0.05)
 
-# Cost model of the split-form scheduler: time of one CTA for one 50-step
-# launch (ms, one CTA per SM, full waves), measured on a B200, by grid size
-# and wires per CTA.  8 wires double the width of every MMA at the same
-# issue count, so a CTA of 8 takes only 1.2-1.6x as long as a CTA of 4:
-# more throughput, more latency.  Other grid sizes scale from the nearest
-# entry by Nk^2 (the exchange work per wire).
+# Default cost model of the split-form scheduler (the server measures its
+# own with tune.SplitTuner on the device it runs on): time of one CTA for
+# one 50-step launch (ms, one CTA per SM, full waves), measured on a B200,
+# by grid size and wires per CTA.  8 wires double the width of every MMA at
+# the same issue count, so a CTA of 8 takes only 1.2-1.6x as long as a CTA
+# of 4: more throughput, more latency.  Other grid sizes scale from the
+# nearest entry by Nk^2 (the exchange work per wire).
 SPLIT_CTA_MS = {(64, 4): 0.49, (64, 8): 0.73, (128, 4): 0.58, (128, 8): 0.84,
                 (256, 4): 0.90, (256, 8): 1.37, (512, 4): 2.53, (512, 8): 3.96,
                 (1024, 4): 8.15, (1024, 8): 9.71}
@@ -57,34 +61,25 @@ def split_cta_cost(nk, w):
     return SPLIT_CTA_MS[(ref, w)] * (nk / ref) ** 2
 
 
-def choose_wires_per_cta(counts, sms, w8_ok=lambda nk: True):
-    """Wires per CTA (4 or 8) of each grid size for one tick.
+def choose_wires_per_cta(counts, sms, w8_ok=lambda nk: True, cost=None, allowed=None):
+    """Wires per CTA of each grid size for one tick.
 
     counts: {nk: solves of that size in the tick}.  A tick lasts about
     max(longest CTA, total CTA time / SMs): with few solves the longest CTA
-    sets it and 4 wires per CTA give the shorter tick (lower latency); once
-    the SMs are full the total sets it and 8 wires per CTA give more
-    throughput.  Starting from 4 everywhere, each size (largest first)
-    moves to 8 if that shortens the estimated tick, or keeps it and frees
-    SM time."""
-    w = {nk: 4 for nk, c in counts.items() if c}
+    sets it and narrow groups give the shorter tick (lower latency); once
+    the SMs are full the total sets it and wide groups give more
+    throughput.  Starting from the narrowest group everywhere, each size
+    (largest first) widens if that shortens the estimated tick, or keeps it
+    and frees SM time (tune.choose_widths).  Without ``cost`` / ``allowed``
+    the default table above is used with widths 4 and 8 (8 where w8_ok)."""
+    from .tune import choose_widths
 
-    def tick(wm):
-        total = sum(-(-counts[nk] // wm[nk]) * split_cta_cost(nk, wm[nk]) for nk in wm)
-        return (max(max(split_cta_cost(nk, wm[nk]) for nk in wm), total / sms), total)
-
-    if not w:
-        return w
-    best = tick(w)
-    for nk in sorted(w, reverse=True):
-        if not w8_ok(nk):
-            continue
-        trial = dict(w)
-        trial[nk] = 8
-        t = tick(trial)
-        if t < best:
-            w, best = trial, t
-    return w
+    if cost is None:
+        cost = split_cta_cost
+    if allowed is None:
+        def allowed(nk):
+            return (4, 8) if w8_ok(nk) else (4,)
+    return choose_widths(counts, sms, cost, allowed)
 
 
 @dataclass
@@ -186,7 +181,7 @@ class Server:
     saturated capacity within the run-to-run spread)."""
 
     def __init__(self, form="split", chunk=50, max_steps=4000, capacity=None,
-                 hbm_budget=150e9, nks=C4_NKS, max_inflight_ticks=2):
+                 hbm_budget=150e9, nks=C4_NKS, max_inflight_ticks=2, hbm_headroom=2 << 30):
         import torch
         from scipy.constants import hbar
 
@@ -206,7 +201,22 @@ class Server:
         self.h_tables = np.ascontiguousarray(tables)
         self.d_tables = device.to_device(self.h_tables)
         cap = dict(capacity or default_capacity(self.nks))
-        self.pool = SlotPool(cap, hbm_budget)
+        # The resident pool (every slot's state, workspace and P(t) records)
+        # is allocated once, here, and sized by the device's free memory
+        # now: if it does not fit min(hbm_budget, free - headroom), every
+        # class is scaled down (at least one slot each).  Requests are then
+        # admitted into free slots within the same byte budget.
+        free, total = torch.cuda.mem_get_info()
+        self.hbm_free_at_start, self.hbm_total = int(free), int(total)
+        per_slot = {nk: request_bytes(nk, self.max_steps, form) for nk in self.nks}
+        need = sum(cap[nk] * per_slot[nk] for nk in self.nks)
+        fit = min(float(hbm_budget), float(free) - float(hbm_headroom))
+        if need > fit:
+            scale = max(0.0, fit) / need
+            cap = {nk: max(1, int(cap[nk] * scale)) for nk in self.nks}
+            need = sum(cap[nk] * per_slot[nk] for nk in self.nks)
+        self.pool_bytes = need
+        self.pool = SlotPool(cap, min(float(hbm_budget), float(need)))
         # slot layout: class c holds cap[nk] slots; global slot index g
         self.cls_base, base, off = {}, 0, 0
         self.slot_off = []
@@ -234,10 +244,16 @@ class Server:
         if form == "split":
             self.ws = torch.empty(int(lib.psb_split_ws_bytes(self.n_state)), dtype=torch.uint8,
                                   device="cuda")
-            # wires per CTA are chosen per tick (choose_wires_per_cta); 8
-            # only where that group fits in shared memory
-            self.w8_max = int(lib.psb_split_max_nk(8))
-            self.sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+            # wires per CTA are chosen per tick (choose_wires_per_cta) from
+            # per-CTA costs measured on this device for the served grids
+            from .tune import shared_tuner
+
+            self.tuner = shared_tuner()
+            self.tuner.table(self.nks)
+            self.sms = self.tuner.sms
+            # per-tick cost of a CTA: the tuner's per-step cost times the tick
+            self._cta_cost = functools.lru_cache(maxsize=None)(
+                lambda nk, w: self.tuner.cost(nk, w) * self.chunk)
         self.model = abi.model_array(hbar)
         self.copy_stream = torch.cuda.Stream()
         self.isz = abi.WIRE_DTYPE.itemsize
@@ -269,6 +285,8 @@ class Server:
         self._ar = {nk: torch.arange(nk, dtype=torch.int64, device="cuda") for nk in self.nks}
         self.pending = []  # retiring batches: (event, entries, host buffers)
         self.results = []
+        self._cancel = set()  # request ids to cancel
+        self._cancelled = set()  # active slots cancelled (retire with STATUS_CANCELLED)
         self.reset_counters()
 
     def reset_counters(self):
@@ -375,7 +393,8 @@ class Server:
         if self.form == "split":
             # the classes share the SMs, so the choice sees every lane's load
             counts = {ln.nk: len(ln.slots) for ln in self.lanes}
-            wg = choose_wires_per_cta(counts, self.sms, lambda n: n <= self.w8_max)[nk]
+            wg = choose_wires_per_cta(counts, self.sms, cost=self._cta_cost,
+                                      allowed=self.tuner.allowed)[nk]
             ng = (slots.size + wg - 1) // wg
             grp = np.zeros(ng, dtype=abi.SPLIT_GROUP_DTYPE)
             grp["table"] = ti
@@ -431,7 +450,11 @@ class Server:
         lane's stream (the current stream), then copy them to pinned host
         memory on the copy stream."""
         torch = self.torch
-        entries = [(int(g), *self.active.pop(int(g))) for g in fin]
+        # (slot, request, steps done, admission time, bytes)
+        entries = []
+        for g in fin:
+            req, _, admitted, nbytes = self.active.pop(int(g))
+            entries.append((int(g), req, int(self.steps_done[int(g)]), admitted, nbytes))
         for g in fin:
             lane.slots.discard(int(g))
         rows = self._rows(foff_t, lane.nk)
@@ -470,16 +493,49 @@ class Server:
             P, Y = hP.numpy(), hy.numpy()
             W = hw.numpy().reshape(-1).view(abi.WIRE_DTYPE)
             o = 0
-            for i, (g, req, _, admitted, nbytes) in enumerate(entries):
-                p = P[i, :req.nsteps]
-                self.results.append(Result(req.rid, req.nk, req.nsteps, req.arrival, admitted, now,
-                                           int(W["status"][i]), p[:, 0] + 1j * p[:, 1],
+            for i, (g, req, done, admitted, nbytes) in enumerate(entries):
+                status, nsteps = int(W["status"][i]), req.nsteps
+                if req.rid in self._cancelled:
+                    self._cancelled.discard(req.rid)
+                    status, nsteps = STATUS_CANCELLED, min(req.nsteps, int(done))
+                p = P[i, :nsteps]
+                self.results.append(Result(req.rid, req.nk, nsteps, req.arrival, admitted, now,
+                                           status, p[:, 0] + 1j * p[:, 1],
                                            Y[o:o + req.nk].copy()))
                 o += req.nk
                 self.pool.give_back(req.nk, g - self.cls_base[req.nk], nbytes)
         self.pending = keep
 
-    def run(self, requests, realtime=True, max_inflight_ticks=None):
+    def cancel(self, rid):
+        """Cancel request ``rid``: a waiting request leaves its queue at once,
+        a running one retires at its next tick boundary (its P(t) records and
+        state up to there are returned); either way its Result has status
+        STATUS_CANCELLED."""
+        self._cancel.add(int(rid))
+
+    def _apply_cancels(self, now):
+        if not self._cancel:
+            return
+        for lane in self.lanes:
+            keep = []
+            for req in lane.waiting:
+                if req.rid in self._cancel:
+                    self._cancel.discard(req.rid)
+                    self.results.append(Result(req.rid, req.nk, 0, req.arrival, now, now,
+                                               STATUS_CANCELLED, np.zeros(0, complex),
+                                               np.zeros((0, 4))))
+                else:
+                    keep.append(req)
+            lane.waiting = keep
+        for g, entry in self.active.items():
+            req = entry[0]
+            if req.rid in self._cancel:
+                self._cancel.discard(req.rid)
+                self._cancelled.add(req.rid)
+                # finish with the next tick: its end is the tick boundary
+                self.steps_req[g] = min(self.steps_req[g], self.steps_done[g] + self.chunk)
+
+    def run(self, requests, realtime=True, max_inflight_ticks=None, cancels=()):
         """Serve ``requests``.  realtime: arrivals are honoured on the wall
         clock (the Poisson stream), else every request is available from the
         start (throughput / capacity runs).
@@ -488,7 +544,10 @@ class Server:
         ticks allow (at most ``max_inflight_ticks`` queued), so a small
         solve advances at its own kernel's pace instead of waiting each tick
         for the largest grid; the classes' launches run concurrently on the
-        GPU.  Largest grids are served first in each round."""
+        GPU.  Largest grids are served first in each round.
+
+        cancels: (time, rid) pairs; at that time (stream clock) ``cancel(rid)``
+        is applied, as a client withdrawing a request would."""
         if max_inflight_ticks is None:
             max_inflight_ticks = self.max_inflight
         assert max_inflight_ticks < self.ring
@@ -501,6 +560,8 @@ class Server:
         by_nk = {lane.nk: lane for lane in self.lanes}
         order = sorted(self.lanes, key=lambda ln: -ln.nk)
         qi, n = 0, len(queue)
+        cq = sorted(cancels)
+        ci = 0
         self.results = []
         self.t_start = time.perf_counter()
         while len(self.results) < n:
@@ -508,6 +569,10 @@ class Server:
             while qi < n and (not realtime or queue[qi].arrival <= now):
                 by_nk[queue[qi].nk].waiting.append(queue[qi])
                 qi += 1
+            while ci < len(cq) and cq[ci][0] <= now:
+                self.cancel(cq[ci][1])
+                ci += 1
+            self._apply_cancels(now)
             self._collect()
             issued = False
             for lane in order:
@@ -526,6 +591,7 @@ class Server:
                 time.sleep(max(0.0, min(1e-3, queue[qi].arrival - now)))
         self.torch.cuda.synchronize()
         self._collect(block=True)
+        self._cancel.clear()
         self.elapsed = time.perf_counter() - self.t_start
         return sorted(self.results, key=lambda r: r.rid)
 
