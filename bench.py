@@ -56,13 +56,22 @@ REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
 L2_FLUSH_BYTES = 256 << 20
-# DRAM bytes per state element and launch, from one ncu capture of each step
-# kernel (dram__bytes_read.sum + dram__bytes_write.sum over the elements of
-# the captured launch; traffic grows with the elements a launch advances,
-# not with its time steps)
-DRAM_BYTES_PER_ELEMENT = {"split": 9.99e6 / (1184 * 256), "plain": 9.91e6 / (1184 * 256)}
-TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + write.sum of the step kernels on 1184 wires x "
-                  "Nk 256, per element, times the elements of this step's launches")
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the step
+# kernels, from one ncu capture of a 20-step call on the configuration-4
+# request mix (16384 solves; profiles/split_rk4_kernel_c4_mix.md,
+# profiles/sbe_f64_kernel_c4_mix.md):
+#   split, state resident in shared memory: per element and launch (the
+#     FP64 state read once and written once)
+#   split, state in the workspace (groups whose grid does not fit shared
+#     memory): per element and time step (the FP32 stage state streams
+#     through L2 and, beyond its capacity, DRAM every stage)
+#   plain: per element and launch
+DRAM_SPLIT_RES_PER_ELEMENT = 75.0e6 / 1.770048e6
+DRAM_SPLIT_WS_PER_ELEMENT_STEP = 2.043e9 / (2.116608e6 * 20)
+DRAM_PLAIN_PER_ELEMENT = (72.03e6 + 43.39e6) / (1.770048e6 + 1.267712e6)
+TRAFFIC_SOURCE = ("ncu dram bytes per element (resident state, per launch) and per element "
+                  "and step (workspace state) of a 20-step capture on the c4 mix, applied to "
+                  "this step's launches")
 METRIC = "SBE wire*k*steps/s at <=1e-6 rel err vs FP64 (batched vs plain); p50/p99 latency"
 
 
@@ -383,6 +392,25 @@ def split_accuracy(wl, nsteps, stream):
             "p_err_vs_peak_median": float(np.median(errp))}
 
 
+def step_traffic(b, S):
+    """Estimated DRAM bytes of one bench step (see DRAM_* above)."""
+    if b.form == "plain":
+        return DRAM_PLAIN_PER_ELEMENT * b.n_state
+    from pulsesuite_b200 import _lib, abi
+
+    lib = _lib.load()
+    nks = b.h_tables["nk"]
+    total = 0.0
+    for wg, groups, ng, nkmax in b.split_launches:
+        g = groups.cpu().numpy().view(abi.SPLIT_GROUP_DTYPE)
+        elements = float(np.sum(g["nw"].astype(np.float64) * nks[g["table"]]))
+        if nkmax <= int(lib.psb_split_max_nk_resident(wg)):
+            total += DRAM_SPLIT_RES_PER_ELEMENT * elements
+        else:
+            total += DRAM_SPLIT_WS_PER_ELEMENT_STEP * elements * S
+    return total
+
+
 def oracle_accuracy(wl, nsteps, stream, nsample=16):
     """Plain-form error against the FP64 oracle on a sample of wires over
     `nsteps` (the check used where the split form does not apply)."""
@@ -684,7 +712,7 @@ def run_ours(a):
         peak, peak_source = 2.0 * peak, "2 x " + peak_source
         bound, unit = "tensor", "TOP/s"
     achieved = flops_launch / (avg_launch_ms * 1e-3) / 1e12
-    traffic = (DRAM_BYTES_PER_ELEMENT[form] * b.n_state) if b.n_state else None
+    traffic = step_traffic(b, S)
 
     line = {
         "metric": METRIC,
