@@ -26,6 +26,7 @@ Host-side logic (request stream, slot allocation, HBM accounting) is plain
 Python and tested without a GPU; the device path needs the sm_100a library.
 """
 
+import collections
 import functools
 import math
 import time
@@ -275,7 +276,7 @@ class Server:
             nb = max(1 << 16, 64 * cap[nk] + 8 * cap[nk] * abi.SPLIT_GROUP_DTYPE.itemsize)
             prio = min(least, greatest + rank[nk])
             self.lanes.append(Server._Lane(
-                ti, nk, torch.cuda.Stream(priority=prio),
+                ti, nk, self.cls_base[nk], cap[nk], torch.cuda.Stream(priority=prio),
                 [torch.empty(nb, dtype=torch.uint8, pin_memory=True) for _ in range(self.ring)],
                 [torch.empty(nb, dtype=torch.uint8, device="cuda") for _ in range(self.ring)]))
         self.tick = 0     # lane ticks issued, all lanes
@@ -285,6 +286,12 @@ class Server:
         self._ar = {nk: torch.arange(nk, dtype=torch.int64, device="cuda") for nk in self.nks}
         self.pending = []  # retiring batches: (event, entries, host buffers)
         self.results = []
+        # launch arguments that do not change between ticks
+        self._common = (device.ptr(self.d_tables), len(self.h_tables), device.ptr(self.tabdata),
+                        self.tabdata.numel(), device.ptr(self.d_wires), self.nslots)
+        self._y_ptr, self._P_ptr = device.ptr(self.y), device.ptr(self.P)
+        self._model_ptr = abi.as_ptr(self.model)
+        self._ws_ptr = device.ptr(self.ws) if form == "split" else None
         self._cancel = set()  # request ids to cancel
         self._cancelled = set()  # active slots cancelled (retire with STATUS_CANCELLED)
         self.reset_counters()
@@ -301,13 +308,24 @@ class Server:
         """One size class: stream, tick count, waiting requests, active
         slots, events of its ticks in flight, staging ring."""
 
-        def __init__(self, ti, nk, stream, stage_h, stage_d):
+        def __init__(self, ti, nk, base, cap, stream, stage_h, stage_d):
             self.ti, self.nk, self.stream = ti, nk, stream
             self.stage_h, self.stage_d = stage_h, stage_d
             self.tick = 0
-            self.waiting = []
-            self.slots = set()
+            self.waiting = collections.deque()
+            # active slots of the class as a mask over its slot range (the
+            # sorted slot list of a tick is one flatnonzero)
+            self.base = base
+            self.mask = np.zeros(cap, dtype=bool)
+            self.nactive = 0
             self.inflight = []
+
+        @property
+        def slots(self):
+            return self.nactive > 0
+
+        def slot_array(self):
+            return self.base + np.flatnonzero(self.mask).astype(np.int64)
 
     # -- staging -------------------------------------------------------------------
     class _Stage:
@@ -346,13 +364,14 @@ class Server:
         """Admit as many of the lane's waiting requests as slots and budget
         allow; returns the staged admission or None.  Their wire descriptors
         and zeroed state reach the device with this tick's staged copy."""
-        recs, slots, left = [], [], []
-        for req in lane.waiting:
+        recs, slots = [], []
+        while lane.waiting:
+            req = lane.waiting[0]
             nbytes = request_bytes(req.nk, req.nsteps, self.form)
-            sl = self.pool.try_take(req.nk, nbytes) if not left else None
+            sl = self.pool.try_take(req.nk, nbytes)
             if sl is None:
-                left.append(req)  # first come, first served within the class
-                continue
+                break  # first come, first served within the class
+            lane.waiting.popleft()
             g = self.cls_base[req.nk] + sl
             rec = wire_record(req, self.grids[lane.ti], table=lane.ti, off=self.slot_off[g],
                               p_off=g * self.max_steps)
@@ -362,8 +381,8 @@ class Server:
             self.active[g] = [req, 0, now, nbytes]
             self.steps_done[g] = 0
             self.steps_req[g] = req.nsteps
-            lane.slots.add(g)
-        lane.waiting = left
+            lane.mask[sl] = True
+            lane.nactive += 1
         if not slots:
             return None
         return (st.add(np.concatenate(recs)), st.add(np.asarray(slots, dtype=np.int64)),
@@ -379,7 +398,7 @@ class Server:
         adm = self._admit(lane, now, st)
         if not lane.slots:
             return False
-        slots = np.fromiter(sorted(lane.slots), dtype=np.int64)
+        slots = lane.slot_array()
         done = self.steps_done[slots]
         r_idx = st.add(slots)
         r_val = st.add(slots * self.max_steps + done)  # P(t) records append
@@ -392,7 +411,7 @@ class Server:
         nk, ti = lane.nk, lane.ti
         if self.form == "split":
             # the classes share the SMs, so the choice sees every lane's load
-            counts = {ln.nk: len(ln.slots) for ln in self.lanes}
+            counts = {ln.nk: ln.nactive for ln in self.lanes}
             wg = choose_wires_per_cta(counts, self.sms, cost=self._cta_cost,
                                       allowed=self.tuner.allowed)[nk]
             ng = (slots.size + wg - 1) // wg
@@ -408,8 +427,7 @@ class Server:
         else:
             wg = 0
             r_grp, n_launch = st.add(slots.astype(np.int32)), slots.size
-        common = (self.device.ptr(self.d_tables), len(self.h_tables), self.device.ptr(self.tabdata),
-                  self.tabdata.numel(), self.device.ptr(self.d_wires), self.nslots)
+        common = self._common
         dt = float(self.active[int(slots[0])][0].dt)
         sm = lane.stream
         self.h2d_bytes += st.n
@@ -425,15 +443,15 @@ class Server:
             ptr = self.device.ptr(st.view(r_grp, torch.uint8))
             if self.form == "split":
                 self._lib.call("psb_rk4_split", *common, ptr, n_launch, wg, nk,
-                               self.device.ptr(self.y), self.n_state, self.device.ptr(self.ws),
-                               self.ws.numel(), self.chunk, dt, self.device.ptr(self.P),
-                               self.P.shape[0], 1, self.max_steps, abi.as_ptr(self.model),
+                               self._y_ptr, self.n_state, self._ws_ptr,
+                               self.ws.numel(), self.chunk, dt, self._P_ptr,
+                               self.P.shape[0], 1, self.max_steps, self._model_ptr,
                                self.device.stream_ptr(sm))
             else:
                 flags = abi.PSB_TAB_SHARED_V if (self.h_tables["flags"][ti] & abi.PSB_TAB_SHARED_V) else 0
-                self._lib.call("psb_rk4_f64", *common, ptr, n_launch, self.device.ptr(self.y),
-                               self.n_state, nk, flags, self.chunk, dt, self.device.ptr(self.P),
-                               self.P.shape[0], 1, self.max_steps, abi.as_ptr(self.model),
+                self._lib.call("psb_rk4_f64", *common, ptr, n_launch, self._y_ptr,
+                               self.n_state, nk, flags, self.chunk, dt, self._P_ptr,
+                               self.P.shape[0], 1, self.max_steps, self._model_ptr,
                                self.device.stream_ptr(sm))
             self.steps_done[slots] += self.chunk
             if fin.size:
@@ -455,8 +473,8 @@ class Server:
         for g in fin:
             req, _, admitted, nbytes = self.active.pop(int(g))
             entries.append((int(g), req, int(self.steps_done[int(g)]), admitted, nbytes))
-        for g in fin:
-            lane.slots.discard(int(g))
+        lane.mask[fin - lane.base] = False
+        lane.nactive -= len(fin)
         rows = self._rows(foff_t, lane.nk)
         Pg = self.P.view(self.nslots, self.max_steps, 2).index_select(0, fin_t)
         yg = self.y.index_select(0, rows)
@@ -517,7 +535,7 @@ class Server:
         if not self._cancel:
             return
         for lane in self.lanes:
-            keep = []
+            keep = collections.deque()
             for req in lane.waiting:
                 if req.rid in self._cancel:
                     self._cancel.discard(req.rid)
