@@ -249,6 +249,63 @@ int psb_leapfrog_f64(const PsbTable* d_tables, int ntab, const double* d_tabdata
  * grid of nk points (for capacity planning; tab_flags as above). */
 int psb_f64_smem_bytes(int nk, int tab_flags);
 
+/* ---- full-matrix form (FP64): fields that vary along the wire ------------- */
+/*
+ * Constants of one wire's full-matrix step.  gam_e + gam_h is the dephasing
+ * of p (GamE, GamH of _preparation without k-dependent dephasing,
+ * SBEs.py:5213-5214); yw = yw(w) and sgnw = (-1)^w are the wire's dipole
+ * signs (qwoptics.py:1099-1112, SBEs.py:5171-5174).
+ */
+typedef struct PsbFullParams {
+  double ehint;     /* electron-hole overlap integral                          */
+  double dcv;       /* interband dipole (C m)                                  */
+  double yw;        /* yw(w)                                                   */
+  double sgnw;      /* (-1)^w                                                  */
+  double gap;       /* band gap (J), added to Ee on the diagonal of Hee         */
+  double gam_e;     /* 1/s                                                     */
+  double gam_h;     /* 1/s                                                     */
+  double hbar;      /* J s                                                     */
+  double dt;        /* step (s)                                                */
+  int32_t excitons; /* mb.params Excitons                                      */
+  int32_t lf;       /* mb.params LF: full Hee/Hhh with the direct terms        */
+} PsbFullParams;
+
+/* Work bytes psb_full_step_f64 needs for a grid of nk (Meh, H, dX). */
+int64_t psb_full_work_bytes(int nk);
+/*
+ * One step of the reference's integrator for one wire with full Nk x Nk
+ * states (SBESolver._sbe_calculator, SBEs.py:5624-5718): Meh from the
+ * wire-space fields (CalcMeh, SBEs.py:5165-5175), CalcH with the exchange
+ * and, with lf, direct Coulomb sums (SBEs.py:819-935), dpdt / dCdt / dDdt
+ * (SBEs.py:1952-1975, 2318-2337, 2617-2636), then X3 = X1 + 2 dt dX with the
+ * occupations |C3_kk|, |D3_kk| rescaled to a common total and X2 = (X1+X3)/2
+ * (SBEs.py:5681-5718).
+ *   d_V3      [3][nk] V_eh, V_ee, V_hh at index distance q (screened if the
+ *             caller screened them for this step, coulomb.py:1195-1230)
+ *   d_Ee/Eh   [nk] band energies
+ *   d_fields  [3][nr] complex: Ex, Ey, Ez in wire q space (after Prop2QW),
+ *             q index of k - k' at (k - k') + nq0
+ *   d_L1..L3  [3][nk][nk] complex each: the levels (p, C, D); the step reads
+ *             L2 (X1) and L3 (X2) and writes L1 = X1, L2 = (X1 + X3)/2,
+ *             L3 = X3 (the checkin of SBEs.py:5082-5092)
+ *   d_work    psb_full_work_bytes(nk) bytes
+ */
+int psb_full_step_f64(int nk, int nr, int nq0, const double* d_V3, const double* d_Ee,
+                      const double* d_Eh, const double* d_fields, const PsbFullParams* params,
+                      double* d_L1, double* d_L2, double* d_L3, void* d_work,
+                      int64_t n_work_bytes, void* stream);
+/*
+ * Wire-space source terms of one level (d_level = [3][nk][nk] complex p, C,
+ * D) on the wire grid r[nr] with the window[nr]: d_out[5][nr] complex =
+ * Px, Py, Pz as the sums of QWPolarization3 before the 2 ehint/(area L)
+ * factor and the transform (qwoptics.py:56-84), and the electron / hole
+ * densities as the sums of QWRho5 before the boundary offset, normalisation
+ * and transform (qwoptics.py:367-381, 948-1078).
+ */
+int psb_full_sources_f64(int nk, int nr, const double* d_kr, const double* d_r,
+                         const double* d_window, double L, double dcv, double yw, double sgnw,
+                         const double* d_level, double* d_out, void* stream);
+
 /* ---- split-precision tensor-core form (sm_100a tcgen05, kind::i8) --------- */
 /*
  * The batched form of the same RK4 step: per group of wires sharing one k

@@ -31,7 +31,7 @@ reference's own way one right-hand side at a time.
 import numpy as np
 from scipy.constants import hbar as HBAR
 
-from . import _lib, abi, device
+from . import _lib, abi, device, wirespace
 
 ii = 1j
 hbar = HBAR
@@ -336,6 +336,7 @@ class SBESolver:
         self.start = False
         self._backend = backend
         self.batch = None
+        self.full = None
         if not QW:
             return
         self._read_qw_params()
@@ -441,6 +442,9 @@ class SBESolver:
     def levels(self, w):
         """Diagonals (p, ne, nh) of the three stored levels of wire w (1-based),
         numpy, as (YY1, YY2, YY3), (CC1, CC2, CC3), (DD1, DD2, DD3)."""
+        if self.full is not None:
+            m = [lv[w - 1].cpu().numpy() for lv in self.full["L"]]  # (3, Nk, Nk) each
+            return tuple([np.diagonal(a[j]).copy() for a in m] for j in range(3))
         s = self.batch.wire_slice(w - 1)
         out = []
         for lv in (self.y0, self.batch.y1, self.batch.y):
@@ -450,6 +454,106 @@ class SBESolver:
                 [a[:, 3] + 0j for a in out])
 
     # -- the step ---------------------------------------------------------------
+    def _is_diagonal(self, Ex, Ey, Ez):
+        if not self.Optics:
+            return True
+        lo, hi = self.NQ0 - (self.Nk - 1), self.NQ0 + self.Nk
+        win = slice(max(lo, 0), hi)
+        ey = np.array(Ey[win], dtype=np.complex128, copy=True)
+        ey[self.NQ0 - win.start] = 0.0
+        return not (np.any(np.asarray(Ex)[win] != 0) or np.any(np.asarray(Ez)[win] != 0)
+                    or np.any(ey != 0))
+
+    def _enter_full(self):
+        """Move the state to full Nk x Nk matrices (the diagonal levels
+        embedded) and set up the full-matrix step's device buffers."""
+        import torch
+
+        from . import device as _dev
+
+        nk, nw = self.Nk, self.Nw
+        levels = []
+        for lv in (self.y0, self.batch.y1, self.batch.y):
+            a = lv.view(nw, nk, 4)
+            m = torch.zeros((nw, 3, nk, nk), dtype=torch.complex128, device="cuda")
+            idx = torch.arange(nk, device="cuda")
+            m[:, 0, idx, idx] = torch.complex(a[:, :, 0], a[:, :, 1])
+            m[:, 1, idx, idx] = torch.complex(a[:, :, 2], torch.zeros_like(a[:, :, 2]))
+            m[:, 2, idx, idx] = torch.complex(a[:, :, 3], torch.zeros_like(a[:, :, 3]))
+            levels.append(m)
+        blk = self.batch.tabdata.view(abi.TAB_BLOCKS, nk)
+        w1 = np.zeros(1, dtype=abi.WIRE_DTYPE)  # one-wire descriptor for the screening
+        w1["table"] = 0
+        self.full = {
+            "L": levels,
+            "work": torch.empty(int(_lib.load().psb_full_work_bytes(nk)), dtype=torch.uint8,
+                                device="cuda"),
+            "V0": blk[0:3].contiguous(),
+            "Ee": blk[abi.TAB_EE].contiguous(),
+            "Eh": blk[abi.TAB_EH].contiguous(),
+            "kr": torch.as_tensor(self.kr, device="cuda"),
+            "r": torch.as_tensor(self.r, device="cuda"),
+            "window": torch.as_tensor(self.window, device="cuda"),
+            "wire1": _dev.to_device(w1),
+            "y1": torch.zeros((nk, 4), dtype=torch.float64, device="cuda"),
+            "eps": torch.zeros((1, nk), dtype=torch.float64, device="cuda"),
+            "out": torch.zeros((5, self.Nr), dtype=torch.complex128, device="cuda"),
+        }
+
+    def _full_step(self, Ex, Ey, Ez, dt, Px, Py, Pz, Re, Rh, w):
+        import torch
+
+        from . import device as _dev
+
+        F = self.full
+        nk, i = self.Nk, w - 1
+        for a in (Px, Py, Pz, Re, Rh):
+            a[:] = 0.0
+        L1, L2, L3 = (lv[i] for lv in F["L"])
+        # Coulomb table of this step: V0, or V0 / eps(q; n1D) from the current
+        # occupations (CalcScreenedArrays, coulomb.py:1195-1230)
+        V3 = F["V0"]
+        if self.Screened:
+            idx = torch.arange(nk, device="cuda")
+            F["y1"][:, 2] = L3[1, idx, idx].real
+            F["y1"][:, 3] = L3[2, idx, idx].real
+            _lib.call("psb_screen_f64", _dev.ptr(self.batch.d_tables), 1,
+                      _dev.ptr(self.batch.tabdata), _dev.ptr(F["wire1"]), 1, _dev.ptr(F["y1"]),
+                      _dev.ptr(F["eps"]), nk, _dev.stream_ptr())
+            V3 = (F["V0"] / F["eps"]).contiguous()
+        fields = torch.as_tensor(np.stack([np.asarray(Ex, np.complex128),
+                                           np.asarray(Ey, np.complex128),
+                                           np.asarray(Ez, np.complex128)]), device="cuda")
+        if not self.Optics:
+            fields.zero_()
+        prm = np.zeros(1, dtype=abi.FULL_PARAMS_DTYPE)
+        prm["ehint"], prm["dcv"], prm["yw"], prm["sgnw"] = self.ehint, self.dcv, yw(w), (-1) ** w
+        prm["gap"], prm["gam_e"], prm["gam_h"] = self.gap, self.gam_e, self.gam_h
+        prm["hbar"], prm["dt"] = HBAR, dt
+        prm["excitons"], prm["lf"] = int(self.Excitons), int(self.LF)
+        _lib.call("psb_full_step_f64", nk, self.Nr, self.NQ0, _dev.ptr(V3), _dev.ptr(F["Ee"]),
+                  _dev.ptr(F["Eh"]), _dev.ptr(fields), abi.as_ptr(prm), _dev.ptr(L1),
+                  _dev.ptr(L2), _dev.ptr(L3), _dev.ptr(F["work"]), F["work"].numel(),
+                  _dev.stream_ptr())
+        if not (self.Optics or self.LF):
+            return
+        _lib.call("psb_full_sources_f64", nk, self.Nr, _dev.ptr(F["kr"]), _dev.ptr(F["r"]),
+                  _dev.ptr(F["window"]), float(self.L), float(self.dcv), float(yw(w)),
+                  float((-1) ** w), _dev.ptr(L3), _dev.ptr(F["out"]), _dev.stream_ptr())
+        out = F["out"].cpu().numpy()
+        if self.Optics:
+            for a, src in zip((Px, Py, Pz), out[:3]):
+                a[:] = src * 2 * self.ehint / self.area / self.L
+                wirespace.fftg(a)
+        if self.LF:
+            c3 = L3[1].diagonal().cpu().numpy()
+            d3 = L3[2].diagonal().cpu().numpy()
+            Re[:] = out[3]
+            Rh[:] = out[4]
+            wirespace.rho_post(Re, Rh, c3, d3, self.r[1] - self.r[0])
+            Re[:] = 2.0 * _e0 * Re / self.area * self.ehint
+            Rh[:] = 2.0 * _e0 * Rh / self.area * self.ehint
+
     def _drive(self, Ex, Ey, Ez):
         """E = Ey[NQ0] after checking that no other q component reaches Meh."""
         if not self.Optics:
@@ -469,7 +573,16 @@ class SBESolver:
         """One leapfrog step of wire w (1-based) driven by the wire-space fields
         (SBEs.py:5624-5836), with its source terms written in place: Px, Py,
         Pz = QWPolarization3 of the new p (qwoptics.py:815-946) and, with LF,
-        Re, Rh = QWRho5 of the new C, D (qwoptics.py:948-1078), all in q space."""
+        Re, Rh = QWRho5 of the new C, D (qwoptics.py:948-1078), all in q space.
+
+        While the state is diagonal and the field reaches the wire only at
+        q = 0 (``Ey[NQ0]``), the step runs in the diagonal kernel; any other
+        field (or a non-diagonal state read from backup files) switches the
+        solver, for good, to the full Nk x Nk state (psb_full_step_f64)."""
+        if self.full is None and not self._is_diagonal(Ex, Ey, Ez):
+            self._enter_full()
+        if self.full is not None:
+            return self._full_step(Ex, Ey, Ez, dt, Px, Py, Pz, Re, Rh, w)
         E = self._drive(Ex, Ey, Ez)
         for a in (Px, Py, Pz, Re, Rh):
             a[:] = 0.0
@@ -523,13 +636,15 @@ class SBESolver:
 
     def QWCalculator(self, Exx, Eyy, Ezz, Vrr, rr, q, dt, w, Pxx, Pyy, Pzz, Rho, DoQWP,
                      DoQWDl):
-        """Per-time-step entry (SBEs.py:5838-6001): bookkeeping of the step
-        counters and the wire-off gate as in the reference, then the step.
-        While the field stays below 1e-3 of Emaxxx the wire is off and the
-        outputs are zero, as in the reference.  A field that switches the
-        wire on reaches the wire through Prop2QW, whose window along the wire
-        gives it every q component: that needs the full-matrix right-hand
-        side, so NotImplementedError is raised."""
+        """Per-time-step entry (SBEs.py:5838-6001): the step counters and the
+        wire-off gate of the reference (while the field stays below 1e-3 of
+        Emaxxx the wire is off and the outputs are zero), then the fields
+        brought onto the wire (Prop2QW: spline resampling, window, real part,
+        transform), one step of wire w, and its sources brought back onto
+        the propagation grid (QW2Prop) in place: Pxx, Pyy, Pzz and
+        Rho = RhoH - RhoE.  The window makes a field along the wire reach
+        every q, so the step runs on the full Nk x Nk state.  The
+        diagnostic files of the reference are not written."""
         for a in (Pxx, Pyy, Pzz, Rho):
             a[:] = 0.0
         if w == 1:
@@ -541,10 +656,20 @@ class SBESolver:
         mag = np.max(np.sqrt(np.abs(Exx) ** 2 + np.abs(Eyy) ** 2 + np.abs(Ezz) ** 2))
         if self.wireoff and mag < 1e-3 * self.Emax0:
             return
-        raise NotImplementedError(
-            "QWCalculator: a propagation-space field drives the wire through Prop2QW "
-            "(qwoptics.py:673-721), whose window makes the state non-diagonal; use "
-            "_sbe_calculator with a q = 0 field, or WireBatch")
+        self.wireoff = False
+        DoQWP[0] = self.Optics
+        DoQWDl[0] = self.LF
+        Ex, Ey, Ez, Vr = wirespace.prop2qw(rr, Exx, Eyy, Ezz, Vrr, self.r, self.window)
+        src = [np.zeros(self.Nr, np.complex128) for _ in range(5)]
+        self._sbe_calculator(Ex, Ey, Ez, Vr, dt, *src, False, w)
+        Px_, Py_, Pz_, RhoE, RhoH = wirespace.qw2prop(self.r, *src, np.asarray(rr), self.LF)
+        Pxx[:] = Px_
+        Pyy[:] = Py_
+        Pzz[:] = Pz_
+        Rho[:] = RhoH - RhoE
+        if self.ignorewire:
+            for a in (Pxx, Pyy, Pzz, Rho):
+                a[:] = 0.0
 
     # -- small accessors (SBEs.py:5516-5534) ---------------------------------------
     def chiqw(self):
@@ -563,8 +688,14 @@ class SBESolver:
     _KEYS = ("CC1", "CC2", "CC3", "DD1", "DD2", "DD3", "YY1", "YY2", "YY3")
 
     def _level_arrays(self):
-        """{key: (Nw, Nk) complex diagonals} of the nine stored arrays."""
+        """{key: (Nw, Nk) complex diagonals} of the nine stored arrays, or
+        (Nw, Nk, Nk) matrices [w, k1, k2] once the state is full."""
         out = {}
+        if self.full is not None:
+            for n, lv in enumerate(self.full["L"], start=1):
+                a = lv.cpu().numpy()
+                out[f"YY{n}"], out[f"CC{n}"], out[f"DD{n}"] = a[:, 0], a[:, 1], a[:, 2]
+            return out
         levels = [lv.view(self.Nw, self.Nk, 4).cpu().numpy()
                   for lv in (self.y0, self.batch.y1, self.batch.y)]
         for n, a in enumerate(levels, start=1):
@@ -587,31 +718,39 @@ class SBESolver:
             for w in range(self.Nw):
                 for k2 in range(self.Nk):
                     for k1 in range(self.Nk):
-                        val = complex(a[w, k1]) if k1 == k2 else 0j
+                        if a.ndim == 3:
+                            val = complex(a[w, k1, k2])
+                        else:
+                            val = complex(a[w, k1]) if k1 == k2 else 0j
                         lines.append(f"{np.real(val)} {np.imag(val)}\n")
             with open(os.path.join(directory, f"{key}.{n}.dat"), "w", encoding="utf-8") as f:
                 f.write("".join(lines))
 
     def read_sbes_data(self, Nt, directory="dataQW/backup/"):
         """Read backup files written by the reference (or write_sbes_data);
-        the arrays must be diagonal in k."""
+        off-diagonal coherences switch the solver to the full Nk x Nk state."""
         import os
 
         import torch
 
-        vals = {}
+        vals, mats, offdiag = {}, {}, False
         for key in self._KEYS:
             with open(os.path.join(directory, f"{key}.{Nt}.dat"), "r", encoding="utf-8") as f:
                 raw = np.array([float(x) for x in f.read().split()], dtype=np.float64)
             m = (raw[0::2] + 1j * raw[1::2]).reshape(self.Nw, self.Nk, self.Nk)  # [w, k2, k1]
-            d = np.einsum("wkk->wk", m)
+            mats[key] = np.ascontiguousarray(np.transpose(m, (0, 2, 1)))  # [w, k1, k2]
+            vals[key] = np.einsum("wkk->wk", m)
             off = m.copy()
             idx = np.arange(self.Nk)
             off[:, idx, idx] = 0.0
-            if np.any(off != 0):
-                raise NotImplementedError(f"{key}: off-diagonal coherences need the full-matrix "
-                                          "SBE state (not provided by pulsesuite_b200)")
-            vals[key] = d
+            offdiag |= bool(np.any(off != 0))
+        if offdiag or self.full is not None:
+            if self.full is None:
+                self._enter_full()
+            for n, lv in enumerate(self.full["L"], start=1):
+                m = np.stack([mats[f"YY{n}"], mats[f"CC{n}"], mats[f"DD{n}"]], 1)
+                lv.copy_(torch.as_tensor(m))
+            return
         for n, lv in enumerate((self.y0, self.batch.y1, self.batch.y), start=1):
             y = np.stack([vals[f"YY{n}"].real, vals[f"YY{n}"].imag, vals[f"CC{n}"].real,
                           vals[f"DD{n}"].real], -1).reshape(-1, 4)

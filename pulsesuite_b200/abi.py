@@ -57,6 +57,13 @@ WIRE_DTYPE = np.dtype(
 
 MODEL_DTYPE = np.dtype([("hbar", "<f8"), ("flags", "<i4"), ("reserved", "<i4")], align=True)
 
+FULL_PARAMS_DTYPE = np.dtype(
+    [("ehint", "<f8"), ("dcv", "<f8"), ("yw", "<f8"), ("sgnw", "<f8"), ("gap", "<f8"),
+     ("gam_e", "<f8"), ("gam_h", "<f8"), ("hbar", "<f8"), ("dt", "<f8"), ("excitons", "<i4"),
+     ("lf", "<i4")],
+    align=True,
+)
+
 PSB_SPLIT_WMAX = 16
 PSB_SPLIT_NOALLOC_SCRATCH_BYTES = 8 * 1024 * 1024
 PSB_SPLIT_NOALLOC_MAX_STATE = (PSB_SPLIT_NOALLOC_SCRATCH_BYTES - 32) // 64
@@ -66,6 +73,7 @@ SPLIT_GROUP_DTYPE = np.dtype(
 assert TABLE_DTYPE.itemsize == 32
 assert WIRE_DTYPE.itemsize == 136
 assert MODEL_DTYPE.itemsize == 16
+assert FULL_PARAMS_DTYPE.itemsize == 80
 assert SPLIT_GROUP_DTYPE.itemsize == 72
 
 

@@ -26,6 +26,7 @@ Cases (all stored as .npz next to this script):
                   (rotating-frame drive, the benchmark configurations' physics)
   leapfrog_*.npz  SBESolver._sbe_calculator, the reference's own driver
   solver_*.npz    the SBESolver API with LF on: source terms, levels, backup files
+  qwcalc_*.npz    QWCalculator driven by propagation-space fields (full-matrix state)
 """
 
 import argparse
@@ -429,6 +430,82 @@ def make_solver_api(R, out, name="solver_lf_nk32", L=2.85e-8, nsteps=300, dt=10e
         os.chdir(cwd)
 
 
+MB_PARAMS_FULL = "1\n1\n0\n{scr}\n0\n0\n1\n0\n0\n0\n0\n0\n0\n0\n0\n"
+
+
+def make_qwcalculator(R, out, name, L=2.85e-8, screened=True, nsteps=200, dt=10e-18):
+    """The reference's QWCalculator as its PSTD caller drives it (rhoPJ.py:311-348):
+    propagation-space fields along the wire axis (a Gaussian profile, so the
+    windowed wire field has every q component and the state is full-matrix),
+    LF on.  Stored: the fields, every step's Pxx/Pyy/Pzz/Rho, and the final
+    full Nk x Nk levels."""
+    cwd = os.getcwd()
+    run = tempfile.mkdtemp(prefix="qwc_", dir=_TMP)
+    os.makedirs(os.path.join(run, "params"))
+    gam = 5e12
+    with open(os.path.join(run, "params", "qw.params"), "w") as f:
+        f.write(QW_PARAMS.format(L=L, gam=gam))
+    with open(os.path.join(run, "params", "mb.params"), "w") as f:
+        f.write(MB_PARAMS_FULL.format(scr=1 if screened else 0))
+    os.chdir(run)
+    try:
+        nrr = 64
+        rr = np.linspace(-5e-8, 5e-8, nrr)
+        qrr = R.SBEs.GetKArray(nrr, nrr * (rr[1] - rr[0]))
+        s = R.SBEs.SBESolver(qrr, rr, 0.0, 1e7, 800e-9, 2, True)
+        nk = s.Nk
+        E0, tw, tp = 2e8, 1.0e-15, 1.0e-15
+        wl = (s.gap + 0.05 * 1.602176634e-19) / R.SBEs.hbar
+        prof = np.exp(-((rr / 3e-8) ** 2))
+        outs = {k: np.zeros((nsteps, 2, nrr), complex) for k in ("Pxx", "Pyy", "Pzz", "Rho")}
+        env = np.zeros(nsteps)
+        t_start = time.time()
+        for n in range(nsteps):
+            t = n * dt
+            E = E0 * np.exp(-(((t - tp) / tw) ** 2)) * np.cos(wl * (t - tp))
+            env[n] = E
+            for w in (1, 2):
+                Exx = (0.3 * E * prof * (rr / 3e-8)).astype(complex)
+                Eyy = (E * prof).astype(complex)
+                Ezz = (0.2 * E * prof).astype(complex)
+                Vrr = np.zeros(nrr, complex)
+                o = [np.zeros(nrr, complex) for _ in range(4)]
+                DoQWP, DoQWDl = [False], [False]
+                s.QWCalculator(Exx, Eyy, Ezz, Vrr, rr, qrr, dt, w, *o, DoQWP, DoQWDl)
+                for k, v in zip(("Pxx", "Pyy", "Pzz", "Rho"), o):
+                    outs[k][n, w - 1] = v
+        el = time.time() - t_start
+        lv = {f"{a}{i}": getattr(s, f"{a}{i}").copy() for a in ("YY", "CC", "DD") for i in (1, 2, 3)}
+        np.savez_compressed(os.path.join(out, f"{name}.npz"), nk=nk, nr=s.Nr, L=L, gam=gam,
+                            dt=dt, nsteps=nsteps, rr=rr, prof=prof, env=env,
+                            screened=screened, seconds=el, **outs, **lv)
+        print(f"{name}: Nk={nk}, {nsteps} steps x 2 wires in {el:.1f} s, "
+              f"max|Pyy| = {np.max(np.abs(outs['Pyy'])):.3e}, "
+              f"offdiag |p| = {np.max(np.abs(lv['YY3'] - np.einsum('iiw->iw', lv['YY3'])[None]*0)):.3e}")
+    finally:
+        os.chdir(cwd)
+
+
+def make_glue(R, out):
+    """The reference's spline resampling and centred transforms on random
+    data (the wire/propagation grid plumbing of QWCalculator)."""
+    from pulsesuite.libpulsesuite import spliner
+
+    rng = np.random.default_rng(17)
+    x0 = np.linspace(-5e-8, 5e-8, 64)
+    z0 = rng.standard_normal(64) + 1j * rng.standard_normal(64)
+    x1 = np.linspace(-6e-8, 6e-8, 70)  # reaches beyond x0 on both sides
+    z1 = np.zeros(70, complex)
+    spliner.rescale_1D(x0, z0, x1, z1)
+    F = z0.copy()
+    R.usefulsubs.FFTG(F)
+    G = z0.copy()
+    R.usefulsubs.iFFTG(G)
+    np.savez_compressed(os.path.join(out, "glue.npz"), x0=x0, z0=z0, x1=x1, z1=z1, fftg=F,
+                        ifftg=G)
+    print("glue: done")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--full-c0", action="store_true")
@@ -456,6 +533,11 @@ def main():
         make_leapfrog(R, out, "leapfrog_screened_nk32", screened=True, nsteps=2000)
     if want("solver"):
         make_solver_api(R, out)
+    if want("glue"):
+        make_glue(R, out)
+    if want("qwcalc"):
+        make_qwcalculator(R, out, "qwcalc_screened_nk32", screened=True)
+        make_qwcalculator(R, out, "qwcalc_nk32", screened=False, nsteps=120)
     if a.full_c0:
         make_rk4(R, out, "rk4_c0_nk128_full", rwa_case(128, 4000))
 

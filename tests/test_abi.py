@@ -52,6 +52,8 @@ int main(void) {
          offsetof(PsbWire, amp), offsetof(PsbWire, p_off), offsetof(PsbWire, status),
          offsetof(PsbWire, steps));
   printf("%zu %zu\n", offsetof(PsbTable, L), offsetof(PsbTable, dens_max));
+  printf("%zu %zu %zu\n", sizeof(PsbFullParams), offsetof(PsbFullParams, dt),
+         offsetof(PsbFullParams, lf));
   return 0;
 }
 '''
@@ -67,4 +69,6 @@ int main(void) {
     W = abi.WIRE_DTYPE
     assert vals[:3] == [abi.TABLE_DTYPE.itemsize, W.itemsize, abi.MODEL_DTYPE.itemsize]
     assert vals[3:9] == [W.fields[f][1] for f in ("gap", "t", "amp", "p_off", "status", "steps")]
-    assert vals[9:] == [abi.TABLE_DTYPE.fields["L"][1], abi.TABLE_DTYPE.fields["dens_max"][1]]
+    assert vals[9:11] == [abi.TABLE_DTYPE.fields["L"][1], abi.TABLE_DTYPE.fields["dens_max"][1]]
+    F = abi.FULL_PARAMS_DTYPE
+    assert vals[11:] == [F.itemsize, F.fields["dt"][1], F.fields["lf"][1]]

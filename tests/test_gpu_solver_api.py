@@ -7,7 +7,9 @@ importing the reference):
     _sbe_calculator with a field at q = 0 of the wire, reproduces the
     reference's levels, P(t) and source terms (Px, Py, Pz; Re, Rh with LF)
     to 1e-10 normwise, and reads / writes the reference's backup files;
-  * QWCalculator keeps the reference's wire-off gate and counters;
+  * QWCalculator keeps the reference's wire-off gate and counters, and
+    with fields along the wire (full Nk x Nk state, psb_full_step_f64)
+    reproduces the reference's Pxx, Pyy, Pzz, Rho and levels;
   * InitializeCoulomb / CalcScreenedArrays / Eps1D / Vint / CalcChi1D /
     K03 reproduce the reference's Coulomb arrays to 1e-12.
 """
@@ -133,24 +135,41 @@ def test_solver_module_shims_and_qwcalculator_gate(cuda, tmp_path):
     SBEs.QWCalculator(weak, weak, weak, weak * 0, rr, None, 1e-17, 1, *out, DoQWP, DoQWDl)
     assert all(np.all(o == 0) for o in out)
     assert DoQWP == [None] and s.xxx == 2 and s.t == pytest.approx(1e-17)
-    strong = np.full(64, 1e5, complex)
-    with pytest.raises(NotImplementedError):
-        SBEs.QWCalculator(strong, strong, strong, weak * 0, rr, None, 1e-17, 1, *out, DoQWP,
-                          DoQWDl)
+    assert s.full is None and s.wireoff
+    strong = np.full(64, 1e5, complex)  # switches the wire on
+    SBEs.QWCalculator(strong, strong, strong, weak * 0, rr, None, 1e-17, 1, *out, DoQWP,
+                      DoQWDl)
+    assert DoQWP == [True] and DoQWDl == [False] and not s.wireoff
+    assert s.full is not None  # a field along the wire: full-matrix state
     assert SBEs.QWArea() == s.area and SBEs.getqc() == s.qc
     SBEs.ShutOffOptics()
     assert s.Optics is False
 
 
-def test_solver_rejects_offdiagonal_field(cuda, tmp_path):
+def test_solver_full_step_agrees_with_diagonal_step(cuda, tmp_path):
+    """A q = 0 field keeps the state diagonal: stepping it on the full
+    Nk x Nk state gives the diagonal kernel's numbers (1e-12), and the
+    off-diagonal elements stay exactly zero."""
     d = golden("leapfrog_nk32")
-    s = make_solver(tmp_path, float(d["L"]), float(d["gam"]))
-    nr = s.Nr
-    Ex, Ey, Ez, Vr = (np.zeros(nr, complex) for _ in range(4))
-    Ey[s.NQ0 + 1] = 1e6
-    srcs = [np.zeros(nr, complex) for _ in range(5)]
-    with pytest.raises(NotImplementedError):
-        s._sbe_calculator(Ex, Ey, Ez, Vr, 1e-17, *srcs, False, 1)
+    a = make_solver(tmp_path, float(d["L"]), float(d["gam"]), lf=True)
+    b = make_solver(tmp_path, float(d["L"]), float(d["gam"]), lf=True)
+    b._enter_full()
+    nr = a.Nr
+    for i in range(200):
+        outs = []
+        for s in (a, b):
+            Ex, Ey, Ez, Vr = (np.zeros(nr, complex) for _ in range(4))
+            Ey[s.NQ0] = d["field"][i]
+            src = [np.zeros(nr, complex) for _ in range(5)]
+            s._sbe_calculator(Ex, Ey, Ez, Vr, float(d["dt"]), *src, False, 1)
+            outs.append(src)
+    assert a.full is None
+    assert relerr(diag_levels(b), diag_levels(a)) < 1e-12
+    for x, y in zip(outs[1][1:], outs[0][1:]):  # Py, Pz, Re, Rh
+        assert relerr(x, y) < 1e-12
+    m = b.full["L"][2][0].cpu().numpy()
+    for j in range(3):
+        assert np.count_nonzero(m[j] - np.diag(np.diagonal(m[j]))) == 0
 
 
 # ---------------------------------------------------------------------------
@@ -195,3 +214,43 @@ def test_coulomb_k03_matches_reference(cuda):
     d = golden("k0_ref")
     for x, ref in zip(d["x"][::17], d["K03"][::17]):
         assert coulomb.K03(x) == pytest.approx(float(ref), rel=1e-12)
+
+
+@pytest.mark.parametrize("name,screened", [("qwcalc_screened_nk32", True),
+                                           ("qwcalc_nk32", False)])
+def test_qwcalculator_full_matrix_matches_reference(cuda, tmp_path, name, screened):
+    """QWCalculator as the PSTD caller drives it (rhoPJ.py:311-348): fields
+    along the wire with a spatial profile, two wires, LF on.  The window of
+    Prop2QW gives the wire field every q component, so the state is full
+    Nk x Nk; every step's Pxx, Pyy, Pzz, Rho and the final nine levels
+    match the reference (1e-10 normwise)."""
+    d = golden(name)
+    s = make_solver(tmp_path, float(d["L"]), float(d["gam"]), screened=screened, lf=True, nw=2)
+    rr, prof = d["rr"], d["prof"]
+    n, nrr = int(d["nsteps"]), rr.size
+    got = {k: np.zeros((n, 2, nrr), complex) for k in ("Pxx", "Pyy", "Pzz", "Rho")}
+    for i in range(n):
+        E = d["env"][i]
+        for w in (1, 2):
+            o = [np.zeros(nrr, complex) for _ in range(4)]
+            s.QWCalculator((0.3 * E * prof * (rr / 3e-8)).astype(complex),
+                           (E * prof).astype(complex), (0.2 * E * prof).astype(complex),
+                           np.zeros(nrr, complex), rr, None, float(d["dt"]), w, *o,
+                           [False], [False])
+            for k, v in zip(("Pxx", "Pyy", "Pzz", "Rho"), o):
+                got[k][i, w - 1] = v
+    assert s.full is not None
+    for k in ("Pyy", "Pzz", "Rho"):
+        assert relerr(got[k], d[k]) < TOL, k
+    assert np.max(np.abs(got["Pxx"] - d["Pxx"])) < TOL * np.max(np.abs(d["Pyy"]))
+    lv = s._level_arrays()
+    for key in ("YY1", "YY2", "YY3", "CC1", "CC2", "CC3", "DD1", "DD2", "DD3"):
+        ref = np.transpose(d[key], (2, 0, 1))  # [w, k1, k2]
+        assert relerr(lv[key], ref) < TOL, key
+    # the full state round-trips through the reference's backup format
+    s.write_sbes_data(3, directory=str(tmp_path / "bk") + "/")
+    s2 = make_solver(tmp_path, float(d["L"]), float(d["gam"]), screened=screened, lf=True, nw=2)
+    s2.read_sbes_data(3, directory=str(tmp_path / "bk") + "/")
+    lv2 = s2._level_arrays()
+    for key in lv:
+        assert relerr(lv2[key], lv[key]) < 1e-15, key
