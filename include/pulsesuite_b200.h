@@ -403,6 +403,39 @@ int psb_rk4_split_noalloc(const PsbTable* d_tables, int ntab, const double* d_ta
                           int64_t n_P, int p_stride, int p_cap, const PsbModel* model,
                           void* stream);
 
+/*
+ * The split form with one Coulomb matrix per wire, for the tables
+ * psb_rk4_split does not take:
+ *  - screened tables (PSB_TAB_SCREENED): every stage divides V(q) by
+ *    eps(q; n1D) of that wire's own stage densities, as psb_rk4_f64 does
+ *    (CalcScreenedArrays, coulomb.py:1212-1230, Eps1D coulomb.py:1172-1193;
+ *    eps in FP64);
+ *  - distinct Veh, Vee, Vhh (tables without PSB_TAB_SHARED_V; the
+ *    reference's CalcCoulombArrays physics, coulomb.py:502-577): p uses Veh,
+ *    ne Vee, nh Vhh.
+ * Same digit arithmetic, accuracy target, state layout, workspace
+ * (psb_split_ws_bytes) and per-wire results as psb_rk4_split; the CTA of a
+ * group contracts its wires one after another, so the tensor-core work per
+ * wire does not shrink with the group size.  wgroup: wires per group, 1 ..
+ * psb_split_wire_max_group(nkmax, tab_flags) (<= PSB_SPLIT_WMAX); nkmax <=
+ * 1024 (512 for distinct matrices).  tab_flags: the PSB_TAB_* flags every
+ * group's table has (PSB_TAB_EXCITONS required; PSB_TAB_SCREENED and
+ * PSB_TAB_SHARED_V as the tables have them).  Replaces, like psb_rk4_f64,
+ * CalcH + dpdt/dCdt/dDdt (SBEs.py:669-935, 1850-2636) integrated by rk4_dpc
+ * (libpulsesuite/integrator.py:143-167).
+ */
+int psb_rk4_split_wire(const PsbTable* d_tables, int ntab, const double* d_tabdata,
+                       int64_t n_tabdata, PsbWire* d_wires, int nw, const PsbSplitGroup* d_groups,
+                       int ngroups, int wgroup, int nkmax, int tab_flags, double* d_y,
+                       int64_t n_state, void* d_ws, int64_t n_ws_bytes, int nsteps, double dt,
+                       double* d_P, int64_t n_P, int p_stride, int p_cap, const PsbModel* model,
+                       void* stream);
+/* Largest group (wires per CTA) psb_rk4_split_wire supports for a grid of nk
+ * with these table flags; 0 when the grid does not fit. */
+int psb_split_wire_max_group(int nk, int tab_flags);
+/* Dynamic shared memory (bytes) of one psb_rk4_split_wire CTA. */
+int psb_split_wire_smem_bytes(int nk, int wgroup, int tab_flags);
+
 /* ---- measurement --------------------------------------------------------- */
 /*
  * FP64 FMA throughput of the current device: runs an in-register FMA loop

@@ -45,6 +45,10 @@ _SIGNATURES = {
                        f64, vp, i64, i32, i32, vp, vp], i32),
     "psb_rk4_split_noalloc": ([vp, i32, vp, i64, vp, i32, vp, i32, i32, i32, vp, i64, i32, f64,
                                vp, i64, i32, i32, vp, vp], i32),
+    "psb_rk4_split_wire": ([vp, i32, vp, i64, vp, i32, vp, i32, i32, i32, i32, vp, i64, vp, i64,
+                            i32, f64, vp, i64, i32, i32, vp, vp], i32),
+    "psb_split_wire_max_group": ([i32, i32], i32),
+    "psb_split_wire_smem_bytes": ([i32, i32, i32], i32),
 }
 
 

@@ -21,8 +21,9 @@ from . import _lib, abi, coulomb, device
 class WireBatch:
     """``form`` selects the step kernel: "plain" (FP64 throughout,
     psb_rk4_f64) or "split" (exchange sums on the int8 tensor cores as exact
-    products of base-254 digits, FP64 right-hand side and state,
-    psb_rk4_split)."""
+    products of base-254 digits, FP64 right-hand side and state:
+    psb_rk4_split for unscreened grids with one shared Coulomb matrix,
+    psb_rk4_split_wire for screened grids or distinct Veh, Vee, Vhh)."""
 
     def __init__(self, grids, wires, screened=False, excitons=True, p_cap=0, tables=None,
                  tabdata=None, form="plain", split_w=None, tune=True):
@@ -89,19 +90,27 @@ class WireBatch:
     def _setup_split(self):
         """Wire groups (one CTA each) and the workspace of the split form.
 
-        A group holds up to W in {4, 8, 16} wires of one grid.  W is chosen
-        per grid by the autotuner (tune.SplitTuner: measured per-CTA cost of
-        each W on this device, times the waves of CTAs the grid's wire count
-        needs); with ``tune=False`` by a rule (W = 8 once a grid has enough
-        wires for roughly two waves of CTAs, else 4); ``split_w`` overrides
-        both per grid.  Groups are launched in classes of (W, state
-        resident in shared memory or not) so that a large grid does not push
-        the small ones out of the resident layout; the classes run
-        concurrently on side streams, the one with the largest grid first."""
-        need = abi.PSB_TAB_EXCITONS | abi.PSB_TAB_SHARED_V
+        Unscreened grids with Veh == Vee == Vhh use psb_rk4_split: a group
+        holds up to W in {4, 8, 16} wires of one grid sharing one Coulomb
+        matrix.  W is chosen per grid by the autotuner (tune.SplitTuner:
+        measured per-CTA cost of each W on this device, times the waves of
+        CTAs the grid's wire count needs); with ``tune=False`` by a rule
+        (W = 8 once a grid has enough wires for roughly two waves of CTAs,
+        else 4); ``split_w`` overrides both per grid.  Groups are launched in
+        classes of (W, state resident in shared memory or not) so that a
+        large grid does not push the small ones out of the resident layout.
+
+        Screened grids and grids with distinct Veh, Vee, Vhh use
+        psb_rk4_split_wire (one matrix per wire, the wires of a group
+        contracted one after another): W is the largest group that fits, but
+        no more wires per CTA than a full wave of CTAs leaves
+        (``split_w`` overrides it, 1 .. psb_split_wire_max_group).
+
+        All classes run concurrently on side streams, the one with the
+        largest grid first."""
         f = self.h_tables["flags"]
-        if ((f & need) != need).any() or (f & abi.PSB_TAB_SCREENED).any():
-            raise _lib.PsbError("split form needs unscreened tables with Veh == Vee == Vhh")
+        if ((f & abi.PSB_TAB_EXCITONS) == 0).any():
+            raise _lib.PsbError("split form needs tables with excitons (the exchange sums)")
         lib = _lib.load()
         maxnk = {wg: int(lib.psb_split_max_nk(wg)) for wg in (4, 8, 16)}
         resnk = {wg: int(lib.psb_split_max_nk_resident(wg)) for wg in (4, 8, 16)}
@@ -110,32 +119,50 @@ class WireBatch:
         sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
         target = float(np.sum(counts * nks.astype(np.float64) ** 2)) / (2.0 * sms)
         classes = {}
+        wclasses = {}
         for t in np.argsort(-nks, kind="stable"):
             nk = int(nks[t])
             if counts[t] == 0:
                 continue
-            wg = 4
-            if self.tune:
-                from .tune import shared_tuner
-
-                wg = shared_tuner().best_width(nk, int(counts[t]))
-            elif nk <= maxnk[8] and 8 * nk * nk <= max(target, 4 * nk * nk):
-                wg = 8
-            if nk in self.split_w:
-                wg = int(self.split_w[nk])
-                if wg not in (4, 8, 16):
-                    raise ValueError("split_w values must be 4, 8 or 16")
-            if nk > maxnk[wg]:
-                raise _lib.PsbError(f"split form: nk {nk} exceeds the supported maximum")
-            key = (wg, nk <= resnk[wg])
             ws = np.nonzero(self.h_wires["table"] == t)[0]
+            tflags = int(f[t]) & (abi.PSB_TAB_EXCITONS | abi.PSB_TAB_SCREENED |
+                                  abi.PSB_TAB_SHARED_V)
+            per_wire = (tflags & abi.PSB_TAB_SCREENED) or not (tflags & abi.PSB_TAB_SHARED_V)
+            if per_wire:
+                wmax = int(lib.psb_split_wire_max_group(nk, tflags))
+                if wmax < 1:
+                    raise _lib.PsbError(f"split form: nk {nk} exceeds the supported maximum "
+                                        "for screened or distinct Coulomb matrices")
+                wg = max(1, min(wmax, -(-len(ws) // sms)))
+                if nk in self.split_w:
+                    wg = int(self.split_w[nk])
+                    if not 1 <= wg <= wmax:
+                        raise ValueError(f"split_w[{nk}] must be 1..{wmax} for these tables")
+                key = (wg, tflags)
+                target_classes = wclasses
+            else:
+                wg = 4
+                if self.tune:
+                    from .tune import shared_tuner
+
+                    wg = shared_tuner().best_width(nk, int(counts[t]))
+                elif nk <= maxnk[8] and 8 * nk * nk <= max(target, 4 * nk * nk):
+                    wg = 8
+                if nk in self.split_w:
+                    wg = int(self.split_w[nk])
+                    if wg not in (4, 8, 16):
+                        raise ValueError("split_w values must be 4, 8 or 16")
+                if nk > maxnk[wg]:
+                    raise _lib.PsbError(f"split form: nk {nk} exceeds the supported maximum")
+                key = (wg, nk <= resnk[wg])
+                target_classes = classes
             for i in range(0, len(ws), wg):
                 g = np.zeros(1, dtype=abi.SPLIT_GROUP_DTYPE)
                 g["table"] = t
                 g["nw"] = len(ws[i:i + wg])
                 g["wire"][0, :] = -1
                 g["wire"][0, :g["nw"][0]] = ws[i:i + wg]
-                classes.setdefault(key, []).append(g)
+                target_classes.setdefault(key, []).append(g)
         self.split_launches = []
         for key in classes:
             ga = np.concatenate(classes[key])
@@ -143,11 +170,19 @@ class WireBatch:
             self.split_launches.append((key[0], device.to_device(ga), len(ga), nkmax))
         # the class with the largest grid first: its CTAs run longest
         self.split_launches.sort(key=lambda l: -l[3])
+        # per-wire classes: (W, groups, count, nkmax, table flags)
+        self.wire_launches = []
+        for key in wclasses:
+            ga = np.concatenate(wclasses[key])
+            nkmax = int(nks[ga["table"]].max())
+            self.wire_launches.append((key[0], device.to_device(ga), len(ga), nkmax, key[1]))
+        self.wire_launches.sort(key=lambda l: -l[3])
         # one stream per class, priorities by grid size (the largest grid's
         # CTAs run longest, so the CTA scheduler serves them first)
         least, greatest = torch.cuda.Stream.priority_range()
+        nl = len(self.split_launches) + len(self.wire_launches)
         self.side_streams = [torch.cuda.Stream(priority=min(least, greatest + r))
-                             for r in range(len(self.split_launches))]
+                             for r in range(nl)]
         self.ws = torch.zeros(int(lib.psb_split_ws_bytes(self.n_state)), dtype=torch.uint8,
                               device="cuda")
 
@@ -184,7 +219,7 @@ class WireBatch:
     def launches_per_call(self):
         """Kernel launches one rk4/leapfrog call issues (one per size class)."""
         if self.form == "split":
-            return len(self.split_launches)
+            return len(self.split_launches) + len(self.wire_launches)
         return len(self.classes)
 
     def rhs(self, stream=None):
@@ -207,6 +242,13 @@ class WireBatch:
                           device.ptr(self.y), self.n_state, device.ptr(self.ws), self.ws.numel(),
                           int(nsteps), float(dt), device.ptr(self.P), self.P.shape[0],
                           int(p_stride), self.p_cap, abi.as_ptr(self.model),
+                          device.stream_ptr(s))
+            for (wg, groups, ng, nkmax, tflags), s in zip(self.wire_launches,
+                                                         streams[len(self.split_launches):]):
+                _lib.call("psb_rk4_split_wire", *self._common(), device.ptr(groups), ng, wg,
+                          nkmax, tflags, device.ptr(self.y), self.n_state, device.ptr(self.ws),
+                          self.ws.numel(), int(nsteps), float(dt), device.ptr(self.P),
+                          self.P.shape[0], int(p_stride), self.p_cap, abi.as_ptr(self.model),
                           device.stream_ptr(s))
             for s in streams:
                 join = torch.cuda.Event()

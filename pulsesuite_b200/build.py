@@ -15,7 +15,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libpulsesuite_b200.so")
-SOURCES = ["capi.cu", "coulomb.cu", "sbe_f64.cu", "sbe_full.cu", "sbe_split.cu"]
+SOURCES = ["capi.cu", "coulomb.cu", "sbe_f64.cu", "sbe_full.cu", "sbe_split.cu",
+           "sbe_split_wire.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
