@@ -409,7 +409,9 @@ int psb_rk4_split_noalloc(const PsbTable* d_tables, int ntab, const double* d_ta
  *  - screened tables (PSB_TAB_SCREENED): every stage divides V(q) by
  *    eps(q; n1D) of that wire's own stage densities, as psb_rk4_f64 does
  *    (CalcScreenedArrays, coulomb.py:1212-1230, Eps1D coulomb.py:1172-1193;
- *    eps in FP64);
+ *    eps in FP64, its logarithms in FP64 near q -> 0 where their argument
+ *    is below 1/2 and as FP32 log1p of the exactly formed argument - 1
+ *    elsewhere, ~3e-8 relative in eps);
  *  - distinct Veh, Vee, Vhh (tables without PSB_TAB_SHARED_V; the
  *    reference's CalcCoulombArrays physics, coulomb.py:502-577): p uses Veh,
  *    ne Vee, nh Vhh.

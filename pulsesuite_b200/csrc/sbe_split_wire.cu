@@ -45,12 +45,17 @@
 //   warps 0..7   drain + epilogue: the whole wire per item (8 warps share
 //                its row tiles), FP64 right-hand side and RK4 stage
 //                combination, then the exact column scales and the digits
-//                of the next stage point, the n1D and P(t) sums;
+//                of the next stage point, the n1D and P(t) sums; for
+//                screened tables, then n1D -> eps(q) in FP64
+//                (coulomb.py:1172-1193) -> V/eps -> VS and digits -> the
+//                wire's quad tables for its next stage;
 //   warps 8..11  A-tile generators;
-//   warp 12      TMEM owner and MMA issuer;
-//   warps 13..15 screened tables: after a wire's epilogue, n1D -> eps(q) in
-//                FP64 (coulomb.py:1172-1193) -> V/eps -> VS and digits ->
-//                that wire's quad tables for its next stage.
+//   warps 12..15 MMA issuers, one per row tile mi (mod 4); warp 12 owns
+//                TMEM.  One thread issues a tcgen05.mma about every 100-120
+//                cycles whatever N is (measured on B200 for M = 128, K = 32
+//                int8, N <= 128), while four issuing warps reach about four
+//                times that rate, so the narrow per-wire MMAs are spread
+//                over four issuers with disjoint accumulators.
 // While one wire's epilogue and table run, the tensor cores work on the
 // other wires of the group.  Every mbarrier wait is bounded (as in
 // sbe_split.cu); a CTA that runs out records PSB_ERR_TIMEOUT in its wires'
@@ -64,8 +69,7 @@ namespace splitw {
 
 using namespace psb::split;
 
-constexpr int kBuildWarp0 = 13;  // warps 13..15: per-wire screened tables
-constexpr int kBuildThreads = 96;
+constexpr int kIssuers = 4;  // warps 12..15 issue MMAs (row tiles mi = k mod 4)
 constexpr int kMaxW = PSB_SPLIT_WMAX;
 constexpr int kSeqRows = 24;                // N rows of a sequence per 16-k block
 constexpr int kSeqBlock = kSeqRows * 16;    // bytes per 16-k block (K-direction stride)
@@ -74,19 +78,18 @@ constexpr int kMaxNkW = 2 * kMaxTilesPerWarp * kTileRows;  // 1024
 constexpr int kMaxSlotsW = 8;
 
 // Fixed part of the shared-memory map (bytes from `misc`).
-constexpr uint32_t kOffAbort = 4, kOffSnap = 8, kOffBflag = 16;
+constexpr uint32_t kOffAbort = 4, kOffSnap = 8;
 constexpr uint32_t kOffPulse = 32;                          // double[16][8]
 constexpr uint32_t kOffWpar = kOffPulse + 64 * kMaxW;      // double4[16]
 constexpr uint32_t kOffGaph = kOffWpar + 32 * kMaxW;       // double[16]
 constexpr uint32_t kOffWt = kOffGaph + 8 * kMaxW;          // double[16][2]
 constexpr uint32_t kOffWoff = kOffWt + 16 * kMaxW;         // int64[16]
 constexpr uint32_t kOffVs = kOffWoff + 8 * kMaxW;          // double[16][3]
-constexpr uint32_t kOffNsum = kOffVs + 24 * kMaxW;         // double[16]
-constexpr uint32_t kOffSx = kOffNsum + 8 * kMaxW;          // int[8 warps][16][4]
+constexpr uint32_t kOffSx = kOffVs + 24 * kMaxW;           // int[8 warps][16][4]
 constexpr uint32_t kOffRed = kOffSx + 16 * kEpiWarps * kMaxW;  // [2][8 warps] x 48 B
 constexpr uint32_t kOffSred = kOffRed + 2 * kEpiWarps * 48;    // double[16][4]
 constexpr uint32_t kMiscBytes = kOffSred + 8 * 4 * 16;
-constexpr int kNumBars = 2 * kMaxSlotsW + 5 + 3 * kMaxW;
+constexpr int kNumBars = 2 * kMaxSlotsW + 5 + 2 * kMaxW;
 
 struct Args {
   const PsbTable* tables;
@@ -118,17 +121,17 @@ struct Args {
 // Shared-memory map of one CTA for a grid of nk, W wires, NT matrices.
 template <int NT>
 struct WLayout {
-  uint32_t seq, tab, tabsz, eps, dig, bars, misc, total;
+  uint32_t seq, tab, tabsz, plane, eps, bars, misc, total;
   int ntab_words;
   __host__ __device__ WLayout(int nk, int W, bool scr) {
     const int kpad = kpad_of(nk), nM = mtiles_of(nk);
     seq = (uint32_t)(kpad / 16) * kSeqBlock;
     tab = (uint32_t)(W * NT) * seq;
     ntab_words = kTileRows * nM + kpad;
-    tabsz = 3u * 4u * (uint32_t)ntab_words;
+    plane = (uint32_t)ntab_words + 16u;  // one digit plane's byte array (see build_tables)
+    tabsz = 3u * plane;
     eps = tab + (uint32_t)((scr ? W : 1) * NT) * tabsz;
-    dig = eps + (scr ? 8u * (uint32_t)nk : 0u);
-    bars = (dig + (uint32_t)(NT * 3 * nk) + 15u) & ~15u;
+    bars = (eps + 8u * (uint32_t)(NT * nk) + 15u) & ~15u;
     misc = (bars + 8u * kNumBars + 127u) & ~127u;
     total = misc + kMiscBytes;
   }
@@ -158,39 +161,66 @@ __host__ __device__ constexpr int mat_of(int v) {
   return NT == 1 ? 0 : (v < 2 ? 0 : v - 1);
 }
 
-// Digit-quad tables of the NT matrices of one wire (screened: V / eps(q;
-// n1d)) or of one grid (unscreened): tq[(t * 3 + p) * ntab_words + i] =
-// bytes (a(d), a(d-1), a(d-2), a(d-3)) of digit plane p of matrix t,
-// d = dlo + i, a(d) = digit of V_t(|d|) / eps(|d|) / VS_t (0 at d = 0 and
-// outside the grid), VS_t = 2 max |V_t / eps| (1 + 2^-20) into vs[t].  Run
-// by the nthr threads from t0 on, synchronised on named barrier `bar`.
+// log|(qc - pn) / (qc + n)| of Eps1D, pn = pi n (see build_tables).
+__device__ __forceinline__ double screen_log(double qc, double pn, double n) {
+  const double den = qc + n;
+  if (qc - pn < 0.5 * den) return log(fabs((qc - pn) / den));
+  return (double)log1pf((float)(-(pn + n) / den));
+}
+
+// Digit tables of the NT matrices of one wire (screened: V / eps(q; n1d))
+// or of one grid (unscreened).  Digit plane p of matrix t is a byte array
+// R = tq + (t * 3 + p) * plane with R[c0 - d] = a(d), c0 = dlo + ntab_words
+// - 1 (the largest d a generator reads), a(d) = digit p of V_t(|d|) /
+// eps(|d|) / VS_t, 0 at d = 0 and outside the grid: the word of the four
+// bytes (a(d), a(d-1), a(d-2), a(d-3)) a generator stores into tensor
+// memory is then the four consecutive bytes from R[c0 - d].  The zeros are
+// written once (the arrays start zeroed); a build rewrites a(+q) and
+// a(-q) for 0 < q < nk.  VS_t = 2 max |V_t / eps| (1 + 2^-20) goes to
+// vs[t].  Run by the nthr threads from t0 on, synchronised on named
+// barrier `bar`; sv (NT x nk doubles) holds V_t(q) / eps(q) between the
+// two passes.
 template <int NT>
 __device__ void build_tables(const double* __restrict__ blk, int nk, int ntab_words, int dlo,
-                             bool scr, double n1d, double* eps, int8_t* dig, uint32_t* tq,
+                             bool scr, double n1d, double* sv, uint8_t* tq, uint32_t plane,
                              double* vs, double* red, int t0, int nthr, int bar) {
   const int t = (int)threadIdx.x - t0;
   const int lane = threadIdx.x & 31, wl = t >> 5;
-  if (scr) {
-    // eps(q) of Eps1D (coulomb.py:1172-1193), in the FP64 form's operation order
-    for (int q = t; q < nk; q += nthr) {
-      const double chie = blk[5 * nk + q], chih = blk[6 * nk + q];
-      const double qe = blk[7 * nk + q], qh = blk[8 * nk + q];
-      const double le = log(fabs((qe - kPi * n1d) / (qe + n1d)));
-      const double lh = log(fabs((qh - kPi * n1d) / (qh + n1d)));
-      eps[q] = (1.0 - __dmul_rn(__dmul_rn(chie, 2.0), le)) - __dmul_rn(__dmul_rn(chih, 2.0), lh);
-    }
-    named_sync(bar, nthr);
-  }
+  // pass 1: V_t(q) / eps(q) with eps of Eps1D (coulomb.py:1172-1193) and
+  // the largest magnitude per matrix; two q per iteration.  The logarithm
+  // of R = (qc - pi n) / (qc + n) is FP64 where R < 1/2 (q -> 0, where the
+  // clamped n brings qc - pi n close to zero); elsewhere it is log1pf of
+  // R - 1 = -(pi + 1) n / (qc + n), formed without cancellation, whose
+  // FP32 error (~1e-7 of log R, itself of order R - 1) moves eps by about
+  // 1e-8 -- below the 2^-24.6 at which the digits represent V / eps
   double vm[NT];
 #pragma unroll
   for (int m = 0; m < NT; ++m) vm[m] = 0.0;
-  for (int q = 1 + t; q < nk; q += nthr) {
-    const double e = scr ? eps[q] : 1.0;
+  const double pn = kPi * n1d;
+  for (int q0 = t; q0 < nk; q0 += 2 * nthr) {
+    double ie[2] = {1.0, 1.0};
+    if (scr) {
 #pragma unroll
-    for (int m = 0; m < NT; ++m) {
-      double v = blk[m * nk + q];
-      if (scr) v = v / e;
-      vm[m] = fmax(vm[m], fabs(v));
+      for (int u = 0; u < 2; ++u) {
+        const int qq = min(q0 + u * nthr, nk - 1);
+        const double chie = blk[5 * nk + qq], chih = blk[6 * nk + qq];
+        const double qe = blk[7 * nk + qq], qh = blk[8 * nk + qq];
+        const double le = screen_log(qe, pn, n1d);
+        const double lh = screen_log(qh, pn, n1d);
+        ie[u] = 1.0 / ((1.0 - __dmul_rn(__dmul_rn(chie, 2.0), le)) -
+                       __dmul_rn(__dmul_rn(chih, 2.0), lh));
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int q = q0 + u * nthr;
+      if (q >= nk) continue;
+#pragma unroll
+      for (int m = 0; m < NT; ++m) {
+        const double v = blk[m * nk + q] * ie[u];
+        sv[m * nk + q] = v;
+        if (q > 0) vm[m] = fmax(vm[m], fabs(v));
+      }
     }
   }
 #pragma unroll
@@ -200,6 +230,7 @@ __device__ void build_tables(const double* __restrict__ blk, int nk, int ntab_wo
     if (lane == 0) red[wl * 4 + m] = vm[m];
   }
   named_sync(bar, nthr);
+  // pass 2: the three digits of each V_t(q) / eps(q) / VS_t
   double ivs[NT];
 #pragma unroll
   for (int m = 0; m < NT; ++m) {
@@ -209,43 +240,22 @@ __device__ void build_tables(const double* __restrict__ blk, int nk, int ntab_wo
     if (t == 0) vs[m] = VS;
     ivs[m] = 1.0 / VS;
   }
-  for (int q = t; q < nk; q += nthr) {
-    const double e = scr ? eps[q] : 1.0;
+  const int c0 = dlo + ntab_words - 1;
+  for (int q = 1 + t; q < nk; q += nthr) {
 #pragma unroll
     for (int m = 0; m < NT; ++m) {
-      double x = 0.0;
-      if (q > 0) {
-        double v = blk[m * nk + q];
-        if (scr) v = v / e;
-        x = v * ivs[m];
-      }
+      const double x = sv[m * nk + q] * ivs[m];
       const double f1 = rint(x * kBase);
       const double r1 = x * kBase - f1;
       const double f2 = rint(r1 * kBase);
       const double r2 = r1 * kBase - f2;
       const double f3 = rint(r2 * kBase);
-      dig[(m * 3 + 0) * nk + q] = (int8_t)(int)f1;
-      dig[(m * 3 + 1) * nk + q] = (int8_t)(int)f2;
-      dig[(m * 3 + 2) * nk + q] = (int8_t)(int)f3;
-    }
-  }
-  named_sync(bar, nthr);
-  for (int i = t; i < ntab_words; i += nthr) {
-    const int d = dlo + i;
-#pragma unroll
-    for (int m = 0; m < NT; ++m) {
+      const uint8_t dg[3] = {(uint8_t)(int)f1, (uint8_t)(int)f2, (uint8_t)(int)f3};
 #pragma unroll
       for (int p = 0; p < 3; ++p) {
-        const int8_t* dg = dig + (m * 3 + p) * nk;
-        uint32_t w = 0u;
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const int dd = d - u;
-          const int ad = dd < 0 ? -dd : dd;
-          const int b = (ad > 0 && ad < nk) ? (int)dg[ad] : 0;
-          w |= ((uint32_t)(b & 0xFF)) << (8 * u);
-        }
-        tq[(m * 3 + p) * ntab_words + i] = w;
+        uint8_t* R = tq + (uint32_t)(m * 3 + p) * plane;
+        R[c0 - q] = dg[p];  // d = +q
+        R[c0 + q] = dg[p];  // d = -q
       }
     }
   }
@@ -290,11 +300,10 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_wire_kernel(Args a) {
   const int nslot = slots_of<NT>(nk), G = nslot / 2;
   const int dmin = -(nK - 1), dmax = 2 * (nM - 1);
   const int dlo = 4 - kpad;
-  const uint32_t tabwords = 3u * (uint32_t)L.ntab_words;  // words of one matrix's table
+  const uint32_t c0 = (uint32_t)(dlo + L.ntab_words - 1);  // R[c0 - d] = a(d)
   uint8_t* xbase = smem;  // sequence (j, t) at xbase + (j NT + t) seq
-  uint32_t* tabq = reinterpret_cast<uint32_t*>(smem + L.tab);
-  double* eps = reinterpret_cast<double*>(smem + L.eps);
-  int8_t* dig = reinterpret_cast<int8_t*>(smem + L.dig);
+  uint8_t* tabq = smem + L.tab;  // digit byte arrays (see build_tables)
+  double* sv = reinterpret_cast<double*>(smem + L.eps);  // V_t(q) / eps(q), table builds
   uint64_t* afull = reinterpret_cast<uint64_t*>(smem + L.bars);
   uint64_t* afree = afull + kMaxSlotsW;
   uint64_t* dfull = afree + kMaxSlotsW;
@@ -302,19 +311,16 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_wire_kernel(Args a) {
   uint64_t* final_bar = dfree + 2;
   uint64_t* xfull = final_bar + 1;     // [W] next stage's digits of wire j written
   uint64_t* tabfull = xfull + kMaxW;   // [W] screened table of wire j's next stage built
-  uint64_t* nsumfull = tabfull + kMaxW;  // [W] n1D sum of wire j's next stage point
   uint8_t* misc = smem + L.misc;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(misc);
   volatile int* abort = reinterpret_cast<volatile int*>(misc + kOffAbort);
   volatile int* snap = reinterpret_cast<volatile int*>(misc + kOffSnap);  // [2]
-  volatile int* bflag = reinterpret_cast<volatile int*>(misc + kOffBflag);
   double* pulse = reinterpret_cast<double*>(misc + kOffPulse);
   double4* wpar = reinterpret_cast<double4*>(misc + kOffWpar);
   double* gaph = reinterpret_cast<double*>(misc + kOffGaph);
   double* wtb = reinterpret_cast<double*>(misc + kOffWt);  // [W][2] by step parity
   int64_t* woff = reinterpret_cast<int64_t*>(misc + kOffWoff);
   double* vsw = reinterpret_cast<double*>(misc + kOffVs);  // [W][3] (unscreened: row 0)
-  double* nsum = reinterpret_cast<double*>(misc + kOffNsum);
   int* sx = reinterpret_cast<int*>(misc + kOffSx);  // [epilogue warp][W][4] column scales
   uint8_t* red = misc + kOffRed;                      // [2][8] {float cm[4], double n1, pr, pi}
   double* sred = reinterpret_cast<double*>(misc + kOffSred);
@@ -329,17 +335,16 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_wire_kernel(Args a) {
   if (tid == 0) {
     for (int b = 0; b < kMaxSlotsW; ++b) {
       mbar_init(&afull[b], kGenWarps);
-      mbar_init(&afree[b], 1);
+      mbar_init(&afree[b], kIssuers);
     }
     for (int b = 0; b < 2; ++b) {
-      mbar_init(&dfull[b], 1);
+      mbar_init(&dfull[b], kIssuers);
       mbar_init(&dfree[b], kEpiWarps);
     }
-    mbar_init(final_bar, 1);
+    mbar_init(final_bar, kIssuers);
     for (int j = 0; j < kMaxW; ++j) {
       mbar_init(&xfull[j], kEpiWarps);
       mbar_init(&tabfull[j], 1);
-      mbar_init(&nsumfull[j], 1);
     }
     *abort = 0;
     snap[0] = 0;
@@ -375,8 +380,9 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_wire_kernel(Args a) {
       for (int j = 0; j < 8; ++j) pc[j] = 0.0;
     }
   }
-  // X sequences start at zero: rows that no digit is written to stay zero
-  for (uint32_t i = tid * 16; i < L.tab; i += kThreadsS * 16)
+  // X sequences and digit tables start at zero: the entries no digit is
+  // written to stay zero
+  for (uint32_t i = tid * 16; i < L.eps; i += kThreadsS * 16)
     *reinterpret_cast<uint4*>(xbase + i) = make_uint4(0, 0, 0, 0);
   __syncthreads();
   // Wire j's stage-0 point (the FP32 copy of y) into the workspace, its
@@ -418,8 +424,9 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_wire_kernel(Args a) {
     if (scr) {
       double n1d = tot / 2.0 / tb.L;
       n1d = n1d < tb.dens_max ? n1d : tb.dens_max;
-      build_tables<NT>(blk, nk, L.ntab_words, dlo, true, n1d, eps, dig,
-                       tabq + (uint32_t)(j * NT) * tabwords, vsw + 3 * j, sred, 0, kThreadsS, 0);
+      build_tables<NT>(blk, nk, L.ntab_words, dlo, true, n1d, sv,
+                       tabq + (uint32_t)(j * NT) * L.tabsz, L.plane, vsw + 3 * j, sred, 0,
+                       kThreadsS, 0);
     }
     int se[4];
     float sc[4];
@@ -450,7 +457,7 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_wire_kernel(Args a) {
     if (tid < 4 * kEpiWarps) sx[((tid >> 2) * kMaxW + j) * 4 + (tid & 3)] = se[tid & 3];
   }
   if (!scr)
-    build_tables<NT>(blk, nk, L.ntab_words, dlo, false, 0.0, eps, dig, tabq, vsw, sred, 0,
+    build_tables<NT>(blk, nk, L.ntab_words, dlo, false, 0.0, sv, tabq, L.plane, vsw, sred, 0,
                      kThreadsS, 0);
   fence_async_smem();
   const int ncols = tmem_cols_w<NT>(nk);
@@ -472,99 +479,84 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_wire_kernel(Args a) {
 
   if (warp >= kMmaWarp) {
     asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(kRegsLow));
-    if (warp == kMmaWarp) {
-      // ---- MMA issuer: items (stage, wire) in order; per item the distinct
-      // tiles d in groups of G slots, every (row tile, k' slice) pair of a
-      // tile, two K steps, three digit planes; lane 0 issues.
-      const bool issuer = lane == 0;
-      uint32_t it = 0;
-      int gb = 0;
-      uint32_t gph = 0;
-      bool go = true;
-      const uint64_t bdesc0 = smem_desc(smem_u32(xbase), kSeqBlock, 128);
-      for (int s = 0; s < total_stages && go; ++s) {
-        for (int j = 0; j < nw && go; ++j, ++it) {
-          const int b = it & 1;
-          bool w8 = true;
-          if (s >= 1) w8 = mbar_wait(&xfull[j], (s - 1) & 1, abort, lim);
-          if (w8 && it >= 2) w8 = mbar_wait(&dfree[b], ((it >> 1) - 1) & 1, abort, lim);
-          go = __all_sync(0xffffffffu, w8);
+    // ---- MMA issuers: items (stage, wire) in order; per item the distinct
+    // tiles d in groups of G slots; issuer k takes the row tiles mi = k
+    // (mod 4) of every (row tile, k' slice) pair of a tile: two K steps,
+    // three digit planes per pair, into that row tile's own accumulator.
+    // Every issuer commits each group (afree) and each item (dfull), so
+    // those barriers expect kIssuers arrivals.  Lane 0 issues.
+    const int ik = warp - kMmaWarp;
+    const bool issuer = lane == 0;
+    uint32_t it = 0;
+    int gb = 0;
+    uint32_t gph = 0;
+    bool go = true;
+    const uint64_t bdesc0 = smem_desc(smem_u32(xbase), kSeqBlock, 128);
+    for (int s = 0; s < total_stages && go; ++s) {
+      for (int j = 0; j < nw && go; ++j, ++it) {
+        const int b = it & 1;
+        bool w8 = true;
+        if (s >= 1) w8 = mbar_wait_sleep(&xfull[j], (s - 1) & 1, abort, lim);
+        if (w8 && it >= 2) w8 = mbar_wait_sleep(&dfree[b], ((it >> 1) - 1) & 1, abort, lim);
+        go = __all_sync(0xffffffffu, w8);
+        if (!go) break;
+        tc_fence_after();
+        const uint32_t dbase = tmem + (uint32_t)b * dstride;
+        // descriptor start addresses count 16-byte units
+        const uint64_t bwire = bdesc0 + (uint64_t)(((uint32_t)(j * NT) * L.seq) >> 4);
+        for (int d0 = dmin; d0 <= dmax; d0 += G) {
+          const int gn = min(G, dmax - d0 + 1);
+          go = __all_sync(0xffffffffu, mbar_wait_sleep(&afull[gb], gph, abort, lim));
           if (!go) break;
           tc_fence_after();
-          const uint32_t dbase = tmem + (uint32_t)b * dstride;
-          // descriptor start addresses count 16-byte units
-          const uint64_t bwire = bdesc0 + (uint64_t)(((uint32_t)(j * NT) * L.seq) >> 4);
-          for (int d0 = dmin; d0 <= dmax; d0 += G) {
-            const int gn = min(G, dmax - d0 + 1);
-            go = __all_sync(0xffffffffu, mbar_wait(&afull[gb], gph, abort, lim));
-            if (!go) break;
-            tc_fence_after();
-            if (issuer) {
-              for (int jj = 0; jj < gn; ++jj) {
-                const int d = d0 + jj;
-                const int mlo = max(0, (d + 1) >> 1), mhi = min(nM - 1, (d + nK - 1) >> 1);
-                const uint32_t aslot =
-                    tmem + acol0 + (uint32_t)((gb * G + jj) * NT * kTileCols);
+          if (issuer) {
+            for (int jj = 0; jj < gn; ++jj) {
+              const int d = d0 + jj;
+              const int mlo = max(0, (d + 1) >> 1), mhi = min(nM - 1, (d + nK - 1) >> 1);
+              // first row tile >= mlo of this issuer
+              const int m0 = mlo + ((ik - mlo) % kIssuers + kIssuers) % kIssuers;
+              const uint32_t aslot = tmem + acol0 + (uint32_t)((gb * G + jj) * NT * kTileCols);
 #pragma unroll
-                for (int t = 0; t < NT; ++t) {
-                  const uint32_t at = aslot + (uint32_t)(t * kTileCols);
-                  const uint64_t bt = bwire + (uint64_t)(((uint32_t)t * L.seq) >> 4);
-                  for (int mi = mlo; mi <= mhi; ++mi) {
-                    const int kj = 2 * mi - d;
-                    const uint32_t dcol = dbase + 16u * (uint32_t)mi;
-                    // the first product into a row tile's accumulator overwrites it
-                    const uint32_t acc0 = (t == 0 && kj == nK - 1) ? 0u : 1u;
-                    const uint64_t bk = bt + (uint64_t)((4 * kj) * (kSeqBlock >> 4));
-                    // K step 0: windows at rows 8, 4, 0 (8 - 4p) of the sequence
-                    umma_i8(dcol, at, bk + 8, idesc16, acc0);
-                    umma_i8(dcol, at + kPlaneCols, bk + 4, idesc16, 1);
-                    umma_i8(dcol, at + 2 * kPlaneCols, bk, idesc16, 1);
-                    // K step 1: 32 k' further (two 16-k blocks)
-                    const uint64_t bk1 = bk + 2 * (kSeqBlock >> 4);
-                    umma_i8(dcol, at + 8, bk1 + 8, idesc16, 1);
-                    umma_i8(dcol, at + kPlaneCols + 8, bk1 + 4, idesc16, 1);
-                    umma_i8(dcol, at + 2 * kPlaneCols + 8, bk1, idesc16, 1);
-                  }
+              for (int t = 0; t < NT; ++t) {
+                const uint32_t at = aslot + (uint32_t)(t * kTileCols);
+                const uint64_t bt = bwire + (uint64_t)(((uint32_t)t * L.seq) >> 4);
+                for (int mi = m0; mi <= mhi; mi += kIssuers) {
+                  const int kj = 2 * mi - d;
+                  const uint32_t dcol = dbase + 16u * (uint32_t)mi;
+                  // the first product into a row tile's accumulator overwrites it
+                  const uint32_t acc0 = (t == 0 && kj == nK - 1) ? 0u : 1u;
+                  const uint64_t bk = bt + (uint64_t)((4 * kj) * (kSeqBlock >> 4));
+                  // K step 0: windows at rows 8, 4, 0 (8 - 4p) of the sequence
+                  umma_i8(dcol, at, bk + 8, idesc16, acc0);
+                  umma_i8(dcol, at + kPlaneCols, bk + 4, idesc16, 1);
+                  umma_i8(dcol, at + 2 * kPlaneCols, bk, idesc16, 1);
+                  // K step 1: 32 k' further (two 16-k blocks)
+                  const uint64_t bk1 = bk + 2 * (kSeqBlock >> 4);
+                  umma_i8(dcol, at + 8, bk1 + 8, idesc16, 1);
+                  umma_i8(dcol, at + kPlaneCols + 8, bk1 + 4, idesc16, 1);
+                  umma_i8(dcol, at + 2 * kPlaneCols + 8, bk1, idesc16, 1);
                 }
               }
-              umma_commit(&afree[gb]);  // the group's slots are free once these finish
             }
-            __syncwarp();
-            if (++gb == 2) {
-              gb = 0;
-              gph ^= 1u;
-            }
+            umma_commit(&afree[gb]);  // the group's slots are free once these finish
           }
-          if (!go) break;
-          if (issuer) umma_commit(&dfull[b]);  // the wire's accumulators are complete
           __syncwarp();
-        }
-      }
-    } else if (scr) {
-      // ---- screened tables of each wire's next stage ---------------------------
-      const int bt = tid - 32 * kBuildWarp0;
-      bool go = true;
-      for (int s = 1; s < total_stages && go; ++s) {
-        for (int j = 0; j < nw; ++j) {
-          if (bt == 0) *bflag = mbar_wait(&nsumfull[j], (s - 1) & 1, abort, lim) ? 1 : 0;
-          named_sync(2, kBuildThreads);
-          if (!*bflag) {
-            go = false;
-            break;
+          if (++gb == 2) {
+            gb = 0;
+            gph ^= 1u;
           }
-          double n1d = nsum[j] / 2.0 / tb.L;
-          n1d = n1d < tb.dens_max ? n1d : tb.dens_max;
-          build_tables<NT>(blk, nk, L.ntab_words, dlo, true, n1d, eps, dig,
-                           tabq + (uint32_t)(j * NT) * tabwords, vsw + 3 * j, sred,
-                           32 * kBuildWarp0, kBuildThreads, 2);
-          if (bt == 0) mbar_arrive(&tabfull[j]);
         }
+        if (!go) break;
+        if (issuer) umma_commit(&dfull[b]);  // this issuer's accumulators are complete
+        __syncwarp();
       }
     }
   } else if (warp >= kGenWarp0) {
     asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(kRegsLow));
     // ---- A-tile generators: row r = 32 gq + lane of tile d is a(64 d + r - c),
-    // c = 0..63; TMEM column jc of a digit plane holds c = 4 jc .. 4 jc + 3.
+    // c = 0..63; TMEM column jc of a digit plane holds c = 4 jc .. 4 jc + 3,
+    // the four bytes from R[c0 - 64 d - r + 4 jc]: 17 aligned words and a
+    // funnel shift give the 16 columns.
     const int gq = warp - kGenWarp0;
     const uint32_t lrow = tmem + ((uint32_t)(32 * gq) << 16);
     int gb = 0;
@@ -573,29 +565,34 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_wire_kernel(Args a) {
     for (int s = 0; s < total_stages && go; ++s) {
       for (int j = 0; j < nw && go; ++j) {
         if (scr && s >= 1) {
-          go = __all_sync(0xffffffffu, mbar_wait(&tabfull[j], (s - 1) & 1, abort, lim));
+          go = __all_sync(0xffffffffu, mbar_wait_sleep(&tabfull[j], (s - 1) & 1, abort, lim));
           if (!go) break;
         }
-        const uint32_t* tq = tabq + (scr ? (uint32_t)(j * NT) * tabwords : 0u);
+        const uint8_t* tq = tabq + (scr ? (uint32_t)(j * NT) * L.tabsz : 0u);
         for (int d0 = dmin; d0 <= dmax; d0 += G) {
           const int gn = min(G, dmax - d0 + 1);
           if (!first) {
-            go = __all_sync(0xffffffffu, mbar_wait(&afree[gb], gph ^ 1u, abort, lim));
+            go = __all_sync(0xffffffffu, mbar_wait_sleep(&afree[gb], gph ^ 1u, abort, lim));
             if (!go) break;
           }
           tc_fence_after();
           for (int jj = 0; jj < gn; ++jj) {
-            const int base = 64 * (d0 + jj) + 32 * gq + lane - dlo;
+            const uint32_t y0 = c0 - (uint32_t)(64 * (d0 + jj) + 32 * gq + lane);
+            const uint32_t sh = 8u * (y0 & 3u);
 #pragma unroll
             for (int t = 0; t < NT; ++t) {
               const uint32_t ta =
                   lrow + acol0 + (uint32_t)(((gb * G + jj) * NT + t) * kTileCols);
 #pragma unroll
               for (int p = 0; p < kDigits; ++p) {
-                const uint32_t* tp = tq + (uint32_t)(t * 3 + p) * (uint32_t)L.ntab_words;
-                uint32_t r[16];
+                const uint32_t* tw = reinterpret_cast<const uint32_t*>(
+                                         tq + (uint32_t)(t * 3 + p) * L.plane) +
+                                     (y0 >> 2);
+                uint32_t w[17], r[16];
 #pragma unroll
-                for (int jc = 0; jc < 16; ++jc) r[jc] = tp[base - 4 * jc];
+                for (int k = 0; k < 17; ++k) w[k] = tw[k];
+#pragma unroll
+                for (int jc = 0; jc < 16; ++jc) r[jc] = __funnelshift_r(w[jc], w[jc + 1], sh);
                 tmem_st16(ta + p * kPlaneCols, r);
               }
             }
@@ -628,13 +625,14 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_wire_kernel(Args a) {
       for (int j = 0; j < nw; ++j, ++it) {
         const int b = it & 1;
         bool got = true;
-        // VS of this wire's stage (screened: built after its previous stage)
-        if (scr && s >= 1) got = mbar_wait(&tabfull[j], (s - 1) & 1, abort, lim);
+        // decode factors VS_t / (hbar 254^2) 2^-sexp (VS of a screened wire's
+        // stage was set by these warps when they built its table); scaling a
+        // float by a power of two is exact
         float fac[4];
 #pragma unroll
         for (int v = 0; v < 4; ++v)
-          fac[v] = (float)ldexp(vsw[(scr ? 3 * j : 0) + mat_of<NT>(v)] * dec_hb,
-                                -sx[(warp * kMaxW + j) * 4 + v]);
+          fac[v] = (float)(vsw[(scr ? 3 * j : 0) + mat_of<NT>(v)] * dec_hb) *
+                   ldexpf(1.f, -sx[(warp * kMaxW + j) * 4 + v]);
         // drive M(t)/hbar of this stage, evaluated by lane 0
         float Mr = 0.f, Mi = 0.f;
         if (lane == 0) {
@@ -820,14 +818,14 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_wire_kernel(Args a) {
           __syncwarp();
           if (lane == 0) mbar_arrive(&xfull[j]);
         }
+        double n1t = 0.0, prt = 0.0, pit = 0.0;
+        for (int wq = 0; wq < kEpiWarps; ++wq) {
+          const double* rd = reinterpret_cast<const double*>(rb + wq * 48 + 16);
+          n1t += rd[0];
+          prt += rd[1];
+          pit += rd[2];
+        }
         if (tid == 0) {
-          double n1t = 0.0, prt = 0.0, pit = 0.0;
-          for (int wq = 0; wq < kEpiWarps; ++wq) {
-            const double* rd = reinterpret_cast<const double*>(rb + wq * 48 + 16);
-            n1t += rd[0];
-            prt += rd[1];
-            pit += rd[2];
-          }
           if (stg == 3 && a.P && a.p_stride > 0 && (step + 1) % a.p_stride == 0) {
             const int rr = (step + 1) / a.p_stride - 1;
             const PsbWire& wd = a.wires[grp.wire[j]];
@@ -836,18 +834,25 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_wire_kernel(Args a) {
               a.P[2 * (wd.p_off + rr) + 1] = wpar[j].w * pit;
             }
           }
-          if (scr && s + 1 < total_stages) {
-            nsum[j] = n1t;
-            mbar_arrive(&nsumfull[j]);
-          }
+        }
+        // screened: this wire's table for its next stage, from the n1D of the
+        // stage point just written (CalcScreenedArrays, coulomb.py:1218-1223)
+        if (scr && s + 1 < total_stages) {
+          double n1d = n1t / 2.0 / tb.L;
+          n1d = n1d < tb.dens_max ? n1d : tb.dens_max;
+          build_tables<NT>(blk, nk, L.ntab_words, dlo, true, n1d, sv,
+                           tabq + (uint32_t)(j * NT) * L.tabsz, L.plane, vsw + 3 * j, sred, 0,
+                           kEpiThreads, 1);
+          if (tid == 0) mbar_arrive(&tabfull[j]);
         }
       }
     }
   }
 
   // ---- teardown -----------------------------------------------------------------
+  // every MMA of every issuer has completed before TMEM is released
+  if (warp >= kMmaWarp && lane == 0) umma_commit(final_bar);
   if (warp == kMmaWarp && lane == 0) {
-    umma_commit(final_bar);
     bool done = false;
     for (uint32_t i = 0; i < kSpinLimit && !done; ++i) done = mbar_try_wait(final_bar, 0);
     if (!done) *abort = 1;

@@ -92,6 +92,19 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volati
   *abort = 1;
   return false;
 }
+// Bounded wait that suspends in try_wait between probes instead of
+// spinning: for roles that wait long (issuers and generators waiting on the
+// epilogue), so that their polling does not take issue slots from the warps
+// doing the arithmetic.  Same contract as mbar_wait.
+__device__ __forceinline__ bool mbar_wait_sleep(uint64_t* bar, uint32_t parity,
+                                                volatile int* abort, uint32_t limit) {
+  for (uint32_t i = 0; i < limit; ++i) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (*abort) return false;
+  }
+  *abort = 1;
+  return false;
+}
 // D[tmem] (+)= A[tmem] * B[smem desc], int8 x int8 -> int32
 __device__ __forceinline__ void umma_i8(uint32_t d_tmem, uint32_t a_tmem, uint64_t bdesc,
                                         uint32_t idesc, uint32_t accum) {
