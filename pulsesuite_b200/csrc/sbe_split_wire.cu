@@ -89,7 +89,7 @@ constexpr uint32_t kOffSx = kOffVs + 24 * kMaxW;           // int[8 warps][16][4
 constexpr uint32_t kOffRed = kOffSx + 16 * kEpiWarps * kMaxW;  // [2][8 warps] x 48 B
 constexpr uint32_t kOffSred = kOffRed + 2 * kEpiWarps * 48;    // double[16][4]
 constexpr uint32_t kMiscBytes = kOffSred + 8 * 4 * 16;
-constexpr int kNumBars = 2 * kMaxSlotsW + 5 + 2 * kMaxW;
+constexpr int kNumBars = 2 * kMaxSlotsW + 5 + 3 * kMaxW;
 
 struct Args {
   const PsbTable* tables;
@@ -121,17 +121,20 @@ struct Args {
 // Shared-memory map of one CTA for a grid of nk, W wires, NT matrices.
 template <int NT>
 struct WLayout {
-  uint32_t seq, tab, tabsz, plane, eps, bars, misc, total;
+  uint32_t seq, tab, tabsz, plane, sv, svsz, qc, vt, bars, misc, total;
   int ntab_words;
   __host__ __device__ WLayout(int nk, int W, bool scr) {
     const int kpad = kpad_of(nk), nM = mtiles_of(nk);
     seq = (uint32_t)(kpad / 16) * kSeqBlock;
     tab = (uint32_t)(W * NT) * seq;
     ntab_words = kTileRows * nM + kpad;
-    plane = (uint32_t)ntab_words + 16u;  // one digit plane's byte array (see build_tables)
+    plane = (uint32_t)ntab_words + 16u;  // one digit plane's byte array (see table_digits)
     tabsz = 3u * plane;
-    eps = tab + (uint32_t)((scr ? W : 1) * NT) * tabsz;
-    bars = (eps + 8u * (uint32_t)(NT * nk) + 15u) & ~15u;
+    sv = tab + (uint32_t)((scr ? W : 1) * NT) * tabsz;  // V / eps per wire (screened)
+    svsz = 8u * (uint32_t)(NT * nk);
+    qc = sv + (uint32_t)(scr ? W : 1) * svsz;          // qe, qh, 2 chi_e, 2 chi_h
+    vt = qc + (scr ? 32u * (uint32_t)nk : 0u);          // V_t
+    bars = (vt + svsz + 15u) & ~15u;
     misc = (bars + 8u * kNumBars + 127u) & ~127u;
     total = misc + kMiscBytes;
   }
@@ -161,7 +164,7 @@ __host__ __device__ constexpr int mat_of(int v) {
   return NT == 1 ? 0 : (v < 2 ? 0 : v - 1);
 }
 
-// log|(qc - pn) / (qc + n)| of Eps1D, pn = pi n (see build_tables).
+// log|(qc - pn) / (qc + n)| of Eps1D, pn = pi n (see table_scaled).
 __device__ __forceinline__ double screen_log(double qc, double pn, double n) {
   const double den = qc + n;
   if (qc - pn < 0.5 * den) return log(fabs((qc - pn) / den));
@@ -175,24 +178,25 @@ __device__ __forceinline__ double screen_log(double qc, double pn, double n) {
 // eps(|d|) / VS_t, 0 at d = 0 and outside the grid: the word of the four
 // bytes (a(d), a(d-1), a(d-2), a(d-3)) a generator stores into tensor
 // memory is then the four consecutive bytes from R[c0 - d].  The zeros are
-// written once (the arrays start zeroed); a build rewrites a(+q) and
-// a(-q) for 0 < q < nk.  VS_t = 2 max |V_t / eps| (1 + 2^-20) goes to
-// vs[t].  Run by the nthr threads from t0 on, synchronised on named
-// barrier `bar`; sv (NT x nk doubles) holds V_t(q) / eps(q) between the
-// two passes.
+// written once (the arrays start zeroed); a build rewrites a(+q) and a(-q)
+// for 0 < q < nk.  It runs in two passes: table_scaled (the epilogue warps,
+// after a wire's stage) and table_digits (the generator warps, before they
+// generate that wire's tiles).
+//
+// Pass 1: sv[t][q] = V_t(q) / eps(q) with eps of Eps1D (coulomb.py:
+// 1172-1193; qc holds qe, qh, 2 chi_e, 2 chi_h per q, vt the matrices) and
+// VS_t = 2 max |sv_t| (1 + 2^-20) into vs[t] (every thread writes the same
+// value).  Two q per iteration.  The logarithm of R = (qc - pi n) / (qc +
+// n) is FP64 where R < 1/2 (q -> 0, where the clamped n brings qc - pi n
+// close to zero); elsewhere it is log1pf of R - 1 = -(pi + 1) n / (qc + n),
+// formed without cancellation, whose FP32 error (~1e-7 of log R, itself of
+// order R - 1) moves eps by about 1e-8 -- below the 2^-24.6 at which the
+// digits represent V / eps.  nthr threads from t0 on, named barrier `bar`.
 template <int NT>
-__device__ void build_tables(const double* __restrict__ blk, int nk, int ntab_words, int dlo,
-                             bool scr, double n1d, double* sv, uint8_t* tq, uint32_t plane,
-                             double* vs, double* red, int t0, int nthr, int bar) {
+__device__ void table_scaled(const double* qc, const double* vt, int nk, bool scr, double n1d,
+                             double* sv, double* vs, double* red, int t0, int nthr, int bar) {
   const int t = (int)threadIdx.x - t0;
   const int lane = threadIdx.x & 31, wl = t >> 5;
-  // pass 1: V_t(q) / eps(q) with eps of Eps1D (coulomb.py:1172-1193) and
-  // the largest magnitude per matrix; two q per iteration.  The logarithm
-  // of R = (qc - pi n) / (qc + n) is FP64 where R < 1/2 (q -> 0, where the
-  // clamped n brings qc - pi n close to zero); elsewhere it is log1pf of
-  // R - 1 = -(pi + 1) n / (qc + n), formed without cancellation, whose
-  // FP32 error (~1e-7 of log R, itself of order R - 1) moves eps by about
-  // 1e-8 -- below the 2^-24.6 at which the digits represent V / eps
   double vm[NT];
 #pragma unroll
   for (int m = 0; m < NT; ++m) vm[m] = 0.0;
@@ -203,12 +207,9 @@ __device__ void build_tables(const double* __restrict__ blk, int nk, int ntab_wo
 #pragma unroll
       for (int u = 0; u < 2; ++u) {
         const int qq = min(q0 + u * nthr, nk - 1);
-        const double chie = blk[5 * nk + qq], chih = blk[6 * nk + qq];
-        const double qe = blk[7 * nk + qq], qh = blk[8 * nk + qq];
-        const double le = screen_log(qe, pn, n1d);
-        const double lh = screen_log(qh, pn, n1d);
-        ie[u] = 1.0 / ((1.0 - __dmul_rn(__dmul_rn(chie, 2.0), le)) -
-                       __dmul_rn(__dmul_rn(chih, 2.0), lh));
+        const double le = screen_log(qc[qq], pn, n1d);
+        const double lh = screen_log(qc[nk + qq], pn, n1d);
+        ie[u] = 1.0 / ((1.0 - __dmul_rn(qc[2 * nk + qq], le)) - __dmul_rn(qc[3 * nk + qq], lh));
       }
     }
 #pragma unroll
@@ -217,7 +218,7 @@ __device__ void build_tables(const double* __restrict__ blk, int nk, int ntab_wo
       if (q >= nk) continue;
 #pragma unroll
       for (int m = 0; m < NT; ++m) {
-        const double v = blk[m * nk + q] * ie[u];
+        const double v = vt[m * nk + q] * ie[u];
         sv[m * nk + q] = v;
         if (q > 0) vm[m] = fmax(vm[m], fabs(v));
       }
@@ -230,17 +231,23 @@ __device__ void build_tables(const double* __restrict__ blk, int nk, int ntab_wo
     if (lane == 0) red[wl * 4 + m] = vm[m];
   }
   named_sync(bar, nthr);
-  // pass 2: the three digits of each V_t(q) / eps(q) / VS_t
-  double ivs[NT];
 #pragma unroll
   for (int m = 0; m < NT; ++m) {
     double mx = 0.0;
     for (int i = 0; i < nthr / 32; ++i) mx = fmax(mx, red[i * 4 + m]);
-    const double VS = mx > 0.0 ? 2.0 * mx * (1.0 + 0x1p-20) : 1.0;
-    if (t == 0) vs[m] = VS;
-    ivs[m] = 1.0 / VS;
+    vs[m] = mx > 0.0 ? 2.0 * mx * (1.0 + 0x1p-20) : 1.0;
   }
-  const int c0 = dlo + ntab_words - 1;
+}
+
+// Pass 2: the three digits of sv_t(q) / VS_t into the byte arrays (threads
+// t0 .. t0 + nthr - 1; the caller synchronises before the tables are read).
+template <int NT>
+__device__ void table_digits(const double* sv, const double* vs, int nk, int c0, uint8_t* tq,
+                             uint32_t plane, int t0, int nthr) {
+  const int t = (int)threadIdx.x - t0;
+  double ivs[NT];
+#pragma unroll
+  for (int m = 0; m < NT; ++m) ivs[m] = 1.0 / vs[m];
   for (int q = 1 + t; q < nk; q += nthr) {
 #pragma unroll
     for (int m = 0; m < NT; ++m) {
@@ -259,7 +266,6 @@ __device__ void build_tables(const double* __restrict__ blk, int nk, int ntab_wo
       }
     }
   }
-  named_sync(bar, nthr);
 }
 
 template <int NT>
@@ -302,15 +308,18 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_wire_kernel(Args a) {
   const int dlo = 4 - kpad;
   const uint32_t c0 = (uint32_t)(dlo + L.ntab_words - 1);  // R[c0 - d] = a(d)
   uint8_t* xbase = smem;  // sequence (j, t) at xbase + (j NT + t) seq
-  uint8_t* tabq = smem + L.tab;  // digit byte arrays (see build_tables)
-  double* sv = reinterpret_cast<double*>(smem + L.eps);  // V_t(q) / eps(q), table builds
+  uint8_t* tabq = smem + L.tab;  // digit byte arrays (see table_scaled)
+  double* svb = reinterpret_cast<double*>(smem + L.sv);  // V_t(q) / eps(q) per wire
+  double* qcs = reinterpret_cast<double*>(smem + L.qc);  // screening constants per q
+  double* vts = reinterpret_cast<double*>(smem + L.vt);  // V_t(q)
   uint64_t* afull = reinterpret_cast<uint64_t*>(smem + L.bars);
   uint64_t* afree = afull + kMaxSlotsW;
   uint64_t* dfull = afree + kMaxSlotsW;
   uint64_t* dfree = dfull + 2;
   uint64_t* final_bar = dfree + 2;
   uint64_t* xfull = final_bar + 1;     // [W] next stage's digits of wire j written
-  uint64_t* tabfull = xfull + kMaxW;   // [W] screened table of wire j's next stage built
+  uint64_t* svfull = xfull + kMaxW;    // [W] V/eps and VS of wire j's next stage written
+  uint64_t* gdone = svfull + kMaxW;    // [W] every generator warp wrote its share of j's digits
   uint8_t* misc = smem + L.misc;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(misc);
   volatile int* abort = reinterpret_cast<volatile int*>(misc + kOffAbort);
@@ -344,7 +353,8 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_wire_kernel(Args a) {
     mbar_init(final_bar, kIssuers);
     for (int j = 0; j < kMaxW; ++j) {
       mbar_init(&xfull[j], kEpiWarps);
-      mbar_init(&tabfull[j], 1);
+      mbar_init(&svfull[j], 1);
+      mbar_init(&gdone[j], kGenWarps);
     }
     *abort = 0;
     snap[0] = 0;
@@ -382,8 +392,19 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_wire_kernel(Args a) {
   }
   // X sequences and digit tables start at zero: the entries no digit is
   // written to stay zero
-  for (uint32_t i = tid * 16; i < L.eps; i += kThreadsS * 16)
+  for (uint32_t i = tid * 16; i < L.sv; i += kThreadsS * 16)
     *reinterpret_cast<uint4*>(xbase + i) = make_uint4(0, 0, 0, 0);
+  // the matrices and screening constants of the grid, per q
+  for (int q = tid; q < nk; q += kThreadsS) {
+#pragma unroll
+    for (int m = 0; m < NT; ++m) vts[m * nk + q] = blk[m * nk + q];
+    if (scr) {
+      qcs[q] = blk[7 * nk + q];
+      qcs[nk + q] = blk[8 * nk + q];
+      qcs[2 * nk + q] = 2.0 * blk[5 * nk + q];
+      qcs[3 * nk + q] = 2.0 * blk[6 * nk + q];
+    }
+  }
   __syncthreads();
   // Wire j's stage-0 point (the FP32 copy of y) into the workspace, its
   // column maxima and n1D sum; then (screened) its tables, and its digits.
@@ -424,9 +445,12 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_wire_kernel(Args a) {
     if (scr) {
       double n1d = tot / 2.0 / tb.L;
       n1d = n1d < tb.dens_max ? n1d : tb.dens_max;
-      build_tables<NT>(blk, nk, L.ntab_words, dlo, true, n1d, sv,
-                       tabq + (uint32_t)(j * NT) * L.tabsz, L.plane, vsw + 3 * j, sred, 0,
-                       kThreadsS, 0);
+      double* svj = svb + (uint32_t)j * (L.svsz / 8);
+      table_scaled<NT>(qcs, vts, nk, true, n1d, svj, vsw + 3 * j, sred, 0, kThreadsS, 0);
+      __syncthreads();
+      table_digits<NT>(svj, vsw + 3 * j, nk, (int)c0, tabq + (uint32_t)(j * NT) * L.tabsz,
+                       L.plane, 0, kThreadsS);
+      __syncthreads();
     }
     int se[4];
     float sc[4];
@@ -456,9 +480,11 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_wire_kernel(Args a) {
     }
     if (tid < 4 * kEpiWarps) sx[((tid >> 2) * kMaxW + j) * 4 + (tid & 3)] = se[tid & 3];
   }
-  if (!scr)
-    build_tables<NT>(blk, nk, L.ntab_words, dlo, false, 0.0, sv, tabq, L.plane, vsw, sred, 0,
-                     kThreadsS, 0);
+  if (!scr) {
+    table_scaled<NT>(qcs, vts, nk, false, 0.0, svb, vsw, sred, 0, kThreadsS, 0);
+    __syncthreads();
+    table_digits<NT>(svb, vsw, nk, (int)c0, tabq, L.plane, 0, kThreadsS);
+  }
   fence_async_smem();
   const int ncols = tmem_cols_w<NT>(nk);
   if (warp == kMmaWarp) {
@@ -565,7 +591,18 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_wire_kernel(Args a) {
     for (int s = 0; s < total_stages && go; ++s) {
       for (int j = 0; j < nw && go; ++j) {
         if (scr && s >= 1) {
-          go = __all_sync(0xffffffffu, mbar_wait_sleep(&tabfull[j], (s - 1) & 1, abort, lim));
+          // the wire's next-stage digits, from the V/eps the epilogue wrote
+          go = __all_sync(0xffffffffu, mbar_wait_sleep(&svfull[j], (s - 1) & 1, abort, lim));
+          if (!go) break;
+          table_digits<NT>(svb + (uint32_t)j * (L.svsz / 8), vsw + 3 * j, nk, (int)c0,
+                           tabq + (uint32_t)(j * NT) * L.tabsz, L.plane, 32 * kGenWarp0,
+                           32 * kGenWarps);
+          // all four warps' digits are written before any tile reads them (a
+          // bounded mbarrier, not a named barrier: a warp that stops on an
+          // abort must not leave the others waiting)
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&gdone[j]);
+          go = __all_sync(0xffffffffu, mbar_wait(&gdone[j], (s - 1) & 1, abort, lim));
           if (!go) break;
         }
         const uint8_t* tq = tabq + (scr ? (uint32_t)(j * NT) * L.tabsz : 0u);
@@ -633,24 +670,22 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_wire_kernel(Args a) {
         for (int v = 0; v < 4; ++v)
           fac[v] = (float)(vsw[(scr ? 3 * j : 0) + mat_of<NT>(v)] * dec_hb) *
                    ldexpf(1.f, -sx[(warp * kMaxW + j) * 4 + v]);
-        // drive M(t)/hbar of this stage, evaluated by lane 0
-        float Mr = 0.f, Mi = 0.f;
-        if (lane == 0) {
+        // drive M(t)/hbar of this stage: lane 0 evaluates pulse 0, lane 1
+        // pulse 1, summed in that order
+        double mr = 0.0, mim = 0.0;
+        if (lane < 2) {
           const double tt = wtb[2 * j + (step & 1)] + (stg == 0 ? 0.0 : (stg == 3 ? h : h / 2.0));
-          const double* pc = pulse + j * 8;
-          double mr = 0.0, mim = 0.0;
-#pragma unroll
-          for (int jj = 0; jj < 2; ++jj) {
-            const double u = tt - pc[4 * jj + 0];
-            const double env = exp(pc[4 * jj + 1] * u * u);
-            mr += pc[4 * jj + 2] * env;
-            mim += pc[4 * jj + 3] * env;
-          }
-          Mr = (float)(mr * inv_hbar);
-          Mi = (float)(mim * inv_hbar);
+          const double* pc = pulse + j * 8 + 4 * lane;
+          const double u = tt - pc[0];
+          const double env = exp(pc[1] * u * u);
+          mr = pc[2] * env;
+          mim = pc[3] * env;
         }
-        Mr = __shfl_sync(0xffffffffu, Mr, 0);
-        Mi = __shfl_sync(0xffffffffu, Mi, 0);
+        const float Mr = (float)((__shfl_sync(0xffffffffu, mr, 0) + __shfl_sync(0xffffffffu, mr, 1)) *
+                                 inv_hbar);
+        const float Mi = (float)((__shfl_sync(0xffffffffu, mim, 0) +
+                                  __shfl_sync(0xffffffffu, mim, 1)) *
+                                 inv_hbar);
         const double gw = wpar[j].y, gj = gaph[j];
         const int64_t wo = woff[j];
         // this thread's elements: loads issued before the accumulator wait
@@ -840,10 +875,9 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_wire_kernel(Args a) {
         if (scr && s + 1 < total_stages) {
           double n1d = n1t / 2.0 / tb.L;
           n1d = n1d < tb.dens_max ? n1d : tb.dens_max;
-          build_tables<NT>(blk, nk, L.ntab_words, dlo, true, n1d, sv,
-                           tabq + (uint32_t)(j * NT) * L.tabsz, L.plane, vsw + 3 * j, sred, 0,
-                           kEpiThreads, 1);
-          if (tid == 0) mbar_arrive(&tabfull[j]);
+          table_scaled<NT>(qcs, vts, nk, true, n1d, svb + (uint32_t)j * (L.svsz / 8), vsw + 3 * j,
+                           sred, 0, kEpiThreads, 1);
+          if (tid == 0) mbar_arrive(&svfull[j]);
         }
       }
     }
