@@ -79,22 +79,31 @@ __device__ __forceinline__ uint32_t x_off(int k, int col, uint32_t sbo) {
   return (uint32_t)((col >> 3) * sbo + (k >> 4) * 128 + (col & 7) * 16 + (k & 15));
 }
 
-// TMEM columns: two row-tile accumulator sets (D2, D3, D4: 3 N each), then
-// the A slots (3 digit planes): all distinct tiles when they fit
-// (persistent), else streamed slots in the remaining columns (up to
-// kMaxSlots), used as two buffers of nslot / 2 slots: the generators fill
-// one group while the MMAs read the other.
+// MMA-issuing warps: one thread issues a tcgen05.mma only every ~100-120
+// cycles whatever N is (measured on B200, M = 128, K = 32 int8, N <= 128),
+// so a group of 4 wires (N = 16, the narrowest MMAs) splits the K slices of
+// every row tile between two issuing warps, each into its own partial
+// accumulators, which the epilogue adds (exact int32 sums).  Wider groups
+// keep one issuer: their accumulators leave no tensor memory for a second
+// set.
+__host__ __device__ constexpr int issuers_of(int n) { return n == 16 ? 2 : 1; }
+// TMEM columns: two row-tile buffers of issuers_of(n) accumulator sets
+// (D2, D3, D4: 3 N each), then the A slots (3 digit planes): all distinct
+// tiles when they fit (persistent), else streamed slots in the remaining
+// columns (up to kMaxSlots), used as two buffers of nslot / 2 slots: the
+// generators fill one group while the MMAs read the other.
 constexpr int kMaxSlots = 8;
+__host__ __device__ inline int acc_cols(int n) { return 6 * n * issuers_of(n); }
 __host__ __device__ inline bool persistent_tiles(int nk, int n) {
-  return 6 * n + kTileCols * ntiles_of(nk) <= kTmemCols;
+  return acc_cols(n) + kTileCols * ntiles_of(nk) <= kTmemCols;
 }
 __host__ __device__ inline int ring_slots(int n) {
-  const int r = (kTmemCols - 6 * n) / kTileCols;
+  const int r = (kTmemCols - acc_cols(n)) / kTileCols;
   return r < kMaxSlots ? r : kMaxSlots;
 }
 __host__ __device__ inline int tmem_cols(int nk, int n) {
   const int slots = persistent_tiles(nk, n) ? ntiles_of(nk) : ring_slots(n);
-  const int need = 6 * n + kTileCols * slots;
+  const int need = acc_cols(n) + kTileCols * slots;
   int c = 32;
   while (c < need) c <<= 1;
   return c;
@@ -158,6 +167,7 @@ struct Layout {
 template <int W, bool RES>
 __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   constexpr int N = 4 * W;
+  constexpr int NI = issuers_of(N);  // MMA-issuing warps (kMmaWarp ..)
   constexpr int WH = W / 2;  // wires per drain/epilogue warp
   extern __shared__ __align__(1024) uint8_t smem[];
   const int tid = threadIdx.x;
@@ -236,13 +246,13 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   if (tid == 0) {
     for (int b = 0; b < kMaxSlots; ++b) {
       mbar_init(&afull[b], kGenWarps);
-      mbar_init(&afree[b], 1);
+      mbar_init(&afree[b], NI);
     }
     for (int b = 0; b < 2; ++b) {
-      mbar_init(&dfull[b], 1);
+      mbar_init(&dfull[b], NI);
       mbar_init(&dfree[b], kEpiWarps);
     }
-    mbar_init(final_bar, 1);
+    mbar_init(final_bar, NI);
     *abort = 0;
     snap[0] = 0;
     snap[1] = 0;
@@ -291,7 +301,7 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   const uint32_t tmem = *tmem_slot;
   // TMEM column map: accumulator set b at 3 N b (D2, D3, D4 at +0, +N,
   // +2N); A slot i at acol0 + kTileCols i (digit plane p at + kPlaneCols p).
-  const uint32_t acol0 = (uint32_t)(6 * N);
+  const uint32_t acol0 = (uint32_t)acc_cols(N);
   double vmax = 0.0;
 #pragma unroll
   for (int i = 0; i < kThreadsS / 32; ++i) vmax = fmax(vmax, vmax_w[i]);
@@ -499,8 +509,8 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   // and 3 down to kRegsLow, the epilogue warpgroups 0 and 1 up to kRegsHigh.
   if (warp >= kMmaWarp) {
     asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(kRegsLow));
-    if (warp == kMmaWarp) {
-    // ---- MMA issuer -----------------------------------------------------------
+    if (warp < kMmaWarp + NI) {
+    // ---- MMA issuers ----------------------------------------------------------
     // The whole warp polls the barriers (uniform control flow) and lane 0
     // alone issues the MMAs and commits.  One thread issues every MMA, and
     // these narrow MMAs are short, so the issuing thread's own instructions
@@ -509,6 +519,11 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
     // three MMAs.  So the MMAs of a row tile (persistent A) or of a group of
     // streamed slots go out in one unbroken sequence, with one poll before
     // it; descriptors and TMEM addresses advance incrementally.
+    // With NI = 2 issuer ik takes the slices kj = ik (mod 2) of every row
+    // tile into accumulator set ik; with streamed A both issuers read every
+    // group (and both release it), so the generators keep filling one
+    // buffer while the issuers read the other.
+    const int ik = warp - kMmaWarp;
     const bool issuer = lane == 0;
     uint32_t it = 0;  // row tiles issued
     int gb = 0;       // streamed group buffer of the next slices (two of G slots)
@@ -533,7 +548,7 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
           if (it >= 2 && !mbar_wait(&dfree[b], ((it >> 1) - 1) & 1, abort, a.spin_limit))
             ok = false;
           tc_fence_after();
-          const uint32_t d2 = tmem + (uint32_t)(3 * N * b);
+          const uint32_t d2 = tmem + (uint32_t)(3 * N * (b * NI + ik));
           const uint32_t d3 = d2 + (uint32_t)N;
           const uint32_t d4 = d2 + (uint32_t)(2 * N);
           // one 64-wide K slice: K step 0 (the tile's first slice overwrites
@@ -550,8 +565,10 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
           if (persist) {
             // persistent slot of slice kj is 2 mi - kj + nK - 1
             if (issuer && ok) {
-              uint32_t a1 = tmem + acol0 + (uint32_t)((2 * mi + nK - 1) * kTileCols);
-              for (int kj = 0; kj < nK; ++kj, a1 -= kTileCols, bd += 32) slice(a1, bd, kj != 0);
+              uint32_t a1 = tmem + acol0 + (uint32_t)((2 * mi + nK - 1 - ik) * kTileCols);
+              bd += 32 * ik;
+              for (int kj = ik; kj < nK; kj += NI, a1 -= NI * kTileCols, bd += 32 * NI)
+                slice(a1, bd, kj != ik);
             }
           } else {
             // streamed: slices k0 .. k0 + gn - 1 sit in slots gb G .. gb G + gn - 1.
@@ -560,7 +577,8 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
             // that has come round again), but it votes on the outcome only
             // once per row tile: a vote costs the issuing lane about as much
             // as the poll.
-            for (int k0 = 0; ok && k0 < nK; k0 += G) {
+            bool first = true;  // this issuer's first slice of the row tile
+            for (int k0 = 0; ok && k0 < nK; k0 += G, bd += 32 * G) {
               const int gn = min(G, nK - k0);
               if (!mbar_wait(&afull[gb], gph, abort, a.spin_limit)) {
                 ok = false;
@@ -569,7 +587,12 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
               tc_fence_after();
               if (issuer) {
                 uint32_t a1 = tmem + acol0 + (uint32_t)(gb * G * kTileCols);
-                for (int j = 0; j < gn; ++j, a1 += kTileCols, bd += 32) slice(a1, bd, k0 + j != 0);
+                uint64_t bj = bd;
+                for (int j = 0; j < gn; ++j, a1 += kTileCols, bj += 32) {
+                  if (((k0 + j) & (NI - 1)) != ik) continue;
+                  slice(a1, bj, !first);
+                  first = false;
+                }
                 umma_commit(&afree[gb]);  // the group's slots are reusable once these finish
               }
               __syncwarp();
@@ -587,7 +610,7 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
       }
       __syncwarp();
       // wait for the epilogue to publish the next stage's X
-      named_sync(1, kEpiThreads + 32);
+      named_sync(1, kEpiThreads + 32 * NI);
       if (snap[s & 1]) break;
     }
     }
@@ -698,10 +721,25 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
           // accumulators of wires w0+jp, w0+jp+1 (8 columns each)
           uint32_t r2[8], r3[8], r4[8];
           if (got) {
-            const uint32_t col = lrow + (uint32_t)(3 * N * b + 4 * (w0 + jp));
+            const uint32_t col = lrow + (uint32_t)(3 * N * b * NI + 4 * (w0 + jp));
             tmem_ld8(col, r2);
             tmem_ld8(col + N, r3);
             tmem_ld8(col + 2 * N, r4);
+            if (NI == 2 && nK > 1) {
+              // the second issuer's partial sums (every row tile has slices
+              // of both issuers when nK > 1)
+              uint32_t s2[8], s3[8], s4[8];
+              tmem_ld8(col + 3 * N, s2);
+              tmem_ld8(col + 4 * N, s3);
+              tmem_ld8(col + 5 * N, s4);
+              tmem_ld_wait();
+#pragma unroll
+              for (int c = 0; c < 8; ++c) {
+                r2[c] += s2[c];
+                r3[c] += s3[c];
+                r4[c] += s4[c];
+              }
+            }
             tmem_ld_wait();
           }
 #pragma unroll
@@ -841,7 +879,7 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
       // this thread's digit stores become visible to the tensor cores
       fence_async_smem();
       if (warp == 0 && lane == 0) snap[s & 1] = *abort;
-      named_sync(1, kEpiThreads + 32);
+      named_sync(1, kEpiThreads + 32 * NI);
       if (snap[s & 1]) break;
     }
     if (!*abort) {
@@ -862,9 +900,9 @@ __global__ void __launch_bounds__(kThreadsS, 1) split_rk4_kernel(Args a) {
   }
 
   // ---- teardown -----------------------------------------------------------------
+  // every MMA of every issuer has completed before TMEM is released
+  if (warp >= kMmaWarp && warp < kMmaWarp + NI && lane == 0) umma_commit(final_bar);
   if (warp == kMmaWarp && lane == 0) {
-    // every MMA this thread issued has completed before TMEM is released
-    umma_commit(final_bar);
     bool done = false;
     for (uint32_t i = 0; i < kSpinLimit && !done; ++i) done = mbar_try_wait(final_bar, 0);
     // MMAs still in flight after the bounded wait: the wires' results are

@@ -119,9 +119,11 @@ def test_split_nonfinite_wire_isolated(cuda):
                                       clean.state()[clean.wire_slice(i)])
 
 
-def test_split_rejects_screened_tables(cuda):
-    grids, w = uneven_case([64], seed=1, nsteps=10)
-    from pulsesuite_b200 import _lib
-
-    with pytest.raises(_lib.PsbError):
-        WireBatch(grids, w, screened=True, form="split")
+def test_split_routes_screened_tables_to_per_wire_kernel(cuda):
+    """psb_rk4_split takes only unscreened tables with one shared matrix;
+    the batch sends screened grids to psb_rk4_split_wire instead."""
+    grids, w = uneven_case([64, 128], seed=1, nsteps=10)
+    b = WireBatch(grids, w, screened=True, form="split")
+    assert not b.split_launches and len(b.wire_launches) >= 1
+    b.rk4(10, 1e-15)
+    assert (b.wires()["status"] == 0).all()
