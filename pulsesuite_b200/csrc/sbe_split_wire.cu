@@ -34,7 +34,8 @@
 // distinct matrices each matrix has its own sequence holding only its
 // columns (zeros elsewhere) and all three add into the same accumulator.
 // A tiles (128 x 64, three digit planes) are generated into TMEM from
-// digit-quad tables as in sbe_split.cu; a tile depends on d = 2 mi - kj
+// per-digit-plane byte arrays (table_scaled / table_digits below); a tile
+// depends on d = 2 mi - kj
 // only, so the MMAs run d by d: each distinct tile is generated once per
 // wire and stage and used for every (row tile, k' slice) pair it serves,
 // with the accumulators of all row tiles of the wire live at once (double
@@ -46,10 +47,10 @@
 //                its row tiles), FP64 right-hand side and RK4 stage
 //                combination, then the exact column scales and the digits
 //                of the next stage point, the n1D and P(t) sums; for
-//                screened tables, then n1D -> eps(q) in FP64
-//                (coulomb.py:1172-1193) -> V/eps -> VS and digits -> the
-//                wire's quad tables for its next stage;
-//   warps 8..11  A-tile generators;
+//                screened tables, then n1D -> eps(q) (coulomb.py:1172-1193)
+//                -> V/eps and VS of the wire's next stage;
+//   warps 8..11  A-tile generators; for a screened wire they first write
+//                the digits of its V/eps / VS into its byte arrays;
 //   warps 12..15 MMA issuers, one per row tile mi (mod 4); warp 12 owns
 //                TMEM.  One thread issues a tcgen05.mma about every 100-120
 //                cycles whatever N is (measured on B200 for M = 128, K = 32
