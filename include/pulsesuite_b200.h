@@ -306,6 +306,62 @@ int psb_full_sources_f64(int nk, int nr, const double* d_kr, const double* d_r,
                          const double* d_window, double L, double dcv, double yw, double sgnw,
                          const double* d_level, double* d_out, void* stream);
 
+/*
+ * The many-body terms of the full-matrix step that mb.params switches on,
+ * all FP64 and in the reference's summation order:
+ *  - diag_dph:    k-dependent dephasing rates GamE, GamH replace gam_e, gam_h
+ *                 in dpdt (CalcGammaE / CalcGammaH, dephasing.py:28-105,
+ *                 540-625; SBEs.py:5225-5228);
+ *  - offdiag_dph: OffDiagDephasing2 added to dpdt (dephasing.py:226-360,
+ *                 713-760; widths gam_eh, gam_h for electrons and gam_e,
+ *                 gam_h for holes, as SBEs.py:5229-5232 passes them);
+ *  - ehs:         carrier-carrier in/out scattering rates MBCE / MBCH
+ *                 (coulomb.py:957-1071, 1298-1326) and
+ *  - phonon:      LO-phonon rates MBPE / MBPH (phonons.py:157-271),
+ *                 applied to the new occupations before the neutrality
+ *                 rescale (SBESolver._relaxation, SBEs.py:5248-5336,
+ *                 5688-5695).
+ * Tables (made once per grid by the caller):
+ *   maps   int32 [6][nk][nk]: k_p_q, k_m_q, k1p, k1p_m_q, k1, k1_m_q of
+ *          InitializeDephasing (dephasing.py:471-538), 0-based, any value
+ *          outside [0, nk) meaning "no partner";
+ *   iq     int32 [nk]: round(|ky / dk|), the index Vxx2 reads (dephasing.py:362);
+ *   xe, xh double [nk] (InitializeDephasing);
+ *   C      double [3][(nk+1)^3]: Ceh, Cee, Chh of CalcMBArrays
+ *          (coulomb.py:367-499), psb_mb_tables_f64;
+ *   ph     double [4][nk][nk]: EP, EPT, HP, HPT of InitializePhonons
+ *          (phonons.py:55-136), vscale its _Vscale;
+ *   eps    double [nk]: eps(q) the step's V3 was screened with (null: 1).
+ * scratch: psb_full_mb_scratch_bytes(nk) bytes, caller-owned.
+ */
+typedef struct PsbFullMB {
+  int32_t diag_dph, offdiag_dph, ehs, phonon;
+  double gam_e, gam_h, gam_eh; /* 1/s */
+  double vscale;               /* phonon coupling scale (J) */
+  const int32_t* maps;
+  const int32_t* iq;
+  const double* xe;
+  const double* xh;
+  const double* C;
+  const double* ph;
+  const double* eps;
+  void* scratch;
+} PsbFullMB;
+
+int64_t psb_full_mb_scratch_bytes(int nk);
+/* Ceh, Cee, Chh of CalcMBArrays into d_C ([3][(nk+1)^3] doubles, every entry
+ * written): Gaussian delta, or Lorentzian when lorentz != 0 (mb.params
+ * LorentzDelta); ge, gh in 1/s. */
+int psb_mb_tables_f64(int nk, const double* d_Ee, const double* d_Eh, double ge, double gh,
+                      double hbar, int lorentz, double* d_C, void* stream);
+/* psb_full_step_f64 with the many-body terms of *mb (host struct holding
+ * device pointers); mb == NULL is psb_full_step_f64. */
+int psb_full_step_mb_f64(int nk, int nr, int nq0, const double* d_V3, const double* d_Ee,
+                         const double* d_Eh, const double* d_fields,
+                         const PsbFullParams* params, const PsbFullMB* mb, double* d_L1,
+                         double* d_L2, double* d_L3, void* d_work, int64_t n_work_bytes,
+                         void* stream);
+
 /* ---- split-precision tensor-core form (sm_100a tcgen05, kind::i8) --------- */
 /*
  * The batched form of the same RK4 step: per group of wires sharing one k

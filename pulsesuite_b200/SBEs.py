@@ -305,16 +305,18 @@ class SBESolver:
     What is supported is the reference's diagonal sub-case: Optics and
     Excitons with the field entering only at q = 0 of the wire
     (``Ey[NQ0]``: a field uniform along the wire, dipole coupling Ycv), in
-    which the reference's full-matrix state stays exactly diagonal.  Flags
-    whose physics is not diagonal-preserving or not provided (EHs, Phonon,
-    DCTrans, DiagDph, OffDiagDph, Recomb) raise NotImplementedError, as do
-    fields with other q components (``QWCalculator`` windows the field
-    along the wire, which gives it every q: that path needs the full-matrix
-    right-hand side).  No data files are written (the reference's
+    which the reference's full-matrix state stays exactly diagonal.  A
+    field with other q components (``QWCalculator`` windows the field along
+    the wire, which gives it every q) moves the solver to the full Nk x Nk
+    state, and so do the many-body flags DiagDph, OffDiagDph, EHs and Phonon
+    (k-dependent and off-diagonal dephasing, carrier-carrier and LO-phonon
+    relaxation: psb_full_step_mb_f64).  DCTrans and Recomb raise
+    NotImplementedError.  No data files are written (the reference's
     diagnostics under dataQW/ are not reproduced).
     """
 
-    _UNSUPPORTED = ("EHs", "Phonon", "DCTrans", "DiagDph", "OffDiagDph", "Recomb")
+    _UNSUPPORTED = ("DCTrans", "Recomb")
+    _MANY_BODY = ("DiagDph", "OffDiagDph", "EHs", "Phonon")
 
     def __init__(self, q, rr, r0, Emaxxx, lam, Nw, QW, backend="auto"):
         # defaults of SBEs.py:4638-4671, overwritten by the params files
@@ -337,6 +339,7 @@ class SBESolver:
         self._backend = backend
         self.batch = None
         self.full = None
+        self._many_body = False
         if not QW:
             return
         self._read_qw_params()
@@ -344,8 +347,9 @@ class SBESolver:
         bad = [f for f in self._UNSUPPORTED if getattr(self, f)]
         if bad:
             raise NotImplementedError(
-                "mb.params flags " + ", ".join(bad) + " need physics beyond the diagonal "
-                "Hartree-Fock SBE step (not provided by pulsesuite_b200)")
+                "mb.params flags " + ", ".join(bad) + " (DC transport, spontaneous "
+                "recombination) are not provided by pulsesuite_b200")
+        self._many_body = any(getattr(self, f) for f in self._MANY_BODY)
         self.Emax0 = float(Emaxxx)
         kmax = np.sqrt(1.2 * self.gap * 2.0 * self.me / (HBAR**2))
         self.dkr = _twopi / (2.0 * self.L)
@@ -499,6 +503,11 @@ class SBESolver:
             "eps": torch.zeros((1, nk), dtype=torch.float64, device="cuda"),
             "out": torch.zeros((5, self.Nr), dtype=torch.complex128, device="cuda"),
         }
+        self.full["mb"] = None
+        if self._many_body:
+            from . import manybody
+
+            self.full["mb"] = manybody.ManyBody(self, self.full["Ee"], self.full["Eh"])
 
     def _full_step(self, Ex, Ey, Ez, dt, Px, Py, Pz, Re, Rh, w):
         import torch
@@ -531,10 +540,19 @@ class SBESolver:
         prm["gap"], prm["gam_e"], prm["gam_h"] = self.gap, self.gam_e, self.gam_h
         prm["hbar"], prm["dt"] = HBAR, dt
         prm["excitons"], prm["lf"] = int(self.Excitons), int(self.LF)
-        _lib.call("psb_full_step_f64", nk, self.Nr, self.NQ0, _dev.ptr(V3), _dev.ptr(F["Ee"]),
-                  _dev.ptr(F["Eh"]), _dev.ptr(fields), abi.as_ptr(prm), _dev.ptr(L1),
-                  _dev.ptr(L2), _dev.ptr(L3), _dev.ptr(F["work"]), F["work"].numel(),
-                  _dev.stream_ptr())
+        if F["mb"] is not None:
+            # many-body terms (SBEs.py:5225-5232, 5688-5695) with the eps the
+            # table was screened with (E1D of CalcScreenedArrays)
+            mbd = F["mb"].descriptor(eps=F["eps"] if self.Screened else None)
+            _lib.call("psb_full_step_mb_f64", nk, self.Nr, self.NQ0, _dev.ptr(V3),
+                      _dev.ptr(F["Ee"]), _dev.ptr(F["Eh"]), _dev.ptr(fields), abi.as_ptr(prm),
+                      abi.as_ptr(mbd), _dev.ptr(L1), _dev.ptr(L2), _dev.ptr(L3),
+                      _dev.ptr(F["work"]), F["work"].numel(), _dev.stream_ptr())
+        else:
+            _lib.call("psb_full_step_f64", nk, self.Nr, self.NQ0, _dev.ptr(V3),
+                      _dev.ptr(F["Ee"]), _dev.ptr(F["Eh"]), _dev.ptr(fields), abi.as_ptr(prm),
+                      _dev.ptr(L1), _dev.ptr(L2), _dev.ptr(L3), _dev.ptr(F["work"]),
+                      F["work"].numel(), _dev.stream_ptr())
         if not (self.Optics or self.LF):
             return
         _lib.call("psb_full_sources_f64", nk, self.Nr, _dev.ptr(F["kr"]), _dev.ptr(F["r"]),
@@ -579,7 +597,7 @@ class SBESolver:
         q = 0 (``Ey[NQ0]``), the step runs in the diagonal kernel; any other
         field (or a non-diagonal state read from backup files) switches the
         solver, for good, to the full Nk x Nk state (psb_full_step_f64)."""
-        if self.full is None and not self._is_diagonal(Ex, Ey, Ez):
+        if self.full is None and (self._many_body or not self._is_diagonal(Ex, Ey, Ez)):
             self._enter_full()
         if self.full is not None:
             return self._full_step(Ex, Ey, Ez, dt, Px, Py, Pz, Re, Rh, w)

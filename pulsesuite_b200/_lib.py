@@ -36,6 +36,10 @@ _SIGNATURES = {
     "psb_full_work_bytes": ([i32], i64),
     "psb_full_step_f64": ([i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, i64, vp], i32),
     "psb_full_sources_f64": ([i32, i32, vp, vp, vp, f64, f64, f64, f64, vp, vp, vp], i32),
+    "psb_full_mb_scratch_bytes": ([i32], i64),
+    "psb_mb_tables_f64": ([i32, vp, vp, f64, f64, f64, i32, vp, vp], i32),
+    "psb_full_step_mb_f64": ([i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, i64, vp],
+                             i32),
     "psb_split_ws_bytes": ([i64], i64),
     "psb_split_set_wait_limit": ([ctypes.c_uint32], i32),
     "psb_split_smem_bytes": ([i32, i32], i32),

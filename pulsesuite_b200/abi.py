@@ -64,6 +64,15 @@ FULL_PARAMS_DTYPE = np.dtype(
     align=True,
 )
 
+# PsbFullMB: flags, rates, and device pointers (as uint64)
+FULL_MB_DTYPE = np.dtype(
+    [("diag_dph", "<i4"), ("offdiag_dph", "<i4"), ("ehs", "<i4"), ("phonon", "<i4"),
+     ("gam_e", "<f8"), ("gam_h", "<f8"), ("gam_eh", "<f8"), ("vscale", "<f8"),
+     ("maps", "<u8"), ("iq", "<u8"), ("xe", "<u8"), ("xh", "<u8"), ("C", "<u8"), ("ph", "<u8"),
+     ("eps", "<u8"), ("scratch", "<u8")],
+    align=True,
+)
+
 PSB_SPLIT_WMAX = 16
 PSB_SPLIT_NOALLOC_SCRATCH_BYTES = 8 * 1024 * 1024
 PSB_SPLIT_NOALLOC_MAX_STATE = (PSB_SPLIT_NOALLOC_SCRATCH_BYTES - 32) // 64
@@ -74,6 +83,7 @@ assert TABLE_DTYPE.itemsize == 32
 assert WIRE_DTYPE.itemsize == 136
 assert MODEL_DTYPE.itemsize == 16
 assert FULL_PARAMS_DTYPE.itemsize == 80
+assert FULL_MB_DTYPE.itemsize == 112
 assert SPLIT_GROUP_DTYPE.itemsize == 72
 
 

@@ -14,6 +14,10 @@
 //   dX    = dpdt, dCdt, dDdt (SBEs.py:1952-1975, 2318-2337, 2617-2636)
 //   X3    = X1 + 2 dt dX, occupations |C3_kk|, |D3_kk| rescaled to a common
 //           total, X2 = (X1 + X3) / 2 (SBEs.py:5681-5718)
+// psb_full_step_mb_f64 adds the many-body terms mb.params switches on
+// (DiagDph, OffDiagDph: k-dependent and off-diagonal dephasing in dpdt;
+// EHs, Phonon: carrier-carrier and LO-phonon relaxation of the new
+// occupations before the rescale); see the mb_* kernels.
 // psb_full_sources_f64 evaluates the wire-space source terms of the new
 // level: the polarisation components of QWPolarization3 and the charge
 // densities of QWRho5 before their transforms (qwoptics.py:56-84, 367-381).
@@ -55,6 +59,13 @@ struct Step {
   double2* Meh;         // work [nk][nk]
   double2* H;           // work [3][nk][nk]: Heh, Hee, Hhh
   double2* dX;          // work [3][nk][nk]: dp, dC, dD
+  // many-body terms (null when off): k-dependent dephasing rates, the
+  // off-diagonal dephasing term of dpdt, and X3 written out so that the
+  // relaxation can change its occupations before the neutrality rescale
+  const double* GamE;   // [nk]
+  const double* GamH;   // [nk]
+  const double2* OffP;  // [nk][nk], OffP[kh][ke]
+  const double2* X3;    // [3][nk][nk]
 };
 
 // Meh[ke][kh] = -ehint (Xcv Ex[q] + Ycv Ey[q] yw + Zcv Ez[q] (-1)^w),
@@ -159,8 +170,10 @@ __global__ void derivs_kernel(Step s) {
     for (int k = 0; k < nk; ++k) t4 = ca(t4, cm(Heh[j * nk + k], D[k * nk + i]));
     double2 r = cs(cs(ca(t1, t2), t3), t4);
     r = ca(r, Heh[j * nk + i]);
-    const double g = s.prm.gam_e + s.prm.gam_h;  // GamE[ke] + GamH[kh]
+    // GamE[ke] + GamH[kh]: the constant rates, or CalcGammaE/H's
+    const double g = s.GamE ? s.GamE[j] + s.GamH[i] : s.prm.gam_e + s.prm.gam_h;
     r = cs(r, cm(make_double2(0.0 * g, hb * g), p[i * nk + j]));
+    if (s.OffP) r = ca(r, s.OffP[e]);  // + OffP[kh][ke]
     s.dX[e] = div_ih(r, hb);
   }
   // dC[k1 = i][k2 = j]
@@ -191,6 +204,7 @@ __global__ void __launch_bounds__(kLfThreads) leapfrog_kernel(Step s) {
   __shared__ double red_e[kLfThreads], red_h[kLfThreads];
   __shared__ double fac[3];
   auto x3_of = [&](int e) -> double2 {
+    if (s.X3) return s.X3[e];  // relaxed occupations (many-body terms)
     return ca(s.L2[e], rs(2.0, rs(dt, s.dX[e])));  // X1 + dX dt 2
   };
   double se = 0.0, sh = 0.0;
@@ -279,6 +293,354 @@ __global__ void sources_kernel(int nk, int nr, const double* kr, const double* r
   out[4 * nr + r] = rh;
 }
 
+
+// ---------------------------------------------------------------------------
+// Many-body terms switched on by mb.params (PsbFullMB).  Each kernel keeps
+// the reference's loop order for every accumulated value.
+// ---------------------------------------------------------------------------
+struct MBView {
+  int nk;
+  const double* V3;    // screened [3][nk] (VC[q, 0, n])
+  const double* Ee;
+  const double* Eh;
+  const double2* L;    // the level the right-hand side reads (p2, C2, D2)
+  double hbar;
+  PsbFullMB mb;
+  double* GamE;
+  double* GamH;
+  double* De;          // [(2 nk + 1)][nk]
+  double* Dh;
+  double2* OffP;
+  double2* X3;         // [3][nk][nk]
+  double* rates;       // [4][nk]: WinE, WoutE, WinH, WoutH
+};
+
+// CalcGammaE / CalcGammaH (dephasing.py:28-105): ne, nh the real parts of
+// the diagonal of C2, D2; Vxx2[q] = V(iq[q])^2; one thread per k.
+__global__ void mb_gamma_kernel(MBView v) {
+  const int nk = v.nk, k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nk) return;
+  const int n2 = nk * nk;
+  const int32_t* kpq = v.mb.maps;
+  const int32_t* kmq = kpq + n2;
+  const int32_t* k1p = kpq + 2 * n2;
+  const int32_t* k1pmq = kpq + 3 * n2;
+  const int32_t* k1 = kpq + 4 * n2;
+  const int32_t* k1mq = kpq + 5 * n2;
+  const double2* C = v.L + n2;
+  const double2* D = v.L + 2 * n2;
+  auto ne = [&](int i) { return C[i * nk + i].x; };
+  auto nh = [&](int i) { return D[i * nk + i].x; };
+  auto in = [&](int i) { return i >= 0 && i < nk; };
+  const double ph = kPi / v.hbar;
+  double ge = 0.0, gh = 0.0;
+  // electron-electron, then electron-hole scattering of electrons
+  for (int q = 0; q < nk; ++q) {
+    const int a = kpq[k * nk + q];
+    if (in(a)) {
+      const double vv = v.V3[nk + v.mb.iq[q]];
+      ge = ge + ph * (vv * vv) * ne(a) * (1.0 - ne(a)) * fabs(v.mb.xe[q]);
+    }
+  }
+  for (int q = 0; q < nk; ++q) {
+    const int a = k1pmq[k * nk + q], b = k1p[k * nk + q], c = kmq[k * nk + q];
+    if (in(a) && in(b) && in(c)) {
+      const double vv = v.V3[v.mb.iq[q]];
+      ge = ge + ph * (vv * vv) *
+                    (nh(a) * (1.0 - nh(b)) * ne(c) + (1.0 - nh(a)) * nh(b) * (1.0 - ne(c))) *
+                    fabs(v.mb.xh[q]);
+    }
+  }
+  // hole-hole, then electron-hole scattering of holes
+  for (int q = 0; q < nk; ++q) {
+    const int a = kpq[k * nk + q];
+    if (in(a)) {
+      const double vv = v.V3[2 * nk + v.mb.iq[q]];
+      gh = gh + ph * (vv * vv) * nh(a) * (1.0 - nh(a)) * fabs(v.mb.xh[q]);
+    }
+  }
+  for (int q = 0; q < nk; ++q) {
+    const int a = k1mq[k * nk + q], b = k1[k * nk + q], c = kmq[k * nk + q];
+    if (in(a) && in(b) && in(c)) {
+      const double vv = v.V3[v.mb.iq[q]];
+      gh = gh + ph * (vv * vv) *
+                    (ne(a) * (1.0 - ne(b)) * nh(c) + (1.0 - ne(a)) * ne(b) * (1.0 - nh(c))) *
+                    fabs(v.mb.xe[q]);
+    }
+  }
+  v.GamE[k] = ge;
+  v.GamH[k] = gh;
+}
+
+__device__ __forceinline__ double lrtz(double a, double b) { return (b / kPi) / (a * a + b * b); }
+
+// CalcOffDiagDeph_E2 / _H2 (dephasing.py:226-318): De[q + nk][k] and
+// Dh[q + nk][k] for q in [-nk, nk], with |C_kk|, |D_kk| as occupations and
+// Vsq(q) = V(|q|)^2 for 0 < |q| < nk; one thread per (q, k), the partner
+// momentum p in the reference's order, then the factor pi / hbar.
+__global__ void mb_offd_kernel(MBView v) {
+  const int nk = v.nk, n2 = nk * nk;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (2 * nk + 1) * nk) return;
+  const int qi = e / nk, k = e - qi * nk, q = qi - nk;
+  const double2* C = v.L + n2;
+  const double2* D = v.L + 2 * n2;
+  const double* Ee = v.Ee;
+  const double* Eh = v.Eh;
+  auto ne = [&](int i) { const double2 c = C[i * nk + i]; return hypot(c.x, c.y); };
+  auto nh = [&](int i) { const double2 c = D[i * nk + i]; return hypot(c.x, c.y); };
+  const int aq = q < 0 ? -q : q;
+  auto vsq = [&](int t) {
+    const double x = (aq > 0 && aq < nk) ? v.V3[t * nk + aq] : 0.0;
+    return x * x;
+  };
+  const double hb = v.hbar;
+  const double b_ee = hb * v.mb.gam_eh, b_eh = hb * v.mb.gam_h;  // De: gee = g[0], geh = g[2]
+  const double b_hh = hb * v.mb.gam_e;                            // Dh: ghh = g[1], geh = g[2]
+  double de = 0.0, dh = 0.0;
+  const int kq = k + q;
+  const bool kin = kq >= 0 && kq < nk;
+  // same-band scattering: q in [max(p - nk, -k), min(p - 1, nk - k - 1)]
+  for (int p = 0; p < nk && kin; ++p) {
+    const int pm = p - q;
+    if (q < max(p - nk, -k) || q > min(p - 1, nk - k - 1) || pm < 0 || pm >= nk) continue;
+    const double Ed = ((Ee[kq] + Ee[pm]) - Ee[p]) - Ee[k];
+    de = de + vsq(1) * lrtz(Ed, b_ee) *
+                  (ne(pm) * (1.0 - ne(p)) * (1.0 - ne(k)) + (1.0 - ne(pm)) * ne(p) * ne(k));
+  }
+  // electron-hole scattering: q in [max(-p, -k), min(nk - p - 1, nk - k - 1)]
+  for (int p = 0; p < nk && kin; ++p) {
+    const int pp = p + q;
+    if (q < max(-p, -k) || q > min(nk - p - 1, nk - k - 1) || pp < 0 || pp >= nk) continue;
+    const double Ed = ((Ee[kq] + Eh[pp]) - Eh[p]) - Ee[k];
+    de = de + vsq(0) * lrtz(Ed, b_eh) *
+                  (nh(pp) * (1.0 - nh(p)) * (1.0 - ne(k)) + (1.0 - nh(pp)) * nh(p) * ne(k));
+  }
+  for (int p = 0; p < nk && kin; ++p) {
+    const int pm = p - q;
+    if (q < max(p - nk, -k) || q > min(p - 1, nk - k - 1) || pm < 0 || pm >= nk) continue;
+    const double Ed = ((Eh[kq] + Eh[pm]) - Eh[p]) - Eh[k];
+    dh = dh + vsq(2) * lrtz(Ed, b_hh) *
+                  (nh(pm) * (1.0 - nh(p)) * (1.0 - nh(k)) + (1.0 - nh(pm)) * nh(p) * nh(k));
+  }
+  for (int p = 0; p < nk && kin; ++p) {
+    const int pp = p + q;
+    if (q < max(-p, -k) || q > min(nk - p - 1, nk - k - 1) || pp < 0 || pp >= nk) continue;
+    const double Ed = ((Eh[kq] + Ee[pp]) - Ee[p]) - Eh[k];
+    dh = dh + vsq(0) * lrtz(Ed, b_eh) *
+                  (ne(pp) * (1.0 - ne(p)) * (1.0 - nh(k)) + (1.0 - ne(pp)) * ne(p) * nh(k));
+  }
+  v.De[e] = de * kPi / hb;
+  v.Dh[e] = dh * kPi / hb;
+}
+
+// OffDiagDephasing2 (dephasing.py:320-359): x[kh][ke] = i hbar (sum_q
+// Dh[q][kh] p[kh + q][ke] + sum_q De[q][ke] p[kh][ke + q]), q != 0; one
+// thread per (kh, ke).
+__global__ void mb_offp_kernel(MBView v) {
+  const int nk = v.nk, e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nk * nk) return;
+  const int kh = e / nk, ke = e - kh * nk;
+  const double2* p = v.L;
+  double2 x = make_double2(0.0, 0.0);
+  for (int q = -kh; q <= nk - kh - 1; ++q) {
+    const double u = q == 0 ? 0.0 : 1.0;  // undel
+    const double d = v.Dh[(q + nk) * nk + kh];
+    const double2 pv = p[(kh + q) * nk + ke];
+    x = ca(x, make_double2(d * pv.x * u, d * pv.y * u));
+  }
+  for (int q = -ke; q <= nk - ke - 1; ++q) {
+    const double u = q == 0 ? 0.0 : 1.0;
+    const double d = v.De[(q + nk) * nk + ke];
+    const double2 pv = p[kh * nk + ke + q];  // p^T[ke + q][kh]
+    x = ca(x, make_double2(d * pv.x * u, d * pv.y * u));
+  }
+  // x * i * hbar
+  v.OffP[e] = make_double2(-x.y * v.hbar, x.x * v.hbar);
+}
+
+// X3 = X1 + 2 dt dX, written out for the relaxation (SBEs.py:5685-5687).
+__global__ void mb_x3_kernel(Step s, double2* X3) {
+  const int n3 = 3 * s.nk * s.nk, e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n3) return;
+  X3[e] = ca(s.L2[e], rs(2.0, rs(s.prm.dt, s.dX[e])));
+}
+
+// In/out scattering rates of the new occupations (SBESolver._relaxation_E/H,
+// SBEs.py:5248-5291): MBCE / MBCH (coulomb.py:957-1071) with |Re n| on the
+// 1-based grid, k3(a, b, c) = a + b - c (1-based, 0 when outside), and the
+// reference's C arrays read at [k - 1][..][..]; then MBPE / MBPH
+// (phonons.py:140-271) with Re n.  One thread per k.
+__global__ void mb_rates_kernel(MBView v) {
+  const int nk = v.nk, k0 = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k0 >= nk) return;
+  const int n2 = nk * nk, N1 = nk + 1;
+  const double2* C3 = v.X3 + n2;
+  const double2* D3 = v.X3 + 2 * n2;
+  // 1-based occupation arrays of MBCE/MBCH: index 0 is 0
+  auto ne1 = [&](int i) { return i == 0 ? 0.0 : fabs(C3[(i - 1) * nk + i - 1].x); };
+  auto nh1 = [&](int i) { return i == 0 ? 0.0 : fabs(D3[(i - 1) * nk + i - 1].x); };
+  auto k3 = [&](int a, int b, int c) {  // 0-based arguments, 1-based result
+    const int r = (a + 1) + (b + 1) - (c + 1);
+    return (r < 1 || r > nk) ? 0 : r;
+  };
+  auto vv2 = [&](int t, int a, int b) {
+    const int d = a > b ? a - b : b - a;
+    const double x = v.V3[t * nk + d];
+    return x * x;
+  };
+  const size_t cs3 = (size_t)N1 * N1 * N1;
+  const double* Ceh = v.mb.C;
+  const double* Cee = Ceh + cs3;
+  const double* Chh = Ceh + 2 * cs3;
+  auto cix = [&](int a, int b, int c) { return ((size_t)a * N1 + b) * N1 + c; };
+  double winE = 0.0, woutE = 0.0, winH = 0.0, woutH = 0.0;
+  if (v.mb.ehs) {
+    const int k = k0 + 1;  // MBCE: k; MBCH: kp
+    for (int q1 = 1; q1 <= nk; ++q1) {
+      for (int q2 = 1; q2 <= nk; ++q2) {
+        {  // electrons (MBCE)
+          const int kp = q1, k1 = q2;
+          int r = k3(kp - 1, k1 - 1, k - 1);
+          if (r > 0)
+            winE += vv2(0, k - 1, k1 - 1) * (1.0 - nh1(kp)) * nh1(r) * ne1(k1) *
+                    Ceh[cix(k - 1, kp - 1, k1 - 1)];
+          r = k3(kp - 1, k - 1, k1 - 1);
+          if (r > 0)
+            woutE += vv2(0, k1 - 1, k - 1) * (1.0 - ne1(k1)) * (1.0 - nh1(kp)) * nh1(r) *
+                     Ceh[cix(k1 - 1, kp - 1, k - 1)];
+          const int k2 = q1, k4 = q2;
+          r = k3(k - 1, k2 - 1, k4 - 1);
+          if (r > 0)
+            winE += vv2(1, k - 1, k4 - 1) * (1.0 - ne1(k2)) * ne1(r) * ne1(k4) *
+                    Cee[cix(k - 1, k2 - 1, k4 - 1)];
+          r = k3(k4 - 1, k2 - 1, k - 1);
+          if (r > 0)
+            woutE += vv2(1, k4 - 1, k - 1) * (1.0 - ne1(k4)) * (1.0 - ne1(k2)) * ne1(r) *
+                     Cee[cix(k4 - 1, k2 - 1, k - 1)];
+        }
+        {  // holes (MBCH): kp is this thread's momentum
+          const int kp = k, kk = q1, k1 = q2;
+          int r = k3(kp - 1, k1 - 1, kk - 1);
+          if (r > 0)
+            winH += vv2(0, kk - 1, k1 - 1) * (1.0 - ne1(kk)) * nh1(r) * ne1(k1) *
+                    Ceh[cix(kk - 1, kp - 1, k1 - 1)];
+          r = k3(kp - 1, kk - 1, k1 - 1);
+          if (r > 0)
+            woutH += vv2(0, k1 - 1, kk - 1) * (1.0 - ne1(kk)) * (1.0 - nh1(r)) * ne1(k1) *
+                     Ceh[cix(kk - 1, r - 1, k1 - 1)];
+          const int k2p = q1, k4p = q2;
+          r = k3(kp - 1, k2p - 1, k4p - 1);
+          if (r > 0)
+            winH += vv2(2, kp - 1, k4p - 1) * (1.0 - nh1(k2p)) * nh1(r) * nh1(k4p) *
+                    Chh[cix(kp - 1, k2p - 1, k4p - 1)];
+          r = k3(k4p - 1, k2p - 1, kp - 1);
+          if (r > 0)
+            woutH += vv2(2, k4p - 1, kp - 1) * (1.0 - nh1(k4p)) * (1.0 - nh1(k2p)) * nh1(r) *
+                     Chh[cix(k4p - 1, k2p - 1, kp - 1)];
+        }
+      }
+    }
+  }
+  if (v.mb.phonon) {
+    // Vep[k][i] = VC_ee[k][i] / E1D[k][i] * Vscale (VC already screened)
+    const double* EP = v.mb.ph;
+    const double* EPT = EP + n2;
+    const double* HP = EP + 2 * n2;
+    const double* HPT = EP + 3 * n2;
+    auto epsd = [&](int d) { return v.mb.eps ? v.mb.eps[d] : 1.0; };
+    double sin_e = 0.0, sout_e = 0.0, sin_h = 0.0, sout_h = 0.0;
+    for (int i = 0; i < nk; ++i) {
+      const int d = i > k0 ? i - k0 : k0 - i;
+      const double vep = v.V3[nk + d] / epsd(d) * v.mb.vscale;
+      const double vhp = v.V3[2 * nk + d] / epsd(d) * v.mb.vscale;
+      const double nei = C3[i * nk + i].x, nhi = D3[i * nk + i].x;
+      sin_e += vep * nei * EPT[i * nk + k0];
+      sout_e += vep * (1.0 - nei) * EP[i * nk + k0];
+      sin_h += vhp * nhi * HPT[i * nk + k0];
+      sout_h += vhp * (1.0 - nhi) * HP[i * nk + k0];
+    }
+    winE = winE + sin_e;
+    woutE = woutE + sout_e;
+    winH = winH + sin_h;
+    woutH = woutH + sout_h;
+  }
+  v.rates[k0] = winE;
+  v.rates[nk + k0] = woutE;
+  v.rates[2 * nk + k0] = winH;
+  v.rates[3 * nk + k0] = woutH;
+}
+
+// n <- exp(-W dt) ((-1 + exp(W dt) + n) Win + n Wout) / (W + small), W = Win
+// + Wout, on the diagonal of C3 and D3 (SBEs.py:5322-5331).
+__global__ void mb_relax_kernel(MBView v, double dt) {
+  const int nk = v.nk, k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nk) return;
+  const int n2 = nk * nk;
+  const double small = 1e-200;
+  for (int b = 0; b < 2; ++b) {
+    const double win = v.rates[2 * b * nk + k], wout = v.rates[(2 * b + 1) * nk + k];
+    const double W = win + wout;
+    double2* c = v.X3 + (1 + b) * n2 + k * nk + k;
+    const double2 n = *c;
+    const double em = exp(-W * dt), ep = exp(W * dt);
+    const double2 s1 = make_double2((-1.0 + ep) + n.x, n.y);
+    const double2 s = make_double2(s1.x * win + n.x * wout, s1.y * win + n.y * wout);
+    const double den = W + small;
+    *c = make_double2(em * s.x / den, em * s.y / den);
+  }
+}
+
+// CalcMBArrays (coulomb.py:367-499) on the (nk+1)^3 grid the reference
+// allocates (index 0 unused); UnDel(i, j) = 0 on row/column 0 and the
+// diagonal, else 1 (coulomb.py:336-366).  One thread per entry.
+__global__ void mb_tables_kernel(int nk, const double* Ee, const double* Eh, double ge,
+                                 double gh, double hb, int lorentz, double* Ceh) {
+  const int N1 = nk + 1;
+  const size_t n3 = (size_t)N1 * N1 * N1;
+  const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n3) return;
+  double* Cee = Ceh + n3;
+  double* Chh = Ceh + 2 * n3;
+  const int a = (int)(e / ((size_t)N1 * N1)), bb = (int)((e / N1) % N1), c = (int)(e % N1);
+  Ceh[e] = Cee[e] = Chh[e] = 0.0;
+  if (a == 0 || bb == 0 || c == 0) return;
+  const int k1 = a - 1, k2 = bb - 1, k4 = c - 1;
+  auto undel = [&](int i, int j) { return (i == 0 || j == 0 || i == j) ? 0.0 : 1.0; };
+  auto gdelta = [&](double x, double w) {
+    if (fabs(w) < 1e-300) return 0.0;
+    return 1.0 / (sqrt(kPi) * w) * exp(-((x / w) * (x / w)));
+  };
+  const double geh = (ge + gh) / 2.0;
+  const double twopi = 2.0 * kPi;
+  // Veh(k1, k2, k30, k4), k30 = k3[k4, k2, k1]
+  int r = (k4 + 1) + (k2 + 1) - (k1 + 1);
+  if (r >= 1 && r <= nk) {
+    const int k30 = r - 1;
+    const double Ed = Ee[k1] + Eh[k2] - Eh[k30] - Ee[k4];
+    if (lorentz) {
+      const double h2 = (hb * geh) * (hb * geh);
+      Ceh[e] = 2.0 * geh * undel(a, c) * undel(bb, r) / (Ed * Ed + h2);
+    } else {
+      Ceh[e] = twopi / hb * undel(a, c) * undel(bb, r) * gdelta(Ed, hb * geh);
+    }
+  }
+  // Vee / Vhh(k1, k2, k30, k4), k30 = k3[k1, k2, k4]
+  r = (k1 + 1) + (k2 + 1) - (k4 + 1);
+  if (r >= 1 && r <= nk) {
+    const int k30 = r - 1;
+    const double Ede = Ee[k1] + Ee[k2] - Ee[k30] - Ee[k4];
+    const double Edh = Eh[k1] + Eh[k2] - Eh[k30] - Eh[k4];
+    if (lorentz) {
+      Cee[e] = 2.0 * ge * undel(a, c) * undel(bb, r) / (Ede * Ede + (hb * ge) * (hb * ge));
+      Chh[e] = 2.0 * gh * undel(a, c) * undel(bb, r) / (Edh * Edh + (hb * gh) * (hb * gh));
+    } else {
+      Cee[e] = twopi / hb * undel(a, c) * undel(bb, r) * gdelta(Ede, hb * ge);
+      Chh[e] = twopi / hb * undel(a, c) * undel(bb, r) * gdelta(Edh, hb * gh);
+    }
+  }
+}
+
 }  // namespace full
 }  // namespace psb
 
@@ -289,11 +651,49 @@ extern "C" int64_t psb_full_work_bytes(int nk) {
   return (int64_t)7 * nk * nk * 16;
 }
 
-extern "C" int psb_full_step_f64(int nk, int nr, int nq0, const double* d_V3, const double* d_Ee,
-                                 const double* d_Eh, const double* d_fields,
-                                 const PsbFullParams* params, double* d_L1, double* d_L2,
-                                 double* d_L3, void* d_work, int64_t n_work_bytes,
+namespace {
+// scratch of the many-body terms: GamE, GamH, De, Dh, OffP, X3, rates
+struct MBScratch {
+  size_t gam, de, dh, offp, x3, rates, total;
+  explicit MBScratch(int nk) {
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const size_t n = (size_t)nk, n2 = n * n, nd = (2 * n + 1) * n;
+    gam = 0;
+    de = al(gam + 2 * n * 8);
+    dh = al(de + nd * 8);
+    offp = al(dh + nd * 8);
+    x3 = al(offp + n2 * 16);
+    rates = al(x3 + 3 * n2 * 16);
+    total = al(rates + 4 * n * 8);
+  }
+};
+}  // namespace
+
+extern "C" int64_t psb_full_mb_scratch_bytes(int nk) {
+  if (nk < 2 || nk > PSB_MAX_NK) return set_error(PSB_ERR_SIZE, "nk %d out of range", nk);
+  return (int64_t)MBScratch(nk).total;
+}
+
+extern "C" int psb_mb_tables_f64(int nk, const double* d_Ee, const double* d_Eh, double ge,
+                                 double gh, double hbar, int lorentz, double* d_C,
                                  void* stream) {
+  if (!d_Ee || !d_Eh || !d_C) return set_error(PSB_ERR_INVALID, "psb_mb_tables_f64: null pointer");
+  if (nk < 2 || nk > PSB_MAX_NK) return set_error(PSB_ERR_SIZE, "psb_mb_tables_f64: nk %d", nk);
+  if (!(hbar > 0.0)) return set_error(PSB_ERR_INVALID, "hbar must be > 0");
+  const size_t n3 = (size_t)(nk + 1) * (nk + 1) * (nk + 1);
+  const int th = 256;
+  const unsigned bl = (unsigned)((n3 + th - 1) / th);
+  full::mb_tables_kernel<<<bl, th, 0, (cudaStream_t)stream>>>(nk, d_Ee, d_Eh, ge, gh, hbar,
+                                                               lorentz ? 1 : 0, d_C);
+  return check_cuda("psb_mb_tables_f64");
+}
+
+extern "C" int psb_full_step_mb_f64(int nk, int nr, int nq0, const double* d_V3,
+                                    const double* d_Ee, const double* d_Eh,
+                                    const double* d_fields, const PsbFullParams* params,
+                                    const PsbFullMB* mb, double* d_L1, double* d_L2,
+                                    double* d_L3, void* d_work, int64_t n_work_bytes,
+                                    void* stream) {
   if (!d_V3 || !d_Ee || !d_Eh || !d_fields || !params || !d_L1 || !d_L2 || !d_L3 || !d_work)
     return set_error(PSB_ERR_INVALID, "psb_full_step_f64: null pointer");
   if (nk < 2 || nk > PSB_MAX_NK || nr < 1 || nq0 < 0 || nq0 >= nr)
@@ -302,6 +702,15 @@ extern "C" int psb_full_step_f64(int nk, int nr, int nq0, const double* d_V3, co
   if (n_work_bytes < psb_full_work_bytes(nk))
     return set_error(PSB_ERR_SIZE, "psb_full_step_f64: work needs psb_full_work_bytes(nk)");
   if (!(params->hbar > 0.0)) return set_error(PSB_ERR_INVALID, "hbar must be > 0");
+  const bool deph = mb && (mb->diag_dph || mb->offdiag_dph);
+  const bool relax = mb && (mb->ehs || mb->phonon);
+  if (mb && (deph || relax)) {
+    if (!mb->scratch) return set_error(PSB_ERR_INVALID, "PsbFullMB.scratch is null");
+    if (mb->diag_dph && (!mb->maps || !mb->iq || !mb->xe || !mb->xh))
+      return set_error(PSB_ERR_INVALID, "PsbFullMB: dephasing tables missing");
+    if ((mb->ehs && !mb->C) || (mb->phonon && !mb->ph))
+      return set_error(PSB_ERR_INVALID, "PsbFullMB: relaxation tables missing");
+  }
   full::Step s{};
   s.nk = nk;
   s.nr = nr;
@@ -319,13 +728,60 @@ extern "C" int psb_full_step_f64(int nk, int nr, int nq0, const double* d_V3, co
   s.Meh = w;
   s.H = w + n2;
   s.dX = w + 4 * n2;
+  full::MBView v{};
+  if (deph || relax) {
+    const MBScratch L(nk);
+    uint8_t* sc = reinterpret_cast<uint8_t*>(mb->scratch);
+    v.nk = nk;
+    v.V3 = d_V3;
+    v.Ee = d_Ee;
+    v.Eh = d_Eh;
+    v.L = s.L3;
+    v.hbar = params->hbar;
+    v.mb = *mb;
+    v.GamE = reinterpret_cast<double*>(sc + L.gam);
+    v.GamH = v.GamE + nk;
+    v.De = reinterpret_cast<double*>(sc + L.de);
+    v.Dh = reinterpret_cast<double*>(sc + L.dh);
+    v.OffP = reinterpret_cast<double2*>(sc + L.offp);
+    v.X3 = reinterpret_cast<double2*>(sc + L.x3);
+    v.rates = reinterpret_cast<double*>(sc + L.rates);
+  }
   cudaStream_t st = (cudaStream_t)stream;
-  const int th = 128, bl = (n2 + th - 1) / th;
+  const int th = 128, bl = (n2 + th - 1) / th, blk = (nk + th - 1) / th;
   full::meh_kernel<<<bl, th, 0, st>>>(s);
   full::calch_kernel<<<bl, th, 0, st>>>(s);
+  // dephasing from the level the right-hand side reads (SBEs.py:5225-5232)
+  if (mb && mb->diag_dph) {
+    full::mb_gamma_kernel<<<blk, th, 0, st>>>(v);
+    s.GamE = v.GamE;
+    s.GamH = v.GamH;
+  }
+  if (mb && mb->offdiag_dph) {
+    const int nd = (2 * nk + 1) * nk;
+    full::mb_offd_kernel<<<(nd + th - 1) / th, th, 0, st>>>(v);
+    full::mb_offp_kernel<<<bl, th, 0, st>>>(v);
+    s.OffP = v.OffP;
+  }
   full::derivs_kernel<<<bl, th, 0, st>>>(s);
+  if (relax) {
+    // X3, its occupations relaxed (SBEs.py:5688-5695), then the rescale
+    full::mb_x3_kernel<<<(3 * n2 + th - 1) / th, th, 0, st>>>(s, v.X3);
+    full::mb_rates_kernel<<<blk, th, 0, st>>>(v);
+    full::mb_relax_kernel<<<blk, th, 0, st>>>(v, params->dt);
+    s.X3 = v.X3;
+  }
   full::leapfrog_kernel<<<1, full::kLfThreads, 0, st>>>(s);
   return check_cuda("psb_full_step_f64");
+}
+
+extern "C" int psb_full_step_f64(int nk, int nr, int nq0, const double* d_V3, const double* d_Ee,
+                                 const double* d_Eh, const double* d_fields,
+                                 const PsbFullParams* params, double* d_L1, double* d_L2,
+                                 double* d_L3, void* d_work, int64_t n_work_bytes,
+                                 void* stream) {
+  return psb_full_step_mb_f64(nk, nr, nq0, d_V3, d_Ee, d_Eh, d_fields, params, nullptr, d_L1,
+                              d_L2, d_L3, d_work, n_work_bytes, stream);
 }
 
 extern "C" int psb_full_sources_f64(int nk, int nr, const double* d_kr, const double* d_r,

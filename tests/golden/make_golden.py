@@ -433,7 +433,7 @@ def make_solver_api(R, out, name="solver_lf_nk32", L=2.85e-8, nsteps=300, dt=10e
 MB_PARAMS_FULL = "1\n1\n0\n{scr}\n0\n0\n1\n0\n0\n0\n0\n0\n0\n0\n0\n"
 
 
-def make_qwcalculator(R, out, name, L=2.85e-8, screened=True, nsteps=200, dt=10e-18):
+def make_qwcalculator(R, out, name, L=2.85e-8, screened=True, nsteps=200, dt=10e-18, mb=None):
     """The reference's QWCalculator as its PSTD caller drives it (rhoPJ.py:311-348):
     propagation-space fields along the wire axis (a Gaussian profile, so the
     windowed wire field has every q component and the state is full-matrix),
@@ -446,7 +446,7 @@ def make_qwcalculator(R, out, name, L=2.85e-8, screened=True, nsteps=200, dt=10e
     with open(os.path.join(run, "params", "qw.params"), "w") as f:
         f.write(QW_PARAMS.format(L=L, gam=gam))
     with open(os.path.join(run, "params", "mb.params"), "w") as f:
-        f.write(MB_PARAMS_FULL.format(scr=1 if screened else 0))
+        f.write(mb if mb is not None else MB_PARAMS_FULL.format(scr=1 if screened else 0))
     os.chdir(run)
     try:
         nrr = 64
@@ -482,6 +482,76 @@ def make_qwcalculator(R, out, name, L=2.85e-8, screened=True, nsteps=200, dt=10e
         print(f"{name}: Nk={nk}, {nsteps} steps x 2 wires in {el:.1f} s, "
               f"max|Pyy| = {np.max(np.abs(outs['Pyy'])):.3e}, "
               f"offdiag |p| = {np.max(np.abs(lv['YY3'] - np.einsum('iiw->iw', lv['YY3'])[None]*0)):.3e}")
+    finally:
+        os.chdir(cwd)
+
+
+MB_PARAMS_MB = "1\n1\n{ehs}\n{scr}\n{ph}\n0\n1\n0\n{dd}\n{od}\n0\n0\n0\n0\n{lor}\n"
+
+
+def _run_dir(prefix, L, gam, mb):
+    run = tempfile.mkdtemp(prefix=prefix, dir=_TMP)
+    os.makedirs(os.path.join(run, "params"))
+    with open(os.path.join(run, "params", "qw.params"), "w") as f:
+        f.write(QW_PARAMS.format(L=L, gam=gam))
+    with open(os.path.join(run, "params", "mb.params"), "w") as f:
+        f.write(mb)
+    return run
+
+
+def make_manybody_units(R, out, L=2.85e-8, gam=5e12):
+    """The reference's many-body functions (CalcGammaE/H, CalcOffDiagDeph_E2
+    /H2, OffDiagDephasing2, MBCE/MBCH, MBPE/MBPH) on random levels of its own
+    grid, unscreened, Lorentzian delta: the inputs one full-matrix step reads
+    (X1 = level 2, X2 = level 3 of the GPU state, dt = 0) and its outputs."""
+    from pulsesuite.PSTD3D import coulomb as C
+    from pulsesuite.PSTD3D import dephasing as D
+    from pulsesuite.PSTD3D import phonons as P
+
+    cwd = os.getcwd()
+    run = _run_dir("mbu_", L, gam, MB_PARAMS_MB.format(ehs=1, scr=0, ph=1, dd=1, od=1, lor=1))
+    os.chdir(run)
+    try:
+        rr = np.linspace(-5e-8, 5e-8, 64)
+        qrr = R.SBEs.GetKArray(64, 64 * (rr[1] - rr[0]))
+        s = R.SBEs.SBESolver(qrr, rr, 0.0, 1e7, 800e-9, 1, True)
+        nk = s.Nk
+        rng = np.random.default_rng(23)
+
+        def level():
+            p = 0.05 * (rng.standard_normal((nk, nk)) + 1j * rng.standard_normal((nk, nk)))
+            c = 0.02 * (rng.standard_normal((nk, nk)) + 1j * rng.standard_normal((nk, nk)))
+            d = 0.02 * (rng.standard_normal((nk, nk)) + 1j * rng.standard_normal((nk, nk)))
+            c[np.diag_indices(nk)] = rng.uniform(0.05, 0.6, nk) + 0.01j * rng.standard_normal(nk)
+            d[np.diag_indices(nk)] = rng.uniform(0.05, 0.6, nk) + 0.01j * rng.standard_normal(nk)
+            return p, c, d
+
+        p1, c1, d1 = level()   # X1 (the new X3 when dt = 0)
+        p2, c2, d2 = level()   # X2 (what the right-hand side reads)
+        ne2, nh2 = np.diag(c2).copy(), np.diag(d2).copy()
+        VC = np.zeros((nk, nk, 3))
+        E1D = np.zeros((nk, nk))
+        C.CalcScreenedArrays(False, s.L, ne2, nh2, VC, E1D)
+        GamE, GamH = np.zeros(nk), np.zeros(nk)
+        D.CalcGammaE(s.kr, ne2, nh2, VC, GamE)
+        D.CalcGammaH(s.kr, ne2, nh2, VC, GamH)
+        g = np.array([s.gam_eh, s.gam_e, s.gam_h])
+        De = D.CalcOffDiagDeph_E2(ne2, nh2, s.kr, s.Ee, s.Eh, g[0], g[2], VC, nk)
+        Dh = D.CalcOffDiagDeph_H2(ne2, nh2, s.kr, s.Ee, s.Eh, g[1], g[2], VC, nk)
+        OffP = np.zeros((nk, nk), complex)
+        D.OffDiagDephasing2(ne2, nh2, p2, s.kr, s.Ee, s.Eh, g, VC, 0.0, OffP)
+        ne3, nh3 = np.real(np.diag(c1)), np.real(np.diag(d1))
+        WinE, WoutE, WinH, WoutH = (np.zeros(nk) for _ in range(4))
+        C.MBCE(ne3, nh3, s.kr, s.Ee, s.Eh, VC, s.gam_eh, s.gam_e, WinE, WoutE)
+        P.MBPE(ne3, VC, E1D, WinE, WoutE)
+        C.MBCH(ne3, nh3, s.kr, s.Ee, s.Eh, VC, s.gam_eh, s.gam_h, WinH, WoutH)
+        P.MBPH(nh3, VC, E1D, WinH, WoutH)
+        np.savez_compressed(os.path.join(out, "manybody_units_nk32.npz"), nk=nk, L=L, gam=gam,
+                            p1=p1, c1=c1, d1=d1, p2=p2, c2=c2, d2=d2, GamE=GamE, GamH=GamH,
+                            De=De, Dh=Dh, OffP=OffP, WinE=WinE, WoutE=WoutE, WinH=WinH,
+                            WoutH=WoutH)
+        print(f"manybody units: Nk={nk}, |GamE| {np.max(np.abs(GamE)):.3e}, |OffP| "
+              f"{np.max(np.abs(OffP)):.3e}, |WinE| {np.max(np.abs(WinE)):.3e}")
     finally:
         os.chdir(cwd)
 
@@ -538,6 +608,10 @@ def main():
     if want("qwcalc"):
         make_qwcalculator(R, out, "qwcalc_screened_nk32", screened=True)
         make_qwcalculator(R, out, "qwcalc_nk32", screened=False, nsteps=120)
+    if want("manybody"):
+        make_manybody_units(R, out)
+        make_qwcalculator(R, out, "qwcalc_manybody_nk32", screened=True, nsteps=120,
+                          mb=MB_PARAMS_MB.format(ehs=1, scr=1, ph=1, dd=1, od=1, lor=0))
     if a.full_c0:
         make_rk4(R, out, "rk4_c0_nk128_full", rwa_case(128, 4000))
 

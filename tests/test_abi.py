@@ -54,6 +54,8 @@ int main(void) {
   printf("%zu %zu\n", offsetof(PsbTable, L), offsetof(PsbTable, dens_max));
   printf("%zu %zu %zu\n", sizeof(PsbFullParams), offsetof(PsbFullParams, dt),
          offsetof(PsbFullParams, lf));
+  printf("%zu %zu %zu %zu\n", sizeof(PsbFullMB), offsetof(PsbFullMB, vscale),
+         offsetof(PsbFullMB, maps), offsetof(PsbFullMB, scratch));
   return 0;
 }
 '''
@@ -71,4 +73,7 @@ int main(void) {
     assert vals[3:9] == [W.fields[f][1] for f in ("gap", "t", "amp", "p_off", "status", "steps")]
     assert vals[9:11] == [abi.TABLE_DTYPE.fields["L"][1], abi.TABLE_DTYPE.fields["dens_max"][1]]
     F = abi.FULL_PARAMS_DTYPE
-    assert vals[11:] == [F.itemsize, F.fields["dt"][1], F.fields["lf"][1]]
+    assert vals[11:14] == [F.itemsize, F.fields["dt"][1], F.fields["lf"][1]]
+    M = abi.FULL_MB_DTYPE
+    assert vals[14:] == [M.itemsize, M.fields["vscale"][1], M.fields["maps"][1],
+                         M.fields["scratch"][1]]
