@@ -320,7 +320,17 @@ int psb_full_sources_f64(int nk, int nr, const double* d_kr, const double* d_r,
  *  - phonon:      LO-phonon rates MBPE / MBPH (phonons.py:157-271),
  *                 applied to the new occupations before the neutrality
  *                 rescale (SBESolver._relaxation, SBEs.py:5248-5336,
- *                 5688-5695).
+ *                 5688-5695);
+ *  - recomb:      spontaneous emission (SpontEmission, emission.py:94-199)
+ *                 from the level the right-hand side reads, applied after
+ *                 that relaxation as n_e *= exp(-Rsp n_h dt), then
+ *                 n_h *= exp(-Rsp n_e dt) (SBEs.py:5335-5337; like the
+ *                 reference, only when ehs or phonon is on);
+ *  - dctrans:     the DC-field transport shift of X3 (Transport,
+ *                 dcfield.py:1169-1247; SBEs.py:5698-5702): with lf the
+ *                 full matrices, else their diagonals, each moved by dc_dk
+ *                 in k as fft -> exp(-i Y dc_dk) -> ifft does, here as the
+ *                 equivalent circular convolution.
  * Tables (made once per grid by the caller):
  *   maps   int32 [6][nk][nk]: k_p_q, k_m_q, k1p, k1p_m_q, k1, k1_m_q of
  *          InitializeDephasing (dephasing.py:471-538), 0-based, any value
@@ -331,7 +341,13 @@ int psb_full_sources_f64(int nk, int nr, const double* d_kr, const double* d_r,
  *          (coulomb.py:367-499), psb_mb_tables_f64;
  *   ph     double [4][nk][nk]: EP, EPT, HP, HPT of InitializePhonons
  *          (phonons.py:55-136), vscale its _Vscale;
- *   eps    double [nk]: eps(q) the step's V3 was screened with (null: 1).
+ *   eps    double [nk]: eps(q) the step's V3 was screened with (null: 1);
+ *   emis   double [2][n_hw]: HOmega and square of InitializeEmission
+ *          (emission.py:35-92, CalcHOmega :220-256), dhw = HOmega[1] -
+ *          HOmega[0], rho0_den = c0^3 pi^2 hbar^3 (rho0, :201-218);
+ *   Y      double [nk]: the FFT wavenumbers of InitializeDC (GetKArray(nk,
+ *          (nk - 1) dky), dcfield.py:39-69, 793).
+ * Per step: dc_dk = -e0 (Edc + Re Ex[nq0]) / hbar * dt (dcfield.py:1240).
  * scratch: psb_full_mb_scratch_bytes(nk) bytes, caller-owned.
  */
 typedef struct PsbFullMB {
@@ -346,6 +362,13 @@ typedef struct PsbFullMB {
   const double* ph;
   const double* eps;
   void* scratch;
+  int32_t recomb, dctrans;
+  double dc_dk;                /* 1/m */
+  double dhw;                  /* J */
+  double rho0_den;             /* c0^3 pi^2 hbar^3 */
+  int32_t n_hw, pad_;
+  const double* emis;
+  const double* Y;
 } PsbFullMB;
 
 int64_t psb_full_mb_scratch_bytes(int nk);
@@ -361,6 +384,39 @@ int psb_full_step_mb_f64(int nk, int nr, int nq0, const double* d_V3, const doub
                          const PsbFullParams* params, const PsbFullMB* mb, double* d_L1,
                          double* d_L2, double* d_L3, void* d_work, int64_t n_work_bytes,
                          void* stream);
+
+/*
+ * All wires of one grid in one step (rhoPJ.QuantumWire's loop over wires,
+ * rhoPJ.py:311-348, each iteration one SBESolver.QWCalculator step): the
+ * kernels of psb_full_step_mb_f64 with the wire as the grid's y index.
+ *   d_tab     the grid's table block [9][nk] (V_eh, V_ee, V_hh, Ee, Eh,
+ *             chi_e, chi_h, qe, qh), as in PsbTable
+ *   screened  each wire's V3 = V / eps(q; n1D) from its own densities
+ *             (L, dens_max as in PsbTable), made in the step; unscreened
+ *             wires share the table's V
+ *   d_fields  [nw][3][nr] complex wire-space fields
+ *   d_wpar    [nw][4] doubles per wire: yw(w), (-1)^w, the DC shift dc_dk
+ *             of that wire (PsbFullMB.dc_dk and .eps are not read), 0
+ *   mb        NULL, or tables shared by the wires with scratch of
+ *             nw * psb_full_mb_scratch_bytes(nk) bytes
+ *   d_L1..L3  [nw][3][nk][nk] complex each
+ *   d_work    psb_full_batch_work_bytes(nw, nk) bytes
+ * A wire's result is the same bits as psb_full_step_mb_f64 on that wire
+ * alone (with the V3 the one-wire screening gives).
+ */
+#define PSB_FULL_MAX_WIRES 65535
+int64_t psb_full_batch_work_bytes(int nw, int nk);
+int psb_full_step_batch_f64(int nw, int nk, int nr, int nq0, const double* d_tab, double L,
+                            double dens_max, int screened, const double* d_fields,
+                            const PsbFullParams* params, const double* d_wpar,
+                            const PsbFullMB* mb, double* d_L1, double* d_L2, double* d_L3,
+                            void* d_work, int64_t n_work_bytes, void* stream);
+/* psb_full_sources_f64 of nw wires: d_levels [nw][3][nk][nk] complex, d_out
+ * [nw][5][nr] complex, yw and (-1)^w of each wire from d_wpar [nw][4]. */
+int psb_full_sources_batch_f64(int nw, int nk, int nr, const double* d_kr, const double* d_r,
+                               const double* d_window, double L, double dcv,
+                               const double* d_wpar, const double* d_levels, double* d_out,
+                               void* stream);
 
 /* ---- split-precision tensor-core form (sm_100a tcgen05, kind::i8) --------- */
 /*

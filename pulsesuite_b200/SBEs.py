@@ -308,15 +308,14 @@ class SBESolver:
     which the reference's full-matrix state stays exactly diagonal.  A
     field with other q components (``QWCalculator`` windows the field along
     the wire, which gives it every q) moves the solver to the full Nk x Nk
-    state, and so do the many-body flags DiagDph, OffDiagDph, EHs and Phonon
-    (k-dependent and off-diagonal dephasing, carrier-carrier and LO-phonon
-    relaxation: psb_full_step_mb_f64).  DCTrans and Recomb raise
-    NotImplementedError.  No data files are written (the reference's
-    diagnostics under dataQW/ are not reproduced).
+    state, and so do the many-body flags DiagDph, OffDiagDph, EHs, Phonon,
+    Recomb and DCTrans (k-dependent and off-diagonal dephasing,
+    carrier-carrier and LO-phonon relaxation, spontaneous emission, DC-field
+    transport: psb_full_step_mb_f64).  No data files are written (the
+    reference's diagnostics under dataQW/ are not reproduced).
     """
 
-    _UNSUPPORTED = ("DCTrans", "Recomb")
-    _MANY_BODY = ("DiagDph", "OffDiagDph", "EHs", "Phonon")
+    _MANY_BODY = ("DiagDph", "OffDiagDph", "EHs", "Phonon", "Recomb", "DCTrans")
 
     def __init__(self, q, rr, r0, Emaxxx, lam, Nw, QW, backend="auto"):
         # defaults of SBEs.py:4638-4671, overwritten by the params files
@@ -344,11 +343,6 @@ class SBESolver:
             return
         self._read_qw_params()
         self._read_mb_params()
-        bad = [f for f in self._UNSUPPORTED if getattr(self, f)]
-        if bad:
-            raise NotImplementedError(
-                "mb.params flags " + ", ".join(bad) + " (DC transport, spontaneous "
-                "recombination) are not provided by pulsesuite_b200")
         self._many_body = any(getattr(self, f) for f in self._MANY_BODY)
         self.Emax0 = float(Emaxxx)
         kmax = np.sqrt(1.2 * self.gap * 2.0 * self.me / (HBAR**2))
@@ -543,7 +537,9 @@ class SBESolver:
         if F["mb"] is not None:
             # many-body terms (SBEs.py:5225-5232, 5688-5695) with the eps the
             # table was screened with (E1D of CalcScreenedArrays)
-            mbd = F["mb"].descriptor(eps=F["eps"] if self.Screened else None)
+            # DC shift of this step from the wire's q = 0 field (SBEs.py:5698-5702)
+            mbd = F["mb"].descriptor(eps=F["eps"] if self.Screened else None,
+                                     eac=float(np.real(np.asarray(Ex)[self.NQ0])), dt=dt)
             _lib.call("psb_full_step_mb_f64", nk, self.Nr, self.NQ0, _dev.ptr(V3),
                       _dev.ptr(F["Ee"]), _dev.ptr(F["Eh"]), _dev.ptr(fields), abi.as_ptr(prm),
                       abi.as_ptr(mbd), _dev.ptr(L1), _dev.ptr(L2), _dev.ptr(L3),
@@ -559,18 +555,85 @@ class SBESolver:
                   _dev.ptr(F["window"]), float(self.L), float(self.dcv), float(yw(w)),
                   float((-1) ** w), _dev.ptr(L3), _dev.ptr(F["out"]), _dev.stream_ptr())
         out = F["out"].cpu().numpy()
+        c3 = L3[1].diagonal().cpu().numpy() if self.LF else None
+        d3 = L3[2].diagonal().cpu().numpy() if self.LF else None
+        self._full_sources_post(out, c3, d3, Px, Py, Pz, Re, Rh)
+
+    def _full_sources_post(self, out, c3, d3, Px, Py, Pz, Re, Rh):
+        """Px, Py, Pz (QWPolarization3's factor and transform) and, with LF,
+        Re, Rh (QWRho5's boundary offset, normalisation, transform) from the
+        sums of psb_full_sources_f64 and the new diagonals c3, d3."""
         if self.Optics:
             for a, src in zip((Px, Py, Pz), out[:3]):
                 a[:] = src * 2 * self.ehint / self.area / self.L
                 wirespace.fftg(a)
         if self.LF:
-            c3 = L3[1].diagonal().cpu().numpy()
-            d3 = L3[2].diagonal().cpu().numpy()
             Re[:] = out[3]
             Rh[:] = out[4]
             wirespace.rho_post(Re, Rh, c3, d3, self.r[1] - self.r[0])
             Re[:] = 2.0 * _e0 * Re / self.area * self.ehint
             Rh[:] = 2.0 * _e0 * Rh / self.area * self.ehint
+
+    def _full_step_batch(self, w0, fields, dt):
+        """One step of wires w0 + 1 .. Nw (1-based) on the full state in one
+        launch set (psb_full_step_batch_f64, psb_full_sources_batch_f64);
+        fields [n][3][Nr] complex wire-space Ex, Ey, Ez.  Returns the five
+        source arrays (Px, Py, Pz, Re, Rh) of each wire, as _full_step writes
+        them."""
+        import torch
+
+        from . import device as _dev
+        from .manybody import dc_shift
+
+        F = self.full
+        nk, nw = self.Nk, self.Nw
+        n = nw - w0
+        fd = torch.as_tensor(np.ascontiguousarray(fields, dtype=np.complex128), device="cuda")
+        if not self.Optics:
+            fd.zero_()
+        wpar = np.zeros((n, 4))
+        for i in range(n):
+            w = w0 + i + 1
+            wpar[i, 0], wpar[i, 1] = yw(w), (-1) ** w
+            if F["mb"] is not None:
+                wpar[i, 2] = dc_shift(F["mb"].edc, float(np.real(fields[i][0][self.NQ0])), dt)
+        wpd = torch.as_tensor(wpar, device="cuda")
+        prm = np.zeros(1, dtype=abi.FULL_PARAMS_DTYPE)
+        prm["ehint"], prm["dcv"] = self.ehint, self.dcv
+        prm["gap"], prm["gam_e"], prm["gam_h"] = self.gap, self.gam_e, self.gam_h
+        prm["hbar"], prm["dt"] = HBAR, dt
+        prm["excitons"], prm["lf"] = int(self.Excitons), int(self.LF)
+        if "bwork" not in F:
+            F["bwork"] = torch.empty(int(_lib.load().psb_full_batch_work_bytes(nw, nk)),
+                                     dtype=torch.uint8, device="cuda")
+            F["bout"] = torch.zeros((nw, 5, self.Nr), dtype=torch.complex128, device="cuda")
+        # the descriptor array must outlive the call (its dc_dk and eps are
+        # per wire here: wpar, and the batch's own screening)
+        mbd_arr = None if F["mb"] is None else F["mb"].descriptor()
+        mbd = None if mbd_arr is None else abi.as_ptr(mbd_arr)
+        tab = self.batch.tabdata.view(abi.TAB_BLOCKS, nk)
+        t0 = self.batch.h_tables[0]
+        L1, L2, L3 = (lv[w0:] for lv in F["L"])
+        _lib.call("psb_full_step_batch_f64", n, nk, self.Nr, self.NQ0, _dev.ptr(tab),
+                  float(t0["L"]), float(t0["dens_max"]), int(self.Screened), _dev.ptr(fd),
+                  abi.as_ptr(prm), _dev.ptr(wpd), mbd, _dev.ptr(L1), _dev.ptr(L2),
+                  _dev.ptr(L3), _dev.ptr(F["bwork"]), F["bwork"].numel(), _dev.stream_ptr())
+        srcs = [[np.zeros(self.Nr, np.complex128) for _ in range(5)] for _ in range(n)]
+        if not (self.Optics or self.LF):
+            return srcs
+        out = F["bout"][:n]
+        _lib.call("psb_full_sources_batch_f64", n, nk, self.Nr, _dev.ptr(F["kr"]),
+                  _dev.ptr(F["r"]), _dev.ptr(F["window"]), float(self.L), float(self.dcv),
+                  _dev.ptr(wpd), _dev.ptr(L3), _dev.ptr(out), _dev.stream_ptr())
+        out = out.cpu().numpy()
+        diag = None
+        if self.LF:
+            diag = torch.diagonal(L3[:, 1:3], dim1=-2, dim2=-1).cpu().numpy()  # [n][2][nk]
+        for i in range(n):
+            c3 = diag[i, 0] if diag is not None else None
+            d3 = diag[i, 1] if diag is not None else None
+            self._full_sources_post(out[i], c3, d3, *srcs[i])
+        return srcs
 
     def _drive(self, Ex, Ey, Ez):
         """E = Ey[NQ0] after checking that no other q component reaches Meh."""
@@ -689,6 +752,70 @@ class SBESolver:
             for a in (Pxx, Pyy, Pzz, Rho):
                 a[:] = 0.0
 
+    def QWCalculatorAll(self, Exx, Eyy, Ezz, Vrr, rr, q, dt, Pxx, Pyy, Pzz, Rho, DoQWP,
+                        DoQWDl):
+        """All Nw wires of one Maxwell step at once: the loop of
+        rhoPJ.QuantumWire (rhoPJ.py:311-348), where wire w + 1 gets the
+        fields sampled along it and one QWCalculator call.  Exx, Eyy, Ezz,
+        Vrr are (Nx,) arrays that every wire sees (rhoPJ samples all wires at
+        one place) or (Nx, Nw) arrays, column w for wire w + 1; Pxx, Pyy,
+        Pzz, Rho are (Nx, Nw) arrays written in place.  The counters, the
+        wire-off gate and every wire's outputs are those of the Nw
+        QWCalculator calls in wire order; the steps of the wires that run
+        are one psb_full_step_batch_f64 and one psb_full_sources_batch_f64
+        launch set (a wire's results are the same bits as its own call's)."""
+        nw = self.Nw
+
+        def col(a, w):
+            a = np.asarray(a)
+            return a if a.ndim == 1 else a[:, w]
+
+        for a in (Pxx, Pyy, Pzz, Rho):
+            a[...] = 0.0
+        # the counters of the call for wire 1 (SBEs.py:5849-5854)
+        if self.jjj == self.jmax:
+            self.jjj = 0
+        self.xxx += 1
+        self.jjj += 1
+        self.t += dt
+        # wire-off gate of each call in order: once a wire switches the
+        # solver on, every later wire runs
+        w0 = nw
+        for w in range(nw):
+            mag = np.max(np.sqrt(np.abs(col(Exx, w)) ** 2 + np.abs(col(Eyy, w)) ** 2
+                                 + np.abs(col(Ezz, w)) ** 2))
+            if not (self.wireoff and mag < 1e-3 * self.Emax0):
+                w0 = w
+                break
+        if w0 == nw:
+            return
+        self.wireoff = False
+        DoQWP[0] = self.Optics
+        DoQWDl[0] = self.LF
+        wf = [wirespace.prop2qw(rr, col(Exx, w), col(Eyy, w), col(Ezz, w), col(Vrr, w), self.r,
+                                self.window) for w in range(w0, nw)]
+        if self.full is None and not self._many_body and all(
+                self._is_diagonal(f[0], f[1], f[2]) for f in wf):
+            # fields only at q = 0: the diagonal kernel, wire by wire
+            srcs = []
+            for i, f in enumerate(wf):
+                src = [np.zeros(self.Nr, np.complex128) for _ in range(5)]
+                self._sbe_calculator(f[0], f[1], f[2], f[3], dt, *src, False, w0 + i + 1)
+                srcs.append(src)
+        else:
+            if self.full is None:
+                self._enter_full()
+            srcs = self._full_step_batch(w0, np.stack([np.stack(f[:3]) for f in wf]), dt)
+        for i, src in enumerate(srcs):
+            w = w0 + i
+            Px_, Py_, Pz_, RhoE, RhoH = wirespace.qw2prop(self.r, *src, np.asarray(rr), self.LF)
+            if self.ignorewire:
+                continue
+            Pxx[:, w] = Px_
+            Pyy[:, w] = Py_
+            Pzz[:, w] = Pz_
+            Rho[:, w] = RhoH - RhoE
+
     # -- small accessors (SBEs.py:5516-5534) ---------------------------------------
     def chiqw(self):
         return self.chiw
@@ -787,6 +914,11 @@ def InitializeSBE(q, rr, r0, Emaxxx, lam, Nw, QW):
 def QWCalculator(Exx, Eyy, Ezz, Vrr, rr, q, dt, w, Pxx, Pyy, Pzz, Rho, DoQWP, DoQWDl):
     _default_solver.QWCalculator(Exx, Eyy, Ezz, Vrr, rr, q, dt, w, Pxx, Pyy, Pzz, Rho, DoQWP,
                                  DoQWDl)
+
+
+def QWCalculatorAll(Exx, Eyy, Ezz, Vrr, rr, q, dt, Pxx, Pyy, Pzz, Rho, DoQWP, DoQWDl):
+    _default_solver.QWCalculatorAll(Exx, Eyy, Ezz, Vrr, rr, q, dt, Pxx, Pyy, Pzz, Rho, DoQWP,
+                                    DoQWDl)
 
 
 def chiqw():

@@ -37,6 +37,10 @@ _SIGNATURES = {
     "psb_full_step_f64": ([i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, i64, vp], i32),
     "psb_full_sources_f64": ([i32, i32, vp, vp, vp, f64, f64, f64, f64, vp, vp, vp], i32),
     "psb_full_mb_scratch_bytes": ([i32], i64),
+    "psb_full_batch_work_bytes": ([i32, i32], i64),
+    "psb_full_step_batch_f64": ([i32, i32, i32, i32, vp, f64, f64, i32, vp, vp, vp, vp, vp, vp,
+                                 vp, vp, i64, vp], i32),
+    "psb_full_sources_batch_f64": ([i32, i32, i32, vp, vp, vp, f64, f64, vp, vp, vp, vp], i32),
     "psb_mb_tables_f64": ([i32, vp, vp, f64, f64, f64, i32, vp, vp], i32),
     "psb_full_step_mb_f64": ([i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, i64, vp],
                              i32),

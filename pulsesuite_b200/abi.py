@@ -69,7 +69,9 @@ FULL_MB_DTYPE = np.dtype(
     [("diag_dph", "<i4"), ("offdiag_dph", "<i4"), ("ehs", "<i4"), ("phonon", "<i4"),
      ("gam_e", "<f8"), ("gam_h", "<f8"), ("gam_eh", "<f8"), ("vscale", "<f8"),
      ("maps", "<u8"), ("iq", "<u8"), ("xe", "<u8"), ("xh", "<u8"), ("C", "<u8"), ("ph", "<u8"),
-     ("eps", "<u8"), ("scratch", "<u8")],
+     ("eps", "<u8"), ("scratch", "<u8"), ("recomb", "<i4"), ("dctrans", "<i4"),
+     ("dc_dk", "<f8"), ("dhw", "<f8"), ("rho0_den", "<f8"), ("n_hw", "<i4"), ("pad_", "<i4"),
+     ("emis", "<u8"), ("Y", "<u8")],
     align=True,
 )
 
@@ -83,7 +85,7 @@ assert TABLE_DTYPE.itemsize == 32
 assert WIRE_DTYPE.itemsize == 136
 assert MODEL_DTYPE.itemsize == 16
 assert FULL_PARAMS_DTYPE.itemsize == 80
-assert FULL_MB_DTYPE.itemsize == 112
+assert FULL_MB_DTYPE.itemsize == 168
 assert SPLIT_GROUP_DTYPE.itemsize == 72
 
 

@@ -64,16 +64,6 @@ __global__ void chi1d_kernel(const double* __restrict__ qc, int nq, double alpha
   out[i] = mass * bessel_k0(qc[i] * R) / qc[i] * scale;
 }
 
-// eps(q; n1D) of one table block at density n1d (coulomb.py:1185-1190).
-__device__ __forceinline__ double eps1d(const double* __restrict__ blk, int nk, int q,
-                                        double n1d) {
-  double chie = blk[5 * nk + q], chih = blk[6 * nk + q];
-  double qe = blk[7 * nk + q], qh = blk[8 * nk + q];
-  double le = log(fabs((qe - kPi * n1d) / (qe + n1d)));
-  double lh = log(fabs((qh - kPi * n1d) / (qh + n1d)));
-  return (1.0 - __dmul_rn(__dmul_rn(chie, 2.0), le)) - __dmul_rn(__dmul_rn(chih, 2.0), lh);
-}
-
 __global__ void __launch_bounds__(256) screen_kernel(const PsbTable* __restrict__ tables,
                                                      int ntab, const double* __restrict__ tabdata,
                                                      const PsbWire* __restrict__ wires,

@@ -17,7 +17,8 @@
 // psb_full_step_mb_f64 adds the many-body terms mb.params switches on
 // (DiagDph, OffDiagDph: k-dependent and off-diagonal dephasing in dpdt;
 // EHs, Phonon: carrier-carrier and LO-phonon relaxation of the new
-// occupations before the rescale); see the mb_* kernels.
+// occupations before the rescale; Recomb: spontaneous emission after that
+// relaxation; DCTrans: the DC-field shift of X3 in k); see the mb_* kernels.
 // psb_full_sources_f64 evaluates the wire-space source terms of the new
 // level: the polarisation components of QWPolarization3 and the charge
 // densities of QWRho5 before their transforms (qwoptics.py:56-84, 367-381).
@@ -66,12 +67,45 @@ struct Step {
   const double* GamH;   // [nk]
   const double2* OffP;  // [nk][nk], OffP[kh][ke]
   const double2* X3;    // [3][nk][nk]
+  // a batch of wires of one grid, wire = blockIdx.y: byte strides between
+  // the wires' V3, fields, levels, work and many-body scratch, and the
+  // per-wire [nw][4] = yw, (-1)^w, dc_dk, 0 (null: prm.yw, prm.sgnw)
+  int64_t st_v3, st_e, st_lv, st_wk, st_sc;
+  const double* wpar;
 };
+
+template <class T>
+__device__ __forceinline__ T* bump(T* p, int64_t bytes) {
+  return p ? reinterpret_cast<T*>(reinterpret_cast<uintptr_t>(p) + bytes) : p;
+}
+
+// the Step of wire blockIdx.y of a batch
+__device__ __forceinline__ Step at_wire(Step s) {
+  const int64_t w = blockIdx.y;
+  s.V3 = bump(s.V3, w * s.st_v3);
+  s.E = bump(s.E, w * s.st_e);
+  s.L1 = bump(s.L1, w * s.st_lv);
+  s.L2 = bump(s.L2, w * s.st_lv);
+  s.L3 = bump(s.L3, w * s.st_lv);
+  s.Meh = bump(s.Meh, w * s.st_wk);
+  s.H = bump(s.H, w * s.st_wk);
+  s.dX = bump(s.dX, w * s.st_wk);
+  s.GamE = bump(s.GamE, w * s.st_sc);
+  s.GamH = bump(s.GamH, w * s.st_sc);
+  s.OffP = bump(s.OffP, w * s.st_sc);
+  s.X3 = bump(s.X3, w * s.st_sc);
+  if (s.wpar) {
+    s.prm.yw = s.wpar[4 * w];
+    s.prm.sgnw = s.wpar[4 * w + 1];
+  }
+  return s;
+}
 
 // Meh[ke][kh] = -ehint (Xcv Ex[q] + Ycv Ey[q] yw + Zcv Ez[q] (-1)^w),
 // q = kkp[ke][kh] = ke - kh + NQ0, Xcv = dcv (-1)^(kh+1), Ycv = dcv,
 // Zcv = -dcv (QWOptics dipoles, qwoptics.py:619-623).
-__global__ void meh_kernel(Step s) {
+__global__ void meh_kernel(Step s0) {
+  const Step s = at_wire(s0);
   const int nk = s.nk;
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= nk * nk) return;
@@ -97,7 +131,8 @@ __device__ __forceinline__ double vq(const double* V, int n, int nk, int q) {
 }
 
 // CalcH (SBEs.py:819-935): one thread per (k1, k2).
-__global__ void calch_kernel(Step s) {
+__global__ void calch_kernel(Step s0) {
+  const Step s = at_wire(s0);
   const int nk = s.nk, n2 = nk * nk;
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= n2) return;
@@ -148,7 +183,8 @@ __global__ void calch_kernel(Step s) {
 
 // dpdt / dCdt / dDdt (SBEs.py:1952-1975, 2318-2337, 2617-2636): one thread
 // per (i, j), the four dot products of each in the reference's order.
-__global__ void derivs_kernel(Step s) {
+__global__ void derivs_kernel(Step s0) {
+  const Step s = at_wire(s0);
   const int nk = s.nk, n2 = nk * nk;
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= n2) return;
@@ -198,7 +234,8 @@ __global__ void derivs_kernel(Step s) {
 
 // Leapfrog with neutrality and reshuffle (SBEs.py:5681-5718), one CTA.
 constexpr int kLfThreads = 256;
-__global__ void __launch_bounds__(kLfThreads) leapfrog_kernel(Step s) {
+__global__ void __launch_bounds__(kLfThreads) leapfrog_kernel(Step s0) {
+  const Step s = at_wire(s0);
   const int nk = s.nk, n2 = nk * nk;
   const double dt = s.prm.dt, small = 1e-200;
   __shared__ double red_e[kLfThreads], red_h[kLfThreads];
@@ -245,12 +282,22 @@ __global__ void __launch_bounds__(kLfThreads) leapfrog_kernel(Step s) {
 // Wire-space sources of one level (one thread per r): the QWPolarization3
 // sums (before the 2 ehint / (area L) factor and the transform) and the
 // QWRho5 sums (before the boundary offset, normalisation and transform).
+// Wire blockIdx.y of a batch: levels [nw][3][nk][nk], out [nw][5][nr], yw and
+// (-1)^w from wpar[4 w], wpar[4 w + 1] when wpar is set.
 __global__ void sources_kernel(int nk, int nr, const double* kr, const double* rpos,
                                const double* window, double L, double dcv, double yw,
-                               double sgnw, const double2* lev, double2* out) {
+                               double sgnw, const double* wpar, const double2* lev,
+                               double2* out) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= nr) return;
   const int n2 = nk * nk;
+  const int64_t w = blockIdx.y;
+  lev += w * 3 * n2;
+  out += w * 5 * nr;
+  if (wpar) {
+    yw = wpar[4 * w];
+    sgnw = wpar[4 * w + 1];
+  }
   const double2* p = lev;
   const double2* C = lev + n2;
   const double2* D = lev + 2 * n2;
@@ -312,12 +359,41 @@ struct MBView {
   double* Dh;
   double2* OffP;
   double2* X3;         // [3][nk][nk]
-  double* rates;       // [4][nk]: WinE, WoutE, WinH, WoutH
+  double* rates;       // [5][nk]: WinE, WoutE, WinH, WoutH, Rsp
+  double2* shift;      // [nk]: circulant kernel of the DC shift
+  double2* tr;         // [3][nk][nk]: DC-shift intermediate
+  double gap;          // J
+  int lf;
+  // a batch of wires (blockIdx.y): byte strides of V3, the levels, the
+  // scratch and eps between wires; wpar[4 w + 2] = dc_dk of wire w
+  int64_t st_v3, st_lv, st_sc, st_eps;
+  const double* wpar;
 };
+
+// the MBView of wire blockIdx.y of a batch
+__device__ __forceinline__ MBView at_wire(MBView v) {
+  const int64_t w = blockIdx.y;
+  v.V3 = bump(v.V3, w * v.st_v3);
+  v.L = bump(v.L, w * v.st_lv);
+  const int64_t b = w * v.st_sc;
+  v.GamE = bump(v.GamE, b);
+  v.GamH = bump(v.GamH, b);
+  v.De = bump(v.De, b);
+  v.Dh = bump(v.Dh, b);
+  v.OffP = bump(v.OffP, b);
+  v.X3 = bump(v.X3, b);
+  v.rates = bump(v.rates, b);
+  v.shift = bump(v.shift, b);
+  v.tr = bump(v.tr, b);
+  v.mb.eps = bump(v.mb.eps, w * v.st_eps);
+  if (v.wpar) v.mb.dc_dk = v.wpar[4 * w + 2];
+  return v;
+}
 
 // CalcGammaE / CalcGammaH (dephasing.py:28-105): ne, nh the real parts of
 // the diagonal of C2, D2; Vxx2[q] = V(iq[q])^2; one thread per k.
-__global__ void mb_gamma_kernel(MBView v) {
+__global__ void mb_gamma_kernel(MBView v0) {
+  const MBView v = at_wire(v0);
   const int nk = v.nk, k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nk) return;
   const int n2 = nk * nk;
@@ -378,7 +454,8 @@ __device__ __forceinline__ double lrtz(double a, double b) { return (b / kPi) / 
 // Dh[q + nk][k] for q in [-nk, nk], with |C_kk|, |D_kk| as occupations and
 // Vsq(q) = V(|q|)^2 for 0 < |q| < nk; one thread per (q, k), the partner
 // momentum p in the reference's order, then the factor pi / hbar.
-__global__ void mb_offd_kernel(MBView v) {
+__global__ void mb_offd_kernel(MBView v0) {
+  const MBView v = at_wire(v0);
   const int nk = v.nk, n2 = nk * nk;
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= (2 * nk + 1) * nk) return;
@@ -437,7 +514,8 @@ __global__ void mb_offd_kernel(MBView v) {
 // OffDiagDephasing2 (dephasing.py:320-359): x[kh][ke] = i hbar (sum_q
 // Dh[q][kh] p[kh + q][ke] + sum_q De[q][ke] p[kh][ke + q]), q != 0; one
 // thread per (kh, ke).
-__global__ void mb_offp_kernel(MBView v) {
+__global__ void mb_offp_kernel(MBView v0) {
+  const MBView v = at_wire(v0);
   const int nk = v.nk, e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= nk * nk) return;
   const int kh = e / nk, ke = e - kh * nk;
@@ -460,7 +538,9 @@ __global__ void mb_offp_kernel(MBView v) {
 }
 
 // X3 = X1 + 2 dt dX, written out for the relaxation (SBEs.py:5685-5687).
-__global__ void mb_x3_kernel(Step s, double2* X3) {
+__global__ void mb_x3_kernel(Step s0, MBView v0) {
+  const Step s = at_wire(s0);
+  double2* X3 = at_wire(v0).X3;
   const int n3 = 3 * s.nk * s.nk, e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= n3) return;
   X3[e] = ca(s.L2[e], rs(2.0, rs(s.prm.dt, s.dX[e])));
@@ -471,7 +551,8 @@ __global__ void mb_x3_kernel(Step s, double2* X3) {
 // 1-based grid, k3(a, b, c) = a + b - c (1-based, 0 when outside), and the
 // reference's C arrays read at [k - 1][..][..]; then MBPE / MBPH
 // (phonons.py:140-271) with Re n.  One thread per k.
-__global__ void mb_rates_kernel(MBView v) {
+__global__ void mb_rates_kernel(MBView v0) {
+  const MBView v = at_wire(v0);
   const int nk = v.nk, k0 = blockIdx.x * blockDim.x + threadIdx.x;
   if (k0 >= nk) return;
   const int n2 = nk * nk, N1 = nk + 1;
@@ -569,11 +650,39 @@ __global__ void mb_rates_kernel(MBView v) {
   v.rates[nk + k0] = woutE;
   v.rates[2 * nk + k0] = winH;
   v.rates[3 * nk + k0] = woutH;
+  if (v.mb.recomb) {
+    // SpontEmission (emission.py:94-131) from the level the right-hand side
+    // reads (SBEs.py:5237-5238): Ec (emission.py:133-172) with Re n and the
+    // screened V, Ek = gap + Ee + Eh + Ec, then SpontIntegral
+    // (emission.py:174-199): sum_n x rho0(x) square_n dhw, x = HOmega_n + Ek,
+    // rho0(x) = x^2 / (c0^3 pi^2 hbar^3)
+    const double2* C2 = v.L + n2;
+    const double2* D2 = v.L + 2 * n2;
+    const double veh0 = v.V3[0], vee0 = v.V3[nk], vhh0 = v.V3[2 * nk];
+    double s1 = 0.0, s2 = 0.0;
+    for (int i = 0; i < nk; ++i) {
+      const int d = i > k0 ? i - k0 : k0 - i;
+      const double ne = C2[i * nk + i].x, nh = D2[i * nk + i].x;
+      s1 += ne * (vee0 - v.V3[nk + d]) + nh * (vhh0 - v.V3[2 * nk + d]);
+      const double id = i == k0 ? 0.0 : 1.0;
+      s2 += ne * veh0 * id - nh * veh0 * id;
+    }
+    const double ek = ((v.gap + v.Ee[k0]) + v.Eh[k0]) + ((s1 + s2) - veh0);
+    const double* hw = v.mb.emis;
+    const double* sq = hw + v.mb.n_hw;
+    double acc = 0.0;
+    for (int n = 0; n < v.mb.n_hw; ++n) {
+      const double x = hw[n] + ek;
+      acc += x * (x * x / v.mb.rho0_den) * sq[n];
+    }
+    v.rates[4 * nk + k0] = acc * v.mb.dhw;
+  }
 }
 
 // n <- exp(-W dt) ((-1 + exp(W dt) + n) Win + n Wout) / (W + small), W = Win
 // + Wout, on the diagonal of C3 and D3 (SBEs.py:5322-5331).
-__global__ void mb_relax_kernel(MBView v, double dt) {
+__global__ void mb_relax_kernel(MBView v0, double dt) {
+  const MBView v = at_wire(v0);
   const int nk = v.nk, k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nk) return;
   const int n2 = nk * nk;
@@ -589,6 +698,95 @@ __global__ void mb_relax_kernel(MBView v, double dt) {
     const double den = W + small;
     *c = make_double2(em * s.x / den, em * s.y / den);
   }
+  if (v.mb.recomb) {
+    // n_e *= exp(-Rsp n_h dt), then n_h *= exp(-Rsp n_e dt) with the new
+    // n_e (SBEs.py:5335-5337), complex as the reference's ne3, nh3
+    const double r = v.rates[4 * nk + k];
+    double2* ce = v.X3 + n2 + k * nk + k;
+    double2* ch = v.X3 + 2 * n2 + k * nk + k;
+    auto cexp_ = [](double x, double y) {
+      const double m = exp(x);
+      return make_double2(m * cos(y), m * sin(y));
+    };
+    const double2 nh = *ch;
+    const double2 ne = cm(*ce, cexp_(-r * nh.x * dt, -r * nh.y * dt));
+    *ce = ne;
+    *ch = cm(nh, cexp_(-r * ne.x * dt, -r * ne.y * dt));
+  }
+}
+
+// DC transport (Transport, dcfield.py:1213-1247): ShiftN1D / ShiftN2D move
+// a vector or matrix in k by fft -> times exp(-i Y dk) -> ifft
+// (dcfield.py:1169-1211), i.e. a circular convolution with
+//   s[d] = (1/nk) sum_m exp(-i Y_m dk) exp(2 pi i m d / nk),
+// applied along both indices of each matrix (lf) or to its diagonal.
+__global__ void mb_shift_kernel(MBView v0) {
+  const MBView v = at_wire(v0);
+  const int nk = v.nk, d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= nk) return;
+  double re = 0.0, im = 0.0;
+  for (int m = 0; m < nk; ++m) {
+    double sy, cy, sw, cw;
+    sincos(-v.mb.Y[m] * v.mb.dc_dk, &sy, &cy);
+    const int r = (int)(((long long)m * d) % nk);
+    sincospi(2.0 * r / nk, &sw, &cw);
+    re += cy * cw - sy * sw;
+    im += cy * sw + sy * cw;
+  }
+  v.shift[d] = make_double2(re / nk, im / nk);
+}
+
+// T[x][a][j] = sum_b X3[x][a][b] s[(j - b) mod nk], one thread per (x, a, j)
+__global__ void mb_shift_rows_kernel(MBView v0) {
+  const MBView v = at_wire(v0);
+  const int nk = v.nk, n2 = nk * nk, e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= 3 * n2) return;
+  const int j = e % nk;
+  const double2* row = v.X3 + (e - j);
+  double2 acc = make_double2(0.0, 0.0);
+  for (int b = 0; b < nk; ++b) {
+    const int d = j - b < 0 ? j - b + nk : j - b;
+    acc = ca(acc, cm(row[b], v.shift[d]));
+  }
+  v.tr[e] = acc;
+}
+
+// X3[x][i][j] = sum_a s[(i - a) mod nk] T[x][a][j]
+__global__ void mb_shift_cols_kernel(MBView v0) {
+  const MBView v = at_wire(v0);
+  const int nk = v.nk, n2 = nk * nk, e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= 3 * n2) return;
+  const int x = e / n2, i = (e % n2) / nk, j = e % nk;
+  const double2* col = v.tr + (size_t)x * n2 + j;
+  double2 acc = make_double2(0.0, 0.0);
+  for (int a = 0; a < nk; ++a) {
+    const int d = i - a < 0 ? i - a + nk : i - a;
+    acc = ca(acc, cm(v.shift[d], col[(size_t)a * nk]));
+  }
+  v.X3[e] = acc;
+}
+
+// without lf only the diagonals move: T[x][a] = sum_n s[(a - n) mod nk] X3[x][n][n]
+__global__ void mb_shift_diag_kernel(MBView v0) {
+  const MBView v = at_wire(v0);
+  const int nk = v.nk, n2 = nk * nk, e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= 3 * nk) return;
+  const int x = e / nk, a = e % nk;
+  const double2* X = v.X3 + (size_t)x * n2;
+  double2 acc = make_double2(0.0, 0.0);
+  for (int n = 0; n < nk; ++n) {
+    const int d = a - n < 0 ? a - n + nk : a - n;
+    acc = ca(acc, cm(v.shift[d], X[n * nk + n]));
+  }
+  v.tr[e] = acc;
+}
+
+__global__ void mb_shift_diag_store_kernel(MBView v0) {
+  const MBView v = at_wire(v0);
+  const int nk = v.nk, e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= 3 * nk) return;
+  const int x = e / nk, a = e % nk;
+  v.X3[(size_t)x * nk * nk + a * nk + a] = v.tr[e];
 }
 
 // CalcMBArrays (coulomb.py:367-499) on the (nk+1)^3 grid the reference
@@ -641,6 +839,45 @@ __global__ void mb_tables_kernel(int nk, const double* Ee, const double* Eh, dou
   }
 }
 
+// Screening of a batch (CalcScreenedArrays, coulomb.py:1195-1230), one CTA
+// per wire: n1D from the diagonals of the level the right-hand side reads,
+// eps(q; n1D) of the grid's table block and V3 = V0 / eps.  The n1D sum
+// has psb_screen_f64's thread mapping and tree, so a wire's V3 is the same
+// bits as the one-wire path's.
+constexpr int kScrThreads = 256;
+__global__ void __launch_bounds__(kScrThreads) screen_batch_kernel(Step s0, const double* tab,
+                                                                   double L, double dens_max,
+                                                                   double* eps, double* V3) {
+  const Step s = at_wire(s0);
+  const int nk = s.nk, n2 = nk * nk;
+  const int64_t w = blockIdx.y;
+  eps = bump(eps, w * s.st_v3);
+  V3 = bump(V3, w * s.st_v3);
+  const double2* C = s.L3 + n2;
+  const double2* D = s.L3 + 2 * n2;
+  double t = 0.0;
+  for (int k = threadIdx.x; k < nk; k += kScrThreads) t += C[k * nk + k].x + D[k * nk + k].x;
+  __shared__ double red[kScrThreads / 32];
+  __shared__ double n1d_s;
+  t = warp_sum(t);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double u = 0.0;
+    for (int i = 0; i < kScrThreads / 32; ++i) u += red[i];
+    const double n1d = u / 2.0 / L;
+    n1d_s = n1d < dens_max ? n1d : dens_max;
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < nk; q += kScrThreads) {
+    const double e = eps1d(tab, nk, q, n1d_s);
+    eps[q] = e;
+    V3[q] = tab[q] / e;
+    V3[nk + q] = tab[nk + q] / e;
+    V3[2 * nk + q] = tab[2 * nk + q] / e;
+  }
+}
+
 }  // namespace full
 }  // namespace psb
 
@@ -653,8 +890,9 @@ extern "C" int64_t psb_full_work_bytes(int nk) {
 
 namespace {
 // scratch of the many-body terms: GamE, GamH, De, Dh, OffP, X3, rates
+// (+ Rsp), the DC-shift kernel and intermediate
 struct MBScratch {
-  size_t gam, de, dh, offp, x3, rates, total;
+  size_t gam, de, dh, offp, x3, rates, shift, tr, total;
   explicit MBScratch(int nk) {
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
     const size_t n = (size_t)nk, n2 = n * n, nd = (2 * n + 1) * n;
@@ -664,7 +902,9 @@ struct MBScratch {
     offp = al(dh + nd * 8);
     x3 = al(offp + n2 * 16);
     rates = al(x3 + 3 * n2 * 16);
-    total = al(rates + 4 * n * 8);
+    shift = al(rates + 5 * n * 8);
+    tr = al(shift + n * 16);
+    total = al(tr + 3 * n2 * 16);
   }
 };
 }  // namespace
@@ -688,6 +928,169 @@ extern "C" int psb_mb_tables_f64(int nk, const double* d_Ee, const double* d_Eh,
   return check_cuda("psb_mb_tables_f64");
 }
 
+namespace {
+// per-wire work of a batch: Meh, H, dX, then the screened V3 and eps
+struct BatchWork {
+  size_t v3, eps, total;
+  explicit BatchWork(int nk) {
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    v3 = al((size_t)7 * nk * nk * 16);
+    eps = al(v3 + 3 * (size_t)nk * 8);
+    total = al(eps + (size_t)nk * 8);
+  }
+};
+
+// one full-matrix step of nw wires of one grid (nw = 1: the one-wire entry)
+struct Launch {
+  int nw, nk, nr, nq0;
+  const double* V3;
+  int64_t st_v3;         // bytes between wires' V3 (0: shared)
+  const double* Ee;
+  const double* Eh;
+  const double* fields;  // [nw][3][nr] complex
+  const PsbFullParams* params;
+  const double* wpar;    // [nw][4] or null
+  const PsbFullMB* mb;
+  double* L1;
+  double* L2;
+  double* L3;
+  void* work;
+  int64_t st_wk;         // bytes between wires' work
+  const double* tab;     // screened batch: the grid's table block, else null
+  double L, dens_max;
+};
+
+int check_mb(const PsbFullMB* mb, bool deph, bool relax, bool dct) {
+  if (!(deph || relax || dct)) return PSB_OK;
+  if (!mb->scratch) return set_error(PSB_ERR_INVALID, "PsbFullMB.scratch is null");
+  if (mb->diag_dph && (!mb->maps || !mb->iq || !mb->xe || !mb->xh))
+    return set_error(PSB_ERR_INVALID, "PsbFullMB: dephasing tables missing");
+  if ((mb->ehs && !mb->C) || (mb->phonon && !mb->ph))
+    return set_error(PSB_ERR_INVALID, "PsbFullMB: relaxation tables missing");
+  if (relax && mb->recomb && (!mb->emis || mb->n_hw < 2 || !(mb->rho0_den > 0.0)))
+    return set_error(PSB_ERR_INVALID, "PsbFullMB: emission tables missing");
+  if (dct && !mb->Y) return set_error(PSB_ERR_INVALID, "PsbFullMB: DC wavenumbers missing");
+  return PSB_OK;
+}
+
+int full_launch(const Launch& a, cudaStream_t st) {
+  const int nk = a.nk, nw = a.nw, n2 = nk * nk;
+  const PsbFullMB* mb = a.mb;
+  const bool deph = mb && (mb->diag_dph || mb->offdiag_dph);
+  const bool relax = mb && (mb->ehs || mb->phonon);
+  const bool dct = mb && mb->dctrans;
+  const int rc = check_mb(mb, deph, relax, dct);
+  if (rc != PSB_OK) return rc;
+  full::Step s{};
+  s.nk = nk;
+  s.nr = a.nr;
+  s.nq0 = a.nq0;
+  s.V3 = a.V3;
+  s.Ee = a.Ee;
+  s.Eh = a.Eh;
+  s.E = reinterpret_cast<const double2*>(a.fields);
+  s.prm = *a.params;
+  s.L1 = reinterpret_cast<double2*>(a.L1);
+  s.L2 = reinterpret_cast<double2*>(a.L2);
+  s.L3 = reinterpret_cast<double2*>(a.L3);
+  double2* w = reinterpret_cast<double2*>(a.work);
+  s.Meh = w;
+  s.H = w + n2;
+  s.dX = w + 4 * n2;
+  s.st_v3 = a.st_v3;
+  s.st_e = (int64_t)3 * a.nr * 16;
+  s.st_lv = (int64_t)3 * n2 * 16;
+  s.st_wk = a.st_wk;
+  s.st_sc = (int64_t)MBScratch(nk).total;
+  s.wpar = a.wpar;
+  const dim3 one(1, nw);
+  const double* eps = mb ? mb->eps : nullptr;
+  int64_t st_eps = 0;
+  if (a.tab) {
+    // each wire's V3 and eps from its own densities, into its work
+    const BatchWork bw(nk);
+    double* v3w = reinterpret_cast<double*>(reinterpret_cast<uint8_t*>(a.work) + bw.v3);
+    double* epsw = reinterpret_cast<double*>(reinterpret_cast<uint8_t*>(a.work) + bw.eps);
+    s.V3 = v3w;
+    s.st_v3 = a.st_wk;
+    full::screen_batch_kernel<<<one, full::kScrThreads, 0, st>>>(s, a.tab, a.L, a.dens_max,
+                                                                  epsw, v3w);
+    eps = epsw;
+    st_eps = a.st_wk;
+  }
+  full::MBView v{};
+  if (deph || relax || dct) {
+    const MBScratch L(nk);
+    uint8_t* sc = reinterpret_cast<uint8_t*>(mb->scratch);
+    v.nk = nk;
+    v.V3 = s.V3;
+    v.Ee = a.Ee;
+    v.Eh = a.Eh;
+    v.L = s.L3;
+    v.hbar = a.params->hbar;
+    v.mb = *mb;
+    v.mb.eps = eps;
+    v.GamE = reinterpret_cast<double*>(sc + L.gam);
+    v.GamH = v.GamE + nk;
+    v.De = reinterpret_cast<double*>(sc + L.de);
+    v.Dh = reinterpret_cast<double*>(sc + L.dh);
+    v.OffP = reinterpret_cast<double2*>(sc + L.offp);
+    v.X3 = reinterpret_cast<double2*>(sc + L.x3);
+    v.rates = reinterpret_cast<double*>(sc + L.rates);
+    v.shift = reinterpret_cast<double2*>(sc + L.shift);
+    v.tr = reinterpret_cast<double2*>(sc + L.tr);
+    v.gap = a.params->gap;
+    v.lf = a.params->lf;
+    v.st_v3 = s.st_v3;
+    v.st_lv = s.st_lv;
+    v.st_sc = s.st_sc;
+    v.st_eps = st_eps;
+    v.wpar = a.wpar;
+  }
+  const int th = 128;
+  const dim3 bl((n2 + th - 1) / th, nw), blk((nk + th - 1) / th, nw);
+  full::meh_kernel<<<bl, th, 0, st>>>(s);
+  full::calch_kernel<<<bl, th, 0, st>>>(s);
+  // dephasing from the level the right-hand side reads (SBEs.py:5225-5232)
+  if (mb && mb->diag_dph) {
+    full::mb_gamma_kernel<<<blk, th, 0, st>>>(v);
+    s.GamE = v.GamE;
+    s.GamH = v.GamH;
+  }
+  if (mb && mb->offdiag_dph) {
+    const int nd = (2 * nk + 1) * nk;
+    full::mb_offd_kernel<<<dim3((nd + th - 1) / th, nw), th, 0, st>>>(v);
+    full::mb_offp_kernel<<<bl, th, 0, st>>>(v);
+    s.OffP = v.OffP;
+  }
+  full::derivs_kernel<<<bl, th, 0, st>>>(s);
+  if (relax || dct) {
+    // X3, its occupations relaxed (SBEs.py:5688-5695) and shifted by the DC
+    // field (SBEs.py:5698-5702), then the rescale
+    const dim3 b3((3 * n2 + th - 1) / th, nw);
+    full::mb_x3_kernel<<<b3, th, 0, st>>>(s, v);
+    if (relax) {
+      full::mb_rates_kernel<<<blk, th, 0, st>>>(v);
+      full::mb_relax_kernel<<<blk, th, 0, st>>>(v, a.params->dt);
+    }
+    if (dct) {
+      full::mb_shift_kernel<<<blk, th, 0, st>>>(v);
+      if (a.params->lf) {
+        full::mb_shift_rows_kernel<<<b3, th, 0, st>>>(v);
+        full::mb_shift_cols_kernel<<<b3, th, 0, st>>>(v);
+      } else {
+        const dim3 bd((3 * nk + th - 1) / th, nw);
+        full::mb_shift_diag_kernel<<<bd, th, 0, st>>>(v);
+        full::mb_shift_diag_store_kernel<<<bd, th, 0, st>>>(v);
+      }
+    }
+    s.X3 = v.X3;
+  }
+  full::leapfrog_kernel<<<one, full::kLfThreads, 0, st>>>(s);
+  return PSB_OK;
+}
+}  // namespace
+
 extern "C" int psb_full_step_mb_f64(int nk, int nr, int nq0, const double* d_V3,
                                     const double* d_Ee, const double* d_Eh,
                                     const double* d_fields, const PsbFullParams* params,
@@ -702,76 +1105,23 @@ extern "C" int psb_full_step_mb_f64(int nk, int nr, int nq0, const double* d_V3,
   if (n_work_bytes < psb_full_work_bytes(nk))
     return set_error(PSB_ERR_SIZE, "psb_full_step_f64: work needs psb_full_work_bytes(nk)");
   if (!(params->hbar > 0.0)) return set_error(PSB_ERR_INVALID, "hbar must be > 0");
-  const bool deph = mb && (mb->diag_dph || mb->offdiag_dph);
-  const bool relax = mb && (mb->ehs || mb->phonon);
-  if (mb && (deph || relax)) {
-    if (!mb->scratch) return set_error(PSB_ERR_INVALID, "PsbFullMB.scratch is null");
-    if (mb->diag_dph && (!mb->maps || !mb->iq || !mb->xe || !mb->xh))
-      return set_error(PSB_ERR_INVALID, "PsbFullMB: dephasing tables missing");
-    if ((mb->ehs && !mb->C) || (mb->phonon && !mb->ph))
-      return set_error(PSB_ERR_INVALID, "PsbFullMB: relaxation tables missing");
-  }
-  full::Step s{};
-  s.nk = nk;
-  s.nr = nr;
-  s.nq0 = nq0;
-  s.V3 = d_V3;
-  s.Ee = d_Ee;
-  s.Eh = d_Eh;
-  s.E = reinterpret_cast<const double2*>(d_fields);
-  s.prm = *params;
-  s.L1 = reinterpret_cast<double2*>(d_L1);
-  s.L2 = reinterpret_cast<double2*>(d_L2);
-  s.L3 = reinterpret_cast<double2*>(d_L3);
-  double2* w = reinterpret_cast<double2*>(d_work);
-  const int n2 = nk * nk;
-  s.Meh = w;
-  s.H = w + n2;
-  s.dX = w + 4 * n2;
-  full::MBView v{};
-  if (deph || relax) {
-    const MBScratch L(nk);
-    uint8_t* sc = reinterpret_cast<uint8_t*>(mb->scratch);
-    v.nk = nk;
-    v.V3 = d_V3;
-    v.Ee = d_Ee;
-    v.Eh = d_Eh;
-    v.L = s.L3;
-    v.hbar = params->hbar;
-    v.mb = *mb;
-    v.GamE = reinterpret_cast<double*>(sc + L.gam);
-    v.GamH = v.GamE + nk;
-    v.De = reinterpret_cast<double*>(sc + L.de);
-    v.Dh = reinterpret_cast<double*>(sc + L.dh);
-    v.OffP = reinterpret_cast<double2*>(sc + L.offp);
-    v.X3 = reinterpret_cast<double2*>(sc + L.x3);
-    v.rates = reinterpret_cast<double*>(sc + L.rates);
-  }
-  cudaStream_t st = (cudaStream_t)stream;
-  const int th = 128, bl = (n2 + th - 1) / th, blk = (nk + th - 1) / th;
-  full::meh_kernel<<<bl, th, 0, st>>>(s);
-  full::calch_kernel<<<bl, th, 0, st>>>(s);
-  // dephasing from the level the right-hand side reads (SBEs.py:5225-5232)
-  if (mb && mb->diag_dph) {
-    full::mb_gamma_kernel<<<blk, th, 0, st>>>(v);
-    s.GamE = v.GamE;
-    s.GamH = v.GamH;
-  }
-  if (mb && mb->offdiag_dph) {
-    const int nd = (2 * nk + 1) * nk;
-    full::mb_offd_kernel<<<(nd + th - 1) / th, th, 0, st>>>(v);
-    full::mb_offp_kernel<<<bl, th, 0, st>>>(v);
-    s.OffP = v.OffP;
-  }
-  full::derivs_kernel<<<bl, th, 0, st>>>(s);
-  if (relax) {
-    // X3, its occupations relaxed (SBEs.py:5688-5695), then the rescale
-    full::mb_x3_kernel<<<(3 * n2 + th - 1) / th, th, 0, st>>>(s, v.X3);
-    full::mb_rates_kernel<<<blk, th, 0, st>>>(v);
-    full::mb_relax_kernel<<<blk, th, 0, st>>>(v, params->dt);
-    s.X3 = v.X3;
-  }
-  full::leapfrog_kernel<<<1, full::kLfThreads, 0, st>>>(s);
+  Launch a{};
+  a.nw = 1;
+  a.nk = nk;
+  a.nr = nr;
+  a.nq0 = nq0;
+  a.V3 = d_V3;
+  a.Ee = d_Ee;
+  a.Eh = d_Eh;
+  a.fields = d_fields;
+  a.params = params;
+  a.mb = mb;
+  a.L1 = d_L1;
+  a.L2 = d_L2;
+  a.L3 = d_L3;
+  a.work = d_work;
+  const int rc = full_launch(a, (cudaStream_t)stream);
+  if (rc != PSB_OK) return rc;
   return check_cuda("psb_full_step_f64");
 }
 
@@ -784,6 +1134,56 @@ extern "C" int psb_full_step_f64(int nk, int nr, int nq0, const double* d_V3, co
                               d_L2, d_L3, d_work, n_work_bytes, stream);
 }
 
+extern "C" int64_t psb_full_batch_work_bytes(int nw, int nk) {
+  if (nk < 2 || nk > PSB_MAX_NK) return set_error(PSB_ERR_SIZE, "nk %d out of range", nk);
+  if (nw < 1 || nw > PSB_FULL_MAX_WIRES) return set_error(PSB_ERR_SIZE, "nw %d out of range", nw);
+  return (int64_t)nw * (int64_t)BatchWork(nk).total;
+}
+
+extern "C" int psb_full_step_batch_f64(int nw, int nk, int nr, int nq0, const double* d_tab,
+                                       double L, double dens_max, int screened,
+                                       const double* d_fields, const PsbFullParams* params,
+                                       const double* d_wpar, const PsbFullMB* mb, double* d_L1,
+                                       double* d_L2, double* d_L3, void* d_work,
+                                       int64_t n_work_bytes, void* stream) {
+  if (!d_tab || !d_fields || !params || !d_wpar || !d_L1 || !d_L2 || !d_L3 || !d_work)
+    return set_error(PSB_ERR_INVALID, "psb_full_step_batch_f64: null pointer");
+  if (nk < 2 || nk > PSB_MAX_NK || nr < 1 || nq0 < 0 || nq0 >= nr || nw < 1 ||
+      nw > PSB_FULL_MAX_WIRES)
+    return set_error(PSB_ERR_SIZE, "psb_full_step_batch_f64: nw %d / nk %d / nr %d / nq0 %d", nw,
+                     nk, nr, nq0);
+  if (n_work_bytes < psb_full_batch_work_bytes(nw, nk))
+    return set_error(PSB_ERR_SIZE, "psb_full_step_batch_f64: work needs "
+                                   "psb_full_batch_work_bytes(nw, nk)");
+  if (!(params->hbar > 0.0)) return set_error(PSB_ERR_INVALID, "hbar must be > 0");
+  if (screened && !(L > 0.0)) return set_error(PSB_ERR_INVALID, "screening needs L > 0");
+  Launch a{};
+  a.nw = nw;
+  a.nk = nk;
+  a.nr = nr;
+  a.nq0 = nq0;
+  a.V3 = d_tab;  // V_eh, V_ee, V_hh rows of the table block, shared when unscreened
+  a.Ee = d_tab + 3 * (size_t)nk;
+  a.Eh = d_tab + 4 * (size_t)nk;
+  a.fields = d_fields;
+  a.params = params;
+  a.wpar = d_wpar;
+  a.mb = mb;
+  a.L1 = d_L1;
+  a.L2 = d_L2;
+  a.L3 = d_L3;
+  a.work = d_work;
+  a.st_wk = (int64_t)BatchWork(nk).total;
+  if (screened) {
+    a.tab = d_tab;
+    a.L = L;
+    a.dens_max = dens_max;
+  }
+  const int rc = full_launch(a, (cudaStream_t)stream);
+  if (rc != PSB_OK) return rc;
+  return check_cuda("psb_full_step_batch_f64");
+}
+
 extern "C" int psb_full_sources_f64(int nk, int nr, const double* d_kr, const double* d_r,
                                     const double* d_window, double L, double dcv, double yw,
                                     double sgnw, const double* d_level, double* d_out,
@@ -794,7 +1194,24 @@ extern "C" int psb_full_sources_f64(int nk, int nr, const double* d_kr, const do
     return set_error(PSB_ERR_SIZE, "psb_full_sources_f64: nk %d / nr %d out of range", nk, nr);
   const int th = 64, bl = (nr + th - 1) / th;
   full::sources_kernel<<<bl, th, 0, (cudaStream_t)stream>>>(
-      nk, nr, d_kr, d_r, d_window, L, dcv, yw, sgnw,
+      nk, nr, d_kr, d_r, d_window, L, dcv, yw, sgnw, nullptr,
       reinterpret_cast<const double2*>(d_level), reinterpret_cast<double2*>(d_out));
   return check_cuda("psb_full_sources_f64");
+}
+
+extern "C" int psb_full_sources_batch_f64(int nw, int nk, int nr, const double* d_kr,
+                                          const double* d_r, const double* d_window, double L,
+                                          double dcv, const double* d_wpar,
+                                          const double* d_levels, double* d_out, void* stream) {
+  if (!d_kr || !d_r || !d_window || !d_wpar || !d_levels || !d_out)
+    return set_error(PSB_ERR_INVALID, "psb_full_sources_batch_f64: null pointer");
+  if (nk < 2 || nk > PSB_MAX_NK || nr < 1 || nw < 1 || nw > PSB_FULL_MAX_WIRES)
+    return set_error(PSB_ERR_SIZE, "psb_full_sources_batch_f64: nw %d / nk %d / nr %d", nw, nk,
+                     nr);
+  const int th = 64;
+  const dim3 bl((nr + th - 1) / th, nw);
+  full::sources_kernel<<<bl, th, 0, (cudaStream_t)stream>>>(
+      nk, nr, d_kr, d_r, d_window, L, dcv, 0.0, 0.0, d_wpar,
+      reinterpret_cast<const double2*>(d_levels), reinterpret_cast<double2*>(d_out));
+  return check_cuda("psb_full_sources_batch_f64");
 }

@@ -433,7 +433,13 @@ def make_solver_api(R, out, name="solver_lf_nk32", L=2.85e-8, nsteps=300, dt=10e
 MB_PARAMS_FULL = "1\n1\n0\n{scr}\n0\n0\n1\n0\n0\n0\n0\n0\n0\n0\n0\n"
 
 
-def make_qwcalculator(R, out, name, L=2.85e-8, screened=True, nsteps=200, dt=10e-18, mb=None):
+def with_edc(params, edc):
+    """qw.params text with the DC field line set to edc (V/m)."""
+    return params.replace("0.0        # Edc", f"{edc!r}        # Edc")
+
+
+def make_qwcalculator(R, out, name, L=2.85e-8, screened=True, nsteps=200, dt=10e-18, mb=None,
+                      edc=0.0):
     """The reference's QWCalculator as its PSTD caller drives it (rhoPJ.py:311-348):
     propagation-space fields along the wire axis (a Gaussian profile, so the
     windowed wire field has every q component and the state is full-matrix),
@@ -444,7 +450,7 @@ def make_qwcalculator(R, out, name, L=2.85e-8, screened=True, nsteps=200, dt=10e
     os.makedirs(os.path.join(run, "params"))
     gam = 5e12
     with open(os.path.join(run, "params", "qw.params"), "w") as f:
-        f.write(QW_PARAMS.format(L=L, gam=gam))
+        f.write(with_edc(QW_PARAMS.format(L=L, gam=gam), edc))
     with open(os.path.join(run, "params", "mb.params"), "w") as f:
         f.write(mb if mb is not None else MB_PARAMS_FULL.format(scr=1 if screened else 0))
     os.chdir(run)
@@ -477,7 +483,7 @@ def make_qwcalculator(R, out, name, L=2.85e-8, screened=True, nsteps=200, dt=10e
         el = time.time() - t_start
         lv = {f"{a}{i}": getattr(s, f"{a}{i}").copy() for a in ("YY", "CC", "DD") for i in (1, 2, 3)}
         np.savez_compressed(os.path.join(out, f"{name}.npz"), nk=nk, nr=s.Nr, L=L, gam=gam,
-                            dt=dt, nsteps=nsteps, rr=rr, prof=prof, env=env,
+                            dt=dt, nsteps=nsteps, rr=rr, prof=prof, env=env, edc=edc,
                             screened=screened, seconds=el, **outs, **lv)
         print(f"{name}: Nk={nk}, {nsteps} steps x 2 wires in {el:.1f} s, "
               f"max|Pyy| = {np.max(np.abs(outs['Pyy'])):.3e}, "
@@ -486,7 +492,12 @@ def make_qwcalculator(R, out, name, L=2.85e-8, screened=True, nsteps=200, dt=10e
         os.chdir(cwd)
 
 
-MB_PARAMS_MB = "1\n1\n{ehs}\n{scr}\n{ph}\n0\n1\n0\n{dd}\n{od}\n0\n0\n0\n0\n{lor}\n"
+MB_PARAMS_MB = ("1\n1\n{ehs}\n{scr}\n{ph}\n{dc}\n{lf}\n0\n{dd}\n{od}\n{rc}\n0\n0\n0\n{lor}\n")
+
+
+def mb_params(ehs=1, scr=0, ph=1, dc=0, lf=1, dd=1, od=1, rc=0, lor=0):
+    """mb.params text: Optics, Excitons on; the many-body flags as given."""
+    return MB_PARAMS_MB.format(ehs=ehs, scr=scr, ph=ph, dc=dc, lf=lf, dd=dd, od=od, rc=rc, lor=lor)
 
 
 def _run_dir(prefix, L, gam, mb):
@@ -501,15 +512,17 @@ def _run_dir(prefix, L, gam, mb):
 
 def make_manybody_units(R, out, L=2.85e-8, gam=5e12):
     """The reference's many-body functions (CalcGammaE/H, CalcOffDiagDeph_E2
-    /H2, OffDiagDephasing2, MBCE/MBCH, MBPE/MBPH) on random levels of its own
-    grid, unscreened, Lorentzian delta: the inputs one full-matrix step reads
-    (X1 = level 2, X2 = level 3 of the GPU state, dt = 0) and its outputs."""
+    /H2, OffDiagDephasing2, MBCE/MBCH, MBPE/MBPH, SpontEmission) on random
+    levels of its own grid, unscreened, Lorentzian delta: the inputs one
+    full-matrix step reads (X1 = level 2, X2 = level 3 of the GPU state,
+    dt = 0) and its outputs."""
     from pulsesuite.PSTD3D import coulomb as C
     from pulsesuite.PSTD3D import dephasing as D
+    from pulsesuite.PSTD3D import emission as EM
     from pulsesuite.PSTD3D import phonons as P
 
     cwd = os.getcwd()
-    run = _run_dir("mbu_", L, gam, MB_PARAMS_MB.format(ehs=1, scr=0, ph=1, dd=1, od=1, lor=1))
+    run = _run_dir("mbu_", L, gam, mb_params(rc=1, lor=1))
     os.chdir(run)
     try:
         rr = np.linspace(-5e-8, 5e-8, 64)
@@ -546,12 +559,19 @@ def make_manybody_units(R, out, L=2.85e-8, gam=5e12):
         P.MBPE(ne3, VC, E1D, WinE, WoutE)
         C.MBCH(ne3, nh3, s.kr, s.Ee, s.Eh, VC, s.gam_eh, s.gam_h, WinH, WoutH)
         P.MBPH(nh3, VC, E1D, WinH, WoutH)
+        Rsp = np.zeros(nk)
+        EM.SpontEmission(ne2, nh2, s.Ee, s.Eh, s.gap, s.gam_eh, VC, Rsp)
+        from pulsesuite.PSTD3D import dcfield as DC
+        # host tables of InitializeEmission / InitializeDC and their inputs
+        host = dict(kr=s.kr, dcv=s.dcv, epsr=s.epsr, gam_eh=s.gam_eh, ehint=s.ehint,
+                    HOmega=EM._HOmega, square=EM._square, Ydc=DC._instance.Y)
         np.savez_compressed(os.path.join(out, "manybody_units_nk32.npz"), nk=nk, L=L, gam=gam,
                             p1=p1, c1=c1, d1=d1, p2=p2, c2=c2, d2=d2, GamE=GamE, GamH=GamH,
                             De=De, Dh=Dh, OffP=OffP, WinE=WinE, WoutE=WoutE, WinH=WinH,
-                            WoutH=WoutH)
+                            WoutH=WoutH, Rsp=Rsp, **host)
         print(f"manybody units: Nk={nk}, |GamE| {np.max(np.abs(GamE)):.3e}, |OffP| "
-              f"{np.max(np.abs(OffP)):.3e}, |WinE| {np.max(np.abs(WinE)):.3e}")
+              f"{np.max(np.abs(OffP)):.3e}, |WinE| {np.max(np.abs(WinE)):.3e}, "
+              f"|Rsp| {np.max(np.abs(Rsp)):.3e}")
     finally:
         os.chdir(cwd)
 
@@ -611,7 +631,14 @@ def main():
     if want("manybody"):
         make_manybody_units(R, out)
         make_qwcalculator(R, out, "qwcalc_manybody_nk32", screened=True, nsteps=120,
-                          mb=MB_PARAMS_MB.format(ehs=1, scr=1, ph=1, dd=1, od=1, lor=0))
+                          mb=mb_params(scr=1))
+    if want("transport"):
+        # all six many-body flags with a DC field: the whole matrices shifted
+        # (LF) or their diagonals only
+        for lf in (1, 0):
+            make_qwcalculator(R, out, f"qwcalc_mb_dc_{'lf' if lf else 'diag'}_nk32",
+                              screened=True, nsteps=120, edc=2e6,
+                              mb=mb_params(scr=1, dc=1, rc=1, lf=lf))
     if a.full_c0:
         make_rk4(R, out, "rk4_c0_nk128_full", rwa_case(128, 4000))
 

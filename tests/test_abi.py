@@ -54,8 +54,9 @@ int main(void) {
   printf("%zu %zu\n", offsetof(PsbTable, L), offsetof(PsbTable, dens_max));
   printf("%zu %zu %zu\n", sizeof(PsbFullParams), offsetof(PsbFullParams, dt),
          offsetof(PsbFullParams, lf));
-  printf("%zu %zu %zu %zu\n", sizeof(PsbFullMB), offsetof(PsbFullMB, vscale),
-         offsetof(PsbFullMB, maps), offsetof(PsbFullMB, scratch));
+  printf("%zu %zu %zu %zu %zu %zu %zu\n", sizeof(PsbFullMB), offsetof(PsbFullMB, vscale),
+         offsetof(PsbFullMB, maps), offsetof(PsbFullMB, scratch), offsetof(PsbFullMB, dc_dk),
+         offsetof(PsbFullMB, n_hw), offsetof(PsbFullMB, Y));
   return 0;
 }
 '''
@@ -75,5 +76,5 @@ int main(void) {
     F = abi.FULL_PARAMS_DTYPE
     assert vals[11:14] == [F.itemsize, F.fields["dt"][1], F.fields["lf"][1]]
     M = abi.FULL_MB_DTYPE
-    assert vals[14:] == [M.itemsize, M.fields["vscale"][1], M.fields["maps"][1],
-                         M.fields["scratch"][1]]
+    assert vals[14:] == [M.itemsize] + [M.fields[f][1] for f in ("vscale", "maps", "scratch",
+                                                                  "dc_dk", "n_hw", "Y")]

@@ -1,18 +1,20 @@
 """GPU parity of the many-body terms of the full-matrix step
 (psb_full_step_mb_f64, switched on by mb.params DiagDph, OffDiagDph, EHs,
-Phonon) against outputs of the reference itself (tests/golden, generated by
-importing the reference):
+Phonon, Recomb, DCTrans) against outputs of the reference itself
+(tests/golden, generated by importing the reference):
 
   * units: on random levels of the reference's own grid, one step (dt = 0,
     so the new level equals the old one) leaves in its scratch the
     k-dependent dephasing rates (CalcGammaE / CalcGammaH), the off-diagonal
     dephasing kernels and term (CalcOffDiagDeph_E2 / _H2,
-    OffDiagDephasing2) and the in/out scattering rates (MBCE + MBPE,
-    MBCH + MBPH, Lorentzian delta) of the reference's functions on the
-    same inputs;
-  * solver: QWCalculator with all four flags, screened, LF, fields along
-    the wire (Gaussian delta): every step's Pxx, Pyy, Pzz, Rho and the
-    final nine levels match the reference's run.
+    OffDiagDephasing2), the in/out scattering rates (MBCE + MBPE,
+    MBCH + MBPH, Lorentzian delta) and the spontaneous-emission rates
+    (SpontEmission) of the reference's functions on the same inputs;
+  * solver: QWCalculator with DiagDph, OffDiagDph, EHs, Phonon, screened,
+    LF, fields along the wire (Gaussian delta), and the same with Recomb and
+    DCTrans in a DC field, with LF (whole matrices shifted) and without
+    (diagonals shifted): every step's Pxx, Pyy, Pzz, Rho and the final nine
+    levels match the reference's run.
 
 Tolerance 1e-10 normwise (measured ~1e-13 and below).
 """
@@ -31,13 +33,17 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-10
 # Optics Excitons EHs Screened Phonon DCTrans LF FreePot DiagDph OffDiagDph
 # Recomb PLSpec ignorewire Xqwparams LorentzDelta
-MB = "1\n1\n1\n{scr}\n1\n0\n1\n0\n1\n1\n0\n0\n0\n0\n{lor}\n"
+MB = "1\n1\n1\n{scr}\n1\n{dc}\n{lf}\n0\n1\n1\n{rc}\n0\n0\n0\n{lor}\n"
 
 
-def make_solver(tmp_path, L, gam, screened, lorentz, nw=1):
+def make_solver(tmp_path, L, gam, screened, lorentz, nw=1, recomb=False, dctrans=False, lf=True,
+                edc=0.0):
     os.makedirs(tmp_path / "params", exist_ok=True)
-    (tmp_path / "params" / "qw.params").write_text(QW_PARAMS.format(L=L, gam=gam))
-    (tmp_path / "params" / "mb.params").write_text(MB.format(scr=int(screened), lor=int(lorentz)))
+    qw = QW_PARAMS.format(L=L, gam=gam).replace("0.0        # Edc", f"{edc!r}        # Edc")
+    (tmp_path / "params" / "qw.params").write_text(qw)
+    (tmp_path / "params" / "mb.params").write_text(
+        MB.format(scr=int(screened), lor=int(lorentz), rc=int(recomb), dc=int(dctrans),
+                  lf=int(lf)))
     cwd = os.getcwd()
     os.chdir(tmp_path)
     try:
@@ -48,7 +54,7 @@ def make_solver(tmp_path, L, gam, screened, lorentz, nw=1):
 
 
 def scratch_views(scratch, nk):
-    """GamE, GamH, De, Dh, OffP, rates in psb_full_step_mb_f64's scratch
+    """GamE, GamH, De, Dh, OffP, rates (+ Rsp) in psb_full_step_mb_f64's scratch
     (layout of its MBScratch: 256-byte aligned blocks in this order)."""
     def al(x):
         return (x + 255) // 256 * 256
@@ -64,12 +70,13 @@ def scratch_views(scratch, nk):
     return {"GamE": f64(0, nk), "GamH": f64(8 * nk, nk),
             "De": f64(de, nd).reshape(2 * nk + 1, nk), "Dh": f64(dh, nd).reshape(2 * nk + 1, nk),
             "OffP": b[offp:offp + 16 * n2].view(np.complex128).reshape(nk, nk),
-            "rates": f64(rates, 4 * nk).reshape(4, nk)}
+            "rates": f64(rates, 5 * nk).reshape(5, nk)}
 
 
 def test_manybody_terms_match_reference_functions(cuda, tmp_path):
     d = golden("manybody_units_nk32")
-    s = make_solver(tmp_path, float(d["L"]), float(d["gam"]), screened=False, lorentz=True)
+    s = make_solver(tmp_path, float(d["L"]), float(d["gam"]), screened=False, lorentz=True,
+                    recomb=True)
     nk = s.Nk
     assert nk == int(d["nk"])
     s._enter_full()
@@ -84,14 +91,18 @@ def test_manybody_terms_match_reference_functions(cuda, tmp_path):
     v = scratch_views(F["mb"].scratch, nk)
     for k in ("GamE", "GamH", "De", "Dh", "OffP"):
         assert relerr(v[k], d[k]) < TOL, (k, relerr(v[k], d[k]))
-    for i, k in enumerate(("WinE", "WoutE", "WinH", "WoutH")):
+    for i, k in enumerate(("WinE", "WoutE", "WinH", "WoutH", "Rsp")):
         assert relerr(v["rates"][i], d[k]) < TOL, (k, relerr(v["rates"][i], d[k]))
 
 
-def test_qwcalculator_many_body_matches_reference(cuda, tmp_path):
-    d = golden("qwcalc_manybody_nk32")
+@pytest.mark.parametrize("name", ["qwcalc_manybody_nk32", "qwcalc_mb_dc_lf_nk32",
+                                  "qwcalc_mb_dc_diag_nk32"])
+def test_qwcalculator_many_body_matches_reference(cuda, tmp_path, name):
+    d = golden(name)
+    dc = name.startswith("qwcalc_mb_dc")
     s = make_solver(tmp_path, float(d["L"]), float(d["gam"]), screened=True, lorentz=False,
-                    nw=2)
+                    nw=2, recomb=dc, dctrans=dc, lf=not name.endswith("diag_nk32"),
+                    edc=float(d["edc"]) if "edc" in d else 0.0)
     rr, prof = d["rr"], d["prof"]
     n, nrr = int(d["nsteps"]), rr.size
     got = {k: np.zeros((n, 2, nrr), complex) for k in ("Pxx", "Pyy", "Pzz", "Rho")}
