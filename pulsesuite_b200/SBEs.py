@@ -578,8 +578,8 @@ class SBESolver:
         """One step of wires w0 + 1 .. Nw (1-based) on the full state in one
         launch set (psb_full_step_batch_f64, psb_full_sources_batch_f64);
         fields [n][3][Nr] complex wire-space Ex, Ey, Ez.  Returns the five
-        source arrays (Px, Py, Pz, Re, Rh) of each wire, as _full_step writes
-        them."""
+        sources (Px, Py, Pz, Re, Rh) of each wire, [n][5][Nr], as _full_step
+        writes them."""
         import torch
 
         from . import device as _dev
@@ -618,7 +618,7 @@ class SBESolver:
                   float(t0["L"]), float(t0["dens_max"]), int(self.Screened), _dev.ptr(fd),
                   abi.as_ptr(prm), _dev.ptr(wpd), mbd, _dev.ptr(L1), _dev.ptr(L2),
                   _dev.ptr(L3), _dev.ptr(F["bwork"]), F["bwork"].numel(), _dev.stream_ptr())
-        srcs = [[np.zeros(self.Nr, np.complex128) for _ in range(5)] for _ in range(n)]
+        srcs = np.zeros((n, 5, self.Nr), np.complex128)
         if not (self.Optics or self.LF):
             return srcs
         out = F["bout"][:n]
@@ -626,13 +626,21 @@ class SBESolver:
                   _dev.ptr(F["r"]), _dev.ptr(F["window"]), float(self.L), float(self.dcv),
                   _dev.ptr(wpd), _dev.ptr(L3), _dev.ptr(out), _dev.stream_ptr())
         out = out.cpu().numpy()
-        diag = None
+        if self.Optics:
+            # QWPolarization3's factor and transform, all wires at once
+            P = out[:, :3] * 2 * self.ehint / self.area / self.L   # contiguous [n][3][Nr]
+            wirespace.fftg(P.reshape(3 * n, self.Nr))
+            srcs[:, :3] = P
         if self.LF:
             diag = torch.diagonal(L3[:, 1:3], dim1=-2, dim2=-1).cpu().numpy()  # [n][2][nk]
-        for i in range(n):
-            c3 = diag[i, 0] if diag is not None else None
-            d3 = diag[i, 1] if diag is not None else None
-            self._full_sources_post(out[i], c3, d3, *srcs[i])
+            dr = self.r[1] - self.r[0]
+            for i in range(n):
+                Re, Rh = srcs[i, 3], srcs[i, 4]
+                Re[:] = out[i, 3]
+                Rh[:] = out[i, 4]
+                wirespace.rho_post(Re, Rh, diag[i, 0], diag[i, 1], dr)
+                Re[:] = 2.0 * _e0 * Re / self.area * self.ehint
+                Rh[:] = 2.0 * _e0 * Rh / self.area * self.ehint
         return srcs
 
     def _drive(self, Ex, Ey, Ez):
@@ -792,29 +800,35 @@ class SBESolver:
         self.wireoff = False
         DoQWP[0] = self.Optics
         DoQWDl[0] = self.LF
-        wf = [wirespace.prop2qw(rr, col(Exx, w), col(Eyy, w), col(Ezz, w), col(Vrr, w), self.r,
-                                self.window) for w in range(w0, nw)]
+        n = nw - w0
+        # Prop2QW of every wire's four fields in one pass (once when all
+        # wires see the same field)
+        if all(np.asarray(a).ndim == 1 for a in (Exx, Eyy, Ezz, Vrr)):
+            f1 = wirespace.prop2qw_rows(rr, np.stack([np.asarray(a, np.complex128) for a in
+                                                      (Exx, Eyy, Ezz, Vrr)]), self.r, self.window)
+            wf = np.broadcast_to(f1, (n,) + f1.shape)
+        else:
+            F = np.stack([np.stack([np.asarray(col(a, w), np.complex128)
+                                    for a in (Exx, Eyy, Ezz, Vrr)]) for w in range(w0, nw)])
+            wf = wirespace.prop2qw_rows(rr, F.reshape(4 * n, -1), self.r,
+                                        self.window).reshape(n, 4, -1)
         if self.full is None and not self._many_body and all(
                 self._is_diagonal(f[0], f[1], f[2]) for f in wf):
             # fields only at q = 0: the diagonal kernel, wire by wire
-            srcs = []
+            srcs = np.zeros((n, 5, self.Nr), np.complex128)
             for i, f in enumerate(wf):
-                src = [np.zeros(self.Nr, np.complex128) for _ in range(5)]
-                self._sbe_calculator(f[0], f[1], f[2], f[3], dt, *src, False, w0 + i + 1)
-                srcs.append(src)
+                self._sbe_calculator(f[0], f[1], f[2], f[3], dt, *srcs[i], False, w0 + i + 1)
         else:
             if self.full is None:
                 self._enter_full()
-            srcs = self._full_step_batch(w0, np.stack([np.stack(f[:3]) for f in wf]), dt)
-        for i, src in enumerate(srcs):
-            w = w0 + i
-            Px_, Py_, Pz_, RhoE, RhoH = wirespace.qw2prop(self.r, *src, np.asarray(rr), self.LF)
-            if self.ignorewire:
-                continue
-            Pxx[:, w] = Px_
-            Pyy[:, w] = Py_
-            Pzz[:, w] = Pz_
-            Rho[:, w] = RhoH - RhoE
+            srcs = self._full_step_batch(w0, np.ascontiguousarray(wf[:, :3]), dt)
+        out = wirespace.qw2prop_rows(self.r, srcs, np.asarray(rr), self.LF)
+        if self.ignorewire:
+            return
+        Pxx[:, w0:] = out[:, 0].T
+        Pyy[:, w0:] = out[:, 1].T
+        Pzz[:, w0:] = out[:, 2].T
+        Rho[:, w0:] = (out[:, 4] - out[:, 3]).T
 
     # -- small accessors (SBEs.py:5516-5534) ---------------------------------------
     def chiqw(self):

@@ -25,6 +25,8 @@
 // Every sum runs in the reference's order; results agree with it to
 // rounding (numpy's pairwise sums and the kernels' sequential ones differ
 // in the last bits).
+#include <mutex>
+
 #include "psb_common.cuh"
 
 namespace psb {
@@ -279,18 +281,27 @@ __global__ void __launch_bounds__(kLfThreads) leapfrog_kernel(Step s0) {
   }
 }
 
-// Wire-space sources of one level (one thread per r): the QWPolarization3
-// sums (before the 2 ehint / (area L) factor and the transform) and the
-// QWRho5 sums (before the boundary offset, normalisation and transform).
-// Wire blockIdx.y of a batch: levels [nw][3][nk][nk], out [nw][5][nr], yw and
-// (-1)^w from wpar[4 w], wpar[4 w + 1] when wpar is set.
-__global__ void sources_kernel(int nk, int nr, const double* kr, const double* rpos,
-                               const double* window, double L, double dcv, double yw,
-                               double sgnw, const double* wpar, const double2* lev,
-                               double2* out) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= nr) return;
-  const int n2 = nk * nk;
+// Wire-space sources of one level: the QWPolarization3 sums (before the
+// 2 ehint / (area L) factor and the transform) and the QWRho5 sums (before
+// the boundary offset, normalisation and transform),
+//   Px(r) = W(r) sum_{kh,ke} Re(conj(Xcv[ke][kh]) p[kh][ke] E[ke] conj(E[kh])),
+//   Py, Pz likewise with dcv yw, -dcv (-1)^w,
+//   Re(r) = W(r)/(2L) sum_{k1,k2} C[k1][k2] conj(E[k1]) E[k2],
+//   Rh(r) = W(r)/(2L) sum_{k1,k2} conj(D[k1][k2]) conj(E[k1]) E[k2],
+// E[k] = exp(i kr[k] r) (qwoptics.py:56-84, 367-381).  One CTA per
+// kSrcR positions and wire (blockIdx.y of a batch: levels [nw][3][nk][nk],
+// out [nw][5][nr], yw and (-1)^w from wpar[4 w], wpar[4 w + 1] when set):
+// the phases of its positions in shared memory, threads over the column
+// (ke, k2) so the rows of p, C, D are read coalesced, each element once for
+// all kSrcR positions, then a block reduction.  The sums run in this tree
+// order, not the reference's sequential one (they agree to rounding).
+constexpr int kSrcThreads = 128, kSrcR = 4;
+__global__ void __launch_bounds__(kSrcThreads) sources_kernel(
+    int nk, int nr, const double* kr, const double* rpos, const double* window, double L,
+    double dcv, double yw, double sgnw, const double* wpar, const double2* lev, double2* out) {
+  extern __shared__ double2 ph[];  // [kSrcR][nk]
+  __shared__ double red[kSrcR][6][kSrcThreads / 32];
+  const int n2 = nk * nk, r0 = blockIdx.x * kSrcR;
   const int64_t w = blockIdx.y;
   lev += w * 3 * n2;
   out += w * 5 * nr;
@@ -298,48 +309,70 @@ __global__ void sources_kernel(int nk, int nr, const double* kr, const double* r
     yw = wpar[4 * w];
     sgnw = wpar[4 * w + 1];
   }
+  for (int e = threadIdx.x; e < kSrcR * nk; e += kSrcThreads) {
+    const int j = e / nk, k = e - j * nk;
+    const int r = min(r0 + j, nr - 1);
+    double sn, cn;
+    sincos(kr[k] * rpos[r], &sn, &cn);
+    ph[e] = make_double2(cn, sn);
+  }
+  __syncthreads();
   const double2* p = lev;
   const double2* C = lev + n2;
   const double2* D = lev + 2 * n2;
-  const double W = window[r], y = rpos[r];
-  double px = 0.0, py = 0.0, pz = 0.0;
-  for (int ke = 0; ke < nk; ++ke) {
-    double se, ce;
-    sincos(kr[ke] * y, &se, &ce);
-    const double2 Ek = make_double2(ce, se);
-    for (int kh = 0; kh < nk; ++kh) {
-      double sh, ch;
-      sincos(kr[kh] * y, &sh, &ch);
-      const double2 Ekc = make_double2(ch, -sh);
-      const double2 pk = p[kh * nk + ke];
-      const double xvc = ((kh + 1) & 1) ? -dcv : dcv;  // conj(Xcv[ke][kh])
-      px = px + cm(cm(rs(xvc, pk), Ek), Ekc).x * W;
-      py = py + cm(cm(rs(dcv, pk), Ek), Ekc).x * W * yw;
-      pz = pz + cm(cm(rs(-dcv, pk), Ek), Ekc).x * W * sgnw;
+  double sx[kSrcR], sp[kSrcR];
+  double2 se[kSrcR], sh[kSrcR];
+#pragma unroll
+  for (int j = 0; j < kSrcR; ++j) {
+    sx[j] = sp[j] = 0.0;
+    se[j] = sh[j] = make_double2(0.0, 0.0);
+  }
+  for (int c = threadIdx.x; c < nk; c += kSrcThreads) {
+    double2 ec[kSrcR];
+#pragma unroll
+    for (int j = 0; j < kSrcR; ++j) ec[j] = ph[j * nk + c];
+    for (int i = 0; i < nk; ++i) {
+      const double2 pv = p[i * nk + c], cv = C[i * nk + c], dv = cconj(D[i * nk + c]);
+      const double xs = ((i + 1) & 1) ? -1.0 : 1.0;  // conj(Xcv) / dcv at kh = i
+#pragma unroll
+      for (int j = 0; j < kSrcR; ++j) {
+        const double2 ei = cconj(ph[j * nk + i]);
+        const double t = cm(cm(pv, ec[j]), ei).x;
+        sx[j] += xs * t;
+        sp[j] += t;
+        se[j] = ca(se[j], cm(cm(cv, ei), ec[j]));
+        sh[j] = ca(sh[j], cm(cm(dv, ei), ec[j]));
+      }
     }
   }
-  double2 re = make_double2(0.0, 0.0), rh = re;
-  for (int k2 = 0; k2 < nk; ++k2) {
-    double s2, c2;
-    sincos(kr[k2] * y, &s2, &c2);
-    const double2 E2 = make_double2(c2, s2);
-    for (int k1 = 0; k1 < nk; ++k1) {
-      double s1, c1;
-      sincos(kr[k1] * y, &s1, &c1);
-      const double2 E1c = make_double2(c1, -s1);
-      const double2 a = rs(W, cm(cm(C[k1 * nk + k2], E1c), E2));
-      const double2 b = rs(W, cm(cm(cconj(D[k1 * nk + k2]), E1c), E2));
-      re = ca(re, make_double2(a.x / (2.0 * L), a.y / (2.0 * L)));
-      rh = ca(rh, make_double2(b.x / (2.0 * L), b.y / (2.0 * L)));
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < kSrcR; ++j) {
+    const double v[6] = {sx[j], sp[j], se[j].x, se[j].y, sh[j].x, sh[j].y};
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      const double u = warp_sum(v[q]);
+      if (lane == 0) red[j][q][wp] = u;
     }
   }
-  out[r] = make_double2(px, 0.0);
-  out[nr + r] = make_double2(py, 0.0);
-  out[2 * nr + r] = make_double2(pz, 0.0);
-  out[3 * nr + r] = re;
-  out[4 * nr + r] = rh;
+  __syncthreads();
+  if (threadIdx.x < kSrcR) {
+    const int j = threadIdx.x, r = r0 + j;
+    if (r < nr) {
+      double t[6];
+      for (int q = 0; q < 6; ++q) {
+        t[q] = 0.0;
+        for (int u = 0; u < kSrcThreads / 32; ++u) t[q] += red[j][q][u];
+      }
+      const double W = window[r], h = W / (2.0 * L);
+      out[r] = make_double2(W * dcv * t[0], 0.0);
+      out[nr + r] = make_double2(W * yw * dcv * t[1], 0.0);
+      out[2 * nr + r] = make_double2(W * sgnw * -dcv * t[1], 0.0);
+      out[3 * nr + r] = make_double2(h * t[2], h * t[3]);
+      out[4 * nr + r] = make_double2(h * t[4], h * t[5]);
+    }
+  }
 }
-
 
 // ---------------------------------------------------------------------------
 // Many-body terms switched on by mb.params (PsbFullMB).  Each kernel keeps
@@ -550,106 +583,134 @@ __global__ void mb_x3_kernel(Step s0, MBView v0) {
 // SBEs.py:5248-5291): MBCE / MBCH (coulomb.py:957-1071) with |Re n| on the
 // 1-based grid, k3(a, b, c) = a + b - c (1-based, 0 when outside), and the
 // reference's C arrays read at [k - 1][..][..]; then MBPE / MBPH
-// (phonons.py:140-271) with Re n.  One thread per k.
-__global__ void mb_rates_kernel(MBView v0) {
+// (phonons.py:140-271) with Re n; with recomb also SpontEmission's Rsp.
+// One CTA per (k, wire): the occupations and V^2 in shared memory, threads
+// over the inner index of each double sum (so C[k][q1][q2] is read along
+// q2), block reductions.  The sums run in this tree order, not the
+// reference's sequential one (they agree to rounding).
+constexpr int kRateThreads = 128;
+
+// sum of K values over the CTA (kRateThreads threads); every thread gets them
+template <int K>
+__device__ __forceinline__ void rate_block_sum(double (&v)[K], double (*red)[kRateThreads / 32]) {
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < K; ++q) {
+    const double u = warp_sum(v[q]);
+    if (lane == 0) red[q][wp] = u;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < K; ++q) {
+    double t = 0.0;
+    for (int u = 0; u < kRateThreads / 32; ++u) t += red[q][u];
+    v[q] = t;
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kRateThreads) mb_rates_kernel(MBView v0) {
   const MBView v = at_wire(v0);
-  const int nk = v.nk, k0 = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k0 >= nk) return;
+  const int nk = v.nk, k0 = blockIdx.x;
   const int n2 = nk * nk, N1 = nk + 1;
+  extern __shared__ double sm[];
+  double* ne1 = sm;             // [nk + 1] |Re n_e|, 1-based, [0] = 0
+  double* nh1 = ne1 + N1;       // [nk + 1]
+  double* v2 = nh1 + N1;        // [3][nk] V(q)^2
+  __shared__ double red[5][kRateThreads / 32];
   const double2* C3 = v.X3 + n2;
   const double2* D3 = v.X3 + 2 * n2;
-  // 1-based occupation arrays of MBCE/MBCH: index 0 is 0
-  auto ne1 = [&](int i) { return i == 0 ? 0.0 : fabs(C3[(i - 1) * nk + i - 1].x); };
-  auto nh1 = [&](int i) { return i == 0 ? 0.0 : fabs(D3[(i - 1) * nk + i - 1].x); };
+  for (int i = threadIdx.x; i <= nk; i += kRateThreads) {
+    ne1[i] = i == 0 ? 0.0 : fabs(C3[(i - 1) * nk + i - 1].x);
+    nh1[i] = i == 0 ? 0.0 : fabs(D3[(i - 1) * nk + i - 1].x);
+  }
+  for (int i = threadIdx.x; i < 3 * nk; i += kRateThreads) {
+    const double x = v.V3[i];
+    v2[i] = x * x;
+  }
+  __syncthreads();
   auto k3 = [&](int a, int b, int c) {  // 0-based arguments, 1-based result
     const int r = (a + 1) + (b + 1) - (c + 1);
     return (r < 1 || r > nk) ? 0 : r;
   };
-  auto vv2 = [&](int t, int a, int b) {
-    const int d = a > b ? a - b : b - a;
-    const double x = v.V3[t * nk + d];
-    return x * x;
-  };
+  auto vv2 = [&](int t, int a, int b) { return v2[t * nk + (a > b ? a - b : b - a)]; };
   const size_t cs3 = (size_t)N1 * N1 * N1;
   const double* Ceh = v.mb.C;
   const double* Cee = Ceh + cs3;
   const double* Chh = Ceh + 2 * cs3;
   auto cix = [&](int a, int b, int c) { return ((size_t)a * N1 + b) * N1 + c; };
-  double winE = 0.0, woutE = 0.0, winH = 0.0, woutH = 0.0;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};  // WinE, WoutE, WinH, WoutH
   if (v.mb.ehs) {
     const int k = k0 + 1;  // MBCE: k; MBCH: kp
     for (int q1 = 1; q1 <= nk; ++q1) {
-      for (int q2 = 1; q2 <= nk; ++q2) {
+      for (int q2 = threadIdx.x + 1; q2 <= nk; q2 += kRateThreads) {
         {  // electrons (MBCE)
           const int kp = q1, k1 = q2;
           int r = k3(kp - 1, k1 - 1, k - 1);
           if (r > 0)
-            winE += vv2(0, k - 1, k1 - 1) * (1.0 - nh1(kp)) * nh1(r) * ne1(k1) *
-                    Ceh[cix(k - 1, kp - 1, k1 - 1)];
+            acc[0] += vv2(0, k - 1, k1 - 1) * (1.0 - nh1[kp]) * nh1[r] * ne1[k1] *
+                      Ceh[cix(k - 1, kp - 1, k1 - 1)];
           r = k3(kp - 1, k - 1, k1 - 1);
           if (r > 0)
-            woutE += vv2(0, k1 - 1, k - 1) * (1.0 - ne1(k1)) * (1.0 - nh1(kp)) * nh1(r) *
-                     Ceh[cix(k1 - 1, kp - 1, k - 1)];
+            acc[1] += vv2(0, k1 - 1, k - 1) * (1.0 - ne1[k1]) * (1.0 - nh1[kp]) * nh1[r] *
+                      Ceh[cix(k1 - 1, kp - 1, k - 1)];
           const int k2 = q1, k4 = q2;
           r = k3(k - 1, k2 - 1, k4 - 1);
           if (r > 0)
-            winE += vv2(1, k - 1, k4 - 1) * (1.0 - ne1(k2)) * ne1(r) * ne1(k4) *
-                    Cee[cix(k - 1, k2 - 1, k4 - 1)];
+            acc[0] += vv2(1, k - 1, k4 - 1) * (1.0 - ne1[k2]) * ne1[r] * ne1[k4] *
+                      Cee[cix(k - 1, k2 - 1, k4 - 1)];
           r = k3(k4 - 1, k2 - 1, k - 1);
           if (r > 0)
-            woutE += vv2(1, k4 - 1, k - 1) * (1.0 - ne1(k4)) * (1.0 - ne1(k2)) * ne1(r) *
-                     Cee[cix(k4 - 1, k2 - 1, k - 1)];
+            acc[1] += vv2(1, k4 - 1, k - 1) * (1.0 - ne1[k4]) * (1.0 - ne1[k2]) * ne1[r] *
+                      Cee[cix(k4 - 1, k2 - 1, k - 1)];
         }
-        {  // holes (MBCH): kp is this thread's momentum
+        {  // holes (MBCH): kp is this CTA's momentum
           const int kp = k, kk = q1, k1 = q2;
           int r = k3(kp - 1, k1 - 1, kk - 1);
           if (r > 0)
-            winH += vv2(0, kk - 1, k1 - 1) * (1.0 - ne1(kk)) * nh1(r) * ne1(k1) *
-                    Ceh[cix(kk - 1, kp - 1, k1 - 1)];
+            acc[2] += vv2(0, kk - 1, k1 - 1) * (1.0 - ne1[kk]) * nh1[r] * ne1[k1] *
+                      Ceh[cix(kk - 1, kp - 1, k1 - 1)];
           r = k3(kp - 1, kk - 1, k1 - 1);
           if (r > 0)
-            woutH += vv2(0, k1 - 1, kk - 1) * (1.0 - ne1(kk)) * (1.0 - nh1(r)) * ne1(k1) *
-                     Ceh[cix(kk - 1, r - 1, k1 - 1)];
+            acc[3] += vv2(0, k1 - 1, kk - 1) * (1.0 - ne1[kk]) * (1.0 - nh1[r]) * ne1[k1] *
+                      Ceh[cix(kk - 1, r - 1, k1 - 1)];
           const int k2p = q1, k4p = q2;
           r = k3(kp - 1, k2p - 1, k4p - 1);
           if (r > 0)
-            winH += vv2(2, kp - 1, k4p - 1) * (1.0 - nh1(k2p)) * nh1(r) * nh1(k4p) *
-                    Chh[cix(kp - 1, k2p - 1, k4p - 1)];
+            acc[2] += vv2(2, kp - 1, k4p - 1) * (1.0 - nh1[k2p]) * nh1[r] * nh1[k4p] *
+                      Chh[cix(kp - 1, k2p - 1, k4p - 1)];
           r = k3(k4p - 1, k2p - 1, kp - 1);
           if (r > 0)
-            woutH += vv2(2, k4p - 1, kp - 1) * (1.0 - nh1(k4p)) * (1.0 - nh1(k2p)) * nh1(r) *
-                     Chh[cix(k4p - 1, k2p - 1, kp - 1)];
+            acc[3] += vv2(2, k4p - 1, kp - 1) * (1.0 - nh1[k4p]) * (1.0 - nh1[k2p]) * nh1[r] *
+                      Chh[cix(k4p - 1, k2p - 1, kp - 1)];
         }
       }
     }
   }
+  rate_block_sum<4>(acc, red);
   if (v.mb.phonon) {
     // Vep[k][i] = VC_ee[k][i] / E1D[k][i] * Vscale (VC already screened)
     const double* EP = v.mb.ph;
     const double* EPT = EP + n2;
     const double* HP = EP + 2 * n2;
     const double* HPT = EP + 3 * n2;
-    auto epsd = [&](int d) { return v.mb.eps ? v.mb.eps[d] : 1.0; };
-    double sin_e = 0.0, sout_e = 0.0, sin_h = 0.0, sout_h = 0.0;
-    for (int i = 0; i < nk; ++i) {
+    double ph[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int i = threadIdx.x; i < nk; i += kRateThreads) {
       const int d = i > k0 ? i - k0 : k0 - i;
-      const double vep = v.V3[nk + d] / epsd(d) * v.mb.vscale;
-      const double vhp = v.V3[2 * nk + d] / epsd(d) * v.mb.vscale;
+      const double e = v.mb.eps ? v.mb.eps[d] : 1.0;
+      const double vep = v.V3[nk + d] / e * v.mb.vscale;
+      const double vhp = v.V3[2 * nk + d] / e * v.mb.vscale;
       const double nei = C3[i * nk + i].x, nhi = D3[i * nk + i].x;
-      sin_e += vep * nei * EPT[i * nk + k0];
-      sout_e += vep * (1.0 - nei) * EP[i * nk + k0];
-      sin_h += vhp * nhi * HPT[i * nk + k0];
-      sout_h += vhp * (1.0 - nhi) * HP[i * nk + k0];
+      ph[0] += vep * nei * EPT[i * nk + k0];
+      ph[1] += vep * (1.0 - nei) * EP[i * nk + k0];
+      ph[2] += vhp * nhi * HPT[i * nk + k0];
+      ph[3] += vhp * (1.0 - nhi) * HP[i * nk + k0];
     }
-    winE = winE + sin_e;
-    woutE = woutE + sout_e;
-    winH = winH + sin_h;
-    woutH = woutH + sout_h;
+    rate_block_sum<4>(ph, red);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[q] = acc[q] + ph[q];
   }
-  v.rates[k0] = winE;
-  v.rates[nk + k0] = woutE;
-  v.rates[2 * nk + k0] = winH;
-  v.rates[3 * nk + k0] = woutH;
+  double rsp = 0.0;
   if (v.mb.recomb) {
     // SpontEmission (emission.py:94-131) from the level the right-hand side
     // reads (SBEs.py:5237-5238): Ec (emission.py:133-172) with Re n and the
@@ -659,23 +720,32 @@ __global__ void mb_rates_kernel(MBView v0) {
     const double2* C2 = v.L + n2;
     const double2* D2 = v.L + 2 * n2;
     const double veh0 = v.V3[0], vee0 = v.V3[nk], vhh0 = v.V3[2 * nk];
-    double s1 = 0.0, s2 = 0.0;
-    for (int i = 0; i < nk; ++i) {
+    double ec[2] = {0.0, 0.0};
+    for (int i = threadIdx.x; i < nk; i += kRateThreads) {
       const int d = i > k0 ? i - k0 : k0 - i;
       const double ne = C2[i * nk + i].x, nh = D2[i * nk + i].x;
-      s1 += ne * (vee0 - v.V3[nk + d]) + nh * (vhh0 - v.V3[2 * nk + d]);
+      ec[0] += ne * (vee0 - v.V3[nk + d]) + nh * (vhh0 - v.V3[2 * nk + d]);
       const double id = i == k0 ? 0.0 : 1.0;
-      s2 += ne * veh0 * id - nh * veh0 * id;
+      ec[1] += ne * veh0 * id - nh * veh0 * id;
     }
-    const double ek = ((v.gap + v.Ee[k0]) + v.Eh[k0]) + ((s1 + s2) - veh0);
+    rate_block_sum<2>(ec, red);
+    const double ek = ((v.gap + v.Ee[k0]) + v.Eh[k0]) + ((ec[0] + ec[1]) - veh0);
     const double* hw = v.mb.emis;
     const double* sq = hw + v.mb.n_hw;
-    double acc = 0.0;
-    for (int n = 0; n < v.mb.n_hw; ++n) {
+    double it[1] = {0.0};
+    for (int n = threadIdx.x; n < v.mb.n_hw; n += kRateThreads) {
       const double x = hw[n] + ek;
-      acc += x * (x * x / v.mb.rho0_den) * sq[n];
+      it[0] += x * (x * x / v.mb.rho0_den) * sq[n];
     }
-    v.rates[4 * nk + k0] = acc * v.mb.dhw;
+    rate_block_sum<1>(it, red);
+    rsp = it[0] * v.mb.dhw;
+  }
+  if (threadIdx.x == 0) {
+    v.rates[k0] = acc[0];
+    v.rates[nk + k0] = acc[1];
+    v.rates[2 * nk + k0] = acc[2];
+    v.rates[3 * nk + k0] = acc[3];
+    if (v.mb.recomb) v.rates[4 * nk + k0] = rsp;
   }
 }
 
@@ -1070,7 +1140,8 @@ int full_launch(const Launch& a, cudaStream_t st) {
     const dim3 b3((3 * n2 + th - 1) / th, nw);
     full::mb_x3_kernel<<<b3, th, 0, st>>>(s, v);
     if (relax) {
-      full::mb_rates_kernel<<<blk, th, 0, st>>>(v);
+      const size_t smr = (2 * (size_t)(nk + 1) + 3 * (size_t)nk) * 8;
+      full::mb_rates_kernel<<<dim3(nk, nw), full::kRateThreads, smr, st>>>(v);
       full::mb_relax_kernel<<<blk, th, 0, st>>>(v, a.params->dt);
     }
     if (dct) {
@@ -1184,6 +1255,22 @@ extern "C" int psb_full_step_batch_f64(int nw, int nk, int nr, int nq0, const do
   return check_cuda("psb_full_step_batch_f64");
 }
 
+namespace {
+// dynamic shared memory of sources_kernel (the phases of its positions),
+// with the opt-in above 48 KB set on first use; 0 if that fails
+size_t sources_smem(int nk) {
+  const size_t sm = (size_t)full::kSrcR * nk * 16;
+  static std::once_flag once;
+  static bool ok = true;
+  if (sm > 48 * 1024)
+    std::call_once(once, [] {
+      ok = cudaFuncSetAttribute(full::sources_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                full::kSrcR * PSB_MAX_NK * 16) == cudaSuccess;
+    });
+  return ok ? sm : 0;
+}
+}  // namespace
+
 extern "C" int psb_full_sources_f64(int nk, int nr, const double* d_kr, const double* d_r,
                                     const double* d_window, double L, double dcv, double yw,
                                     double sgnw, const double* d_level, double* d_out,
@@ -1192,8 +1279,10 @@ extern "C" int psb_full_sources_f64(int nk, int nr, const double* d_kr, const do
     return set_error(PSB_ERR_INVALID, "psb_full_sources_f64: null pointer");
   if (nk < 2 || nk > PSB_MAX_NK || nr < 1)
     return set_error(PSB_ERR_SIZE, "psb_full_sources_f64: nk %d / nr %d out of range", nk, nr);
-  const int th = 64, bl = (nr + th - 1) / th;
-  full::sources_kernel<<<bl, th, 0, (cudaStream_t)stream>>>(
+  const size_t sm = sources_smem(nk);
+  if (!sm) return set_error(PSB_ERR_CUDA, "psb_full_sources_f64: shared memory");
+  full::sources_kernel<<<(nr + full::kSrcR - 1) / full::kSrcR, full::kSrcThreads, sm,
+                         (cudaStream_t)stream>>>(
       nk, nr, d_kr, d_r, d_window, L, dcv, yw, sgnw, nullptr,
       reinterpret_cast<const double2*>(d_level), reinterpret_cast<double2*>(d_out));
   return check_cuda("psb_full_sources_f64");
@@ -1208,9 +1297,10 @@ extern "C" int psb_full_sources_batch_f64(int nw, int nk, int nr, const double* 
   if (nk < 2 || nk > PSB_MAX_NK || nr < 1 || nw < 1 || nw > PSB_FULL_MAX_WIRES)
     return set_error(PSB_ERR_SIZE, "psb_full_sources_batch_f64: nw %d / nk %d / nr %d", nw, nk,
                      nr);
-  const int th = 64;
-  const dim3 bl((nr + th - 1) / th, nw);
-  full::sources_kernel<<<bl, th, 0, (cudaStream_t)stream>>>(
+  const size_t sm = sources_smem(nk);
+  if (!sm) return set_error(PSB_ERR_CUDA, "psb_full_sources_batch_f64: shared memory");
+  const dim3 bl((nr + full::kSrcR - 1) / full::kSrcR, nw);
+  full::sources_kernel<<<bl, full::kSrcThreads, sm, (cudaStream_t)stream>>>(
       nk, nr, d_kr, d_r, d_window, L, dcv, 0.0, 0.0, d_wpar,
       reinterpret_cast<const double2*>(d_levels), reinterpret_cast<double2*>(d_out));
   return check_cuda("psb_full_sources_batch_f64");

@@ -24,3 +24,26 @@ def test_centred_transforms_match_reference():
     np.testing.assert_array_equal(G, d["ifftg"])
     ws.fftg(G)  # round trip
     assert np.max(np.abs(G - d["z0"])) < 1e-14 * np.max(np.abs(d["z0"]))
+
+
+def test_row_versions_equal_one_signal_calls():
+    """prop2qw_rows / qw2prop_rows (all wires of a Maxwell step at once) give
+    every row the bits of its own one-signal call."""
+    rng = np.random.default_rng(5)
+    RR = np.linspace(-5e-8, 5e-8, 64)
+    r = np.linspace(-6e-8, 6e-8, 230)
+    window = np.exp(-((r / 5e-8) ** 150))
+    F = (rng.standard_normal((12, 64)) + 1j * rng.standard_normal((12, 64))) * 1e7
+    rows = ws.prop2qw_rows(RR, F, r, window)
+    for j in range(3):
+        one = ws.prop2qw(RR, F[4 * j], F[4 * j + 1], F[4 * j + 2], F[4 * j + 3], r, window)
+        for k in range(4):
+            np.testing.assert_array_equal(rows[4 * j + k], one[k])
+    for plasmonics in (False, True):
+        S = rng.standard_normal((3, 5, 230)) + 1j * rng.standard_normal((3, 5, 230))
+        got = ws.qw2prop_rows(r, S.copy(), RR, plasmonics)
+        for j in range(3):
+            a = [S[j, k].copy() for k in range(5)]
+            one = ws.qw2prop(r, *a, RR, plasmonics)
+            for k in range(5):
+                np.testing.assert_array_equal(got[j, k], one[k])
