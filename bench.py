@@ -81,7 +81,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c4", choices=["c1", "c2", "c3", "c4"])
+    ap.add_argument("--workload", default="c4", choices=["c1", "c2", "c3", "c4", "pstd"])
     ap.add_argument("--chunk", type=int, default=100, help="time steps per bench step")
     ap.add_argument("--form", default="split", choices=["plain", "split"],
                     help="split int8-digit tensor-core kernel or plain FP64 kernel")
@@ -166,6 +166,246 @@ WORKLOAD_NAMES = {
     "c4": "c4: Poisson 2000 requests/s for 60 s, Nk in {64,128,256,512,1024} "
           "p={.3,.3,.2,.15,.05}, 1-4 ps at 1 fs, parameters as c1, 150 GB HBM budget",
 }
+
+
+# ---------------------------------------------------------------------------
+# pstd: the PSTD caller's step of all its wires (rhoPJ.QuantumWire's loop of
+# QWCalculator calls, rhoPJ.py:311-348) on the full Nk x Nk state with every
+# many-body term.
+# ---------------------------------------------------------------------------
+PSTD_QW = """{L}     # L
+5e-9       # Delta0
+1.5        # gap
+0.07       # me
+0.45       # mh
+100e-3     # HO
+5e12       # gam_e
+5e12       # gam_h
+5e12       # gam_eh
+9.1        # epsr
+36e-3      # Oph
+3e-3       # Gph
+2000000.0  # Edc
+1000000    # jmax
+20000      # ntmax
+"""
+# Optics Excitons EHs Screened Phonon DCTrans LF FreePot DiagDph OffDiagDph
+# Recomb PLSpec ignorewire Xqwparams LorentzDelta
+PSTD_MB = "1\n1\n1\n1\n1\n1\n1\n0\n1\n1\n1\n0\n0\n0\n0\n"
+PSTD_L, PSTD_NRR, PSTD_DT, PSTD_E0 = 1e-7, 64, 1e-17, 1e8
+PSTD_METRIC = "full-matrix wire-steps/s (QWCalculator steps of all wires per Maxwell step)"
+
+
+def pstd_config(nw):
+    return {"workload": f"pstd: one Maxwell step of {nw} quantum wires (rhoPJ.QuantumWire's "
+                        "QWCalculator loop), L 100 nm (Nk 114), 64-point propagation grid, "
+                        "full Nk x Nk state, screened, LF, DiagDph OffDiagDph EHs Phonon "
+                        "Recomb DCTrans (Edc 2 MV/m), dt 10 as",
+            "wires_per_gpu": int(nw), "time_steps_per_bench_step": 1,
+            "l2": "256 MiB write between timed steps (outside the events)",
+            "parallelism": "wires sharded, independent GPU(s)"}
+
+
+def pstd_solver(path, nw):
+    from pulsesuite_b200 import SBEs
+
+    os.makedirs(os.path.join(path, "params"), exist_ok=True)
+    with open(os.path.join(path, "params", "qw.params"), "w") as f:
+        f.write(PSTD_QW.format(L=PSTD_L))
+    with open(os.path.join(path, "params", "mb.params"), "w") as f:
+        f.write(PSTD_MB)
+    cwd = os.getcwd()
+    os.chdir(path)
+    try:
+        return SBEs.SBESolver(None, np.linspace(-5e-8, 5e-8, PSTD_NRR), 0.0, 1e7, 800e-9, nw,
+                              True)
+    finally:
+        os.chdir(cwd)
+
+
+def pstd_fields(i):
+    """The propagation-space fields along the wire at step i: a Gaussian
+    profile (every q on the wire) under a carrier at 1.55 eV."""
+    rr = np.linspace(-5e-8, 5e-8, PSTD_NRR)
+    prof = np.exp(-((rr / 3e-8) ** 2))
+    E = PSTD_E0 * np.cos(2.35e15 * i * PSTD_DT)
+    return rr, [(0.3 * E * prof * (rr / 3e-8)).astype(complex), (E * prof).astype(complex),
+                (0.2 * E * prof).astype(complex), np.zeros(PSTD_NRR, complex)]
+
+
+def pstd_reference_sample(threads, nsteps=2):
+    """The reference's own QWCalculator on the host cores, one wire of the
+    same configuration: (wire-steps/s, the cpu_baseline record)."""
+    from oracle import numba_ref
+
+    if not numba_ref.available():
+        return None, {"unavailable": "reference not installed under baseline/_ref"}
+    import platform
+
+    R = numba_ref.load(threads=threads)
+    sec, nk = numba_ref.qwcalc_seconds_per_wire_step(R, PSTD_QW.format(L=PSTD_L), PSTD_MB,
+                                                     nrr=PSTD_NRR, nsteps=nsteps, E0=PSTD_E0)
+    return 1.0 / sec, {"value": 1.0 / sec, "unit": "wire-steps/s", "cores": int(R.threads),
+                       "kind": "reference", "cpu": platform.processor() or platform.machine(),
+                       "sample": f"reference SBESolver.QWCalculator, one wire, Nk {nk}, "
+                                 f"mean of {nsteps} calls after one compiling call: "
+                                 f"{sec * 1e3:.1f} ms per wire-step"}
+
+
+def run_pstd(a):
+    """One bench step = one Maxwell step of all the rank's wires (one
+    QWCalculator step per wire).  value: the batched full step
+    (psb_full_step_batch_f64 + psb_full_sources_batch_f64) with the
+    wire-space fields resident on the device, CUDA events, max over ranks;
+    e2e: SBESolver.QWCalculatorAll with host fields in and host sources out
+    (Prop2QW / QW2Prop on the host, copies each way); per_wire_loop: the
+    reference's calling pattern, one QWCalculator call per wire.  The
+    reference arm times the reference's own QWCalculator on the host cores."""
+    import tempfile
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    nw = a.nwires or 64
+    threads = os.cpu_count() or 1
+    if a.impl == "reference":
+        if rank != 0:
+            return
+        for _ in range(max(1, a.warmup)):
+            pstd_reference_sample(threads, nsteps=1)
+        t0 = time.perf_counter()
+        vals = [pstd_reference_sample(threads, nsteps=1) for _ in range(a.steps)]
+        wall = time.perf_counter() - t0
+        if vals[-1][0] is None:
+            print(json.dumps({"impl": "reference", "unavailable": vals[-1][1]["unavailable"]}))
+            return
+        v = float(np.mean([x[0] for x in vals]))
+        cb = dict(vals[-1][1])
+        cb["value"] = v
+        print(json.dumps({
+            "impl": "reference", "metric": PSTD_METRIC, "value": v, "unit": "wire-steps/s",
+            "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": wall * 1e3 / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (deterministic fields)",
+            "config": pstd_config(nw),
+            "form": "reference SBESolver.QWCalculator (Python + Numba), one wire per bench step",
+            "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": "wire-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}), flush=True)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    from pulsesuite_b200 import _lib, device, wirespace
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    tmp = tempfile.mkdtemp(prefix="psb_pstd_")
+    s = pstd_solver(os.path.join(tmp, "a"), nw)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def maxwell_step(solver, i, batched=True):
+        rr, f = pstd_fields(i)
+        o = [np.zeros((PSTD_NRR, nw), complex) for _ in range(4)]
+        if batched:
+            solver.QWCalculatorAll(*f, rr, None, PSTD_DT, *o, [False], [False])
+        else:
+            for w in range(nw):
+                ow = [np.zeros(PSTD_NRR, complex) for _ in range(4)]
+                solver.QWCalculator(*f, rr, None, PSTD_DT, w + 1, *ow, [False], [False])
+                for x, y in zip(o, ow):
+                    x[:, w] = y
+        return o
+
+    for i in range(max(1, a.warmup)):
+        maxwell_step(s, i)
+    # device-resident inputs: the wire-space fields of one step
+    rr, f = pstd_fields(a.warmup)
+    wf = wirespace.prop2qw_rows(rr, np.stack(f), s.r, s.window)
+    fd, wpd = s._full_batch_inputs(0, np.ascontiguousarray(np.broadcast_to(wf[:3], (nw, 3, s.Nr))),
+                                   PSTD_DT)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(a.steps)]
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    with Clocks(local) as clk:
+        for k in range(a.steps):
+            flush.fill_(float(k))
+            evs[k][0].record(stream)
+            s._full_launch_batch(0, fd, wpd, PSTD_DT)
+            evs[k][1].record(stream)
+        torch.cuda.synchronize()
+    total_ms = float(sum(e0.elapsed_time(e1) for e0, e1 in evs))
+    # end to end through the public API
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in range(a.steps):
+        maxwell_step(s, a.warmup + 1 + k)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    # the per-wire calling pattern of the reference's caller, on a second solver
+    b = pstd_solver(os.path.join(tmp, "b"), nw)
+    maxwell_step(b, 0, batched=False)
+    kl = min(a.steps, 3)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in range(kl):
+        maxwell_step(b, 1 + k, batched=False)
+    torch.cuda.synchronize()
+    loop_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([total_ms, e2e_s, loop_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms, e2e_s, loop_s = (float(x) for x in t.tolist())
+        dist.barrier()
+    value = nw * a.steps * world / (total_ms * 1e-3)
+    nk, nr = s.Nk, s.Nr
+    mb = s.full["mb"]
+    # screen; meh, calch; gamma, offd, offp; derivs; x3, rates, relax;
+    # shift, rows, cols; leapfrog; sources
+    launches = 1 + 2 + 3 + 1 + 3 + 3 + 1 + 1
+    assert mb is not None and s.Screened and s.LF
+    fp64 = fp64_peak_tflops(torch, _lib, device)
+    ach = 96.0 * nk ** 3 * nw / (total_ms / a.steps * 1e-3) / 1e12
+    line = {
+        "metric": PSTD_METRIC, "value": value, "unit": "wire-steps/s", "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": total_ms / a.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (deterministic fields)", "config": pstd_config(nw),
+        "e2e": {"value": nw * a.steps * world / e2e_s, "unit": "wire-steps/s",
+                "h2d_bytes_per_step": nw * (3 * nr * 16 + 4 * 8),
+                "d2h_bytes_per_step": nw * (5 * nr * 16 + 2 * nk * 16),
+                "api": "pulsesuite_b200.SBEs.SBESolver.QWCalculatorAll (host arrays, "
+                       "Prop2QW / QW2Prop on the host)",
+                "ms_per_step": e2e_s * 1e3 / a.steps},
+        "per_wire_loop": {"value": nw * kl * world / loop_s, "unit": "wire-steps/s",
+                          "api": "SBESolver.QWCalculator once per wire (rhoPJ.py:311-348)",
+                          "ms_per_step": loop_s * 1e3 / kl},
+        "roofline": {"bound": "fp64", "achieved": ach, "peak": fp64, "unit": "TFLOP/s",
+                     "frac": ach / fp64, "traffic": None,
+                     "work": "96 Nk^3 flops per wire-step: the 12 complex Nk x Nk x Nk "
+                             "products of dpdt/dCdt/dDdt; the step's other O(Nk^3) kernels "
+                             "(exchange sums, dephasing, scattering, DC shift, source sums) "
+                             "count as overhead",
+                     "peak_source": "measured in this run: psb_probe_fp64_fma"},
+        "gpu_launches": launches * a.steps,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and not a.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = pstd_reference_sample(threads)[1]
+        except Exception as ex:
+            line["cpu_baseline"] = {"unavailable": f"{type(ex).__name__}: {ex}"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
 
 
 # ---------------------------------------------------------------------------
@@ -820,7 +1060,9 @@ def run_reference(a):
 
 def main():
     a = parse()
-    if a.impl == "reference":
+    if a.workload == "pstd":
+        run_pstd(a)
+    elif a.impl == "reference":
         run_reference(a)
     else:
         run_ours(a)

@@ -147,3 +147,42 @@ def seconds_per_step(R, grid, wire, dt, nsteps=1):
     for _ in range(nsteps):
         t = R.integrator.rk4_dpc(y, D(t, y), t, dt, D)
     return (time.perf_counter() - t0) / nsteps
+
+
+def qwcalc_seconds_per_wire_step(R, qw_params, mb_params, nrr=64, nsteps=2, E0=1e8):
+    """Wall seconds of one call of the reference's SBESolver.QWCalculator
+    (SBEs.py:5838-6001) for one wire -- the step the PSTD caller makes per
+    wire per Maxwell step (rhoPJ.py:311-348) -- with the given params-file
+    texts, driven by fields along the wire with a Gaussian profile (the
+    full-matrix state with every many-body term mb.params switches on).
+    The solver is built in a scratch directory (it reads params/ and writes
+    dataQW/ there); one untimed call compiles the Numba kernels.  Returns
+    (seconds, Nk)."""
+    run = tempfile.mkdtemp(prefix="psb_qwc_")
+    os.makedirs(os.path.join(run, "params"))
+    with open(os.path.join(run, "params", "qw.params"), "w") as f:
+        f.write(qw_params)
+    with open(os.path.join(run, "params", "mb.params"), "w") as f:
+        f.write(mb_params)
+    cwd = os.getcwd()
+    os.chdir(run)
+    try:
+        rr = np.linspace(-5e-8, 5e-8, nrr)
+        qrr = R.SBEs.GetKArray(nrr, nrr * (rr[1] - rr[0]))
+        s = R.SBEs.SBESolver(qrr, rr, 0.0, 1e7, 800e-9, 1, True)
+        prof = np.exp(-((rr / 3e-8) ** 2))
+        dt = 1e-17
+
+        def call():
+            o = [np.zeros(nrr, complex) for _ in range(4)]
+            s.QWCalculator((0.3 * E0 * prof * (rr / 3e-8)).astype(complex),
+                           (E0 * prof).astype(complex), (0.2 * E0 * prof).astype(complex),
+                           np.zeros(nrr, complex), rr, qrr, dt, 1, *o, [False], [False])
+
+        call()
+        t0 = time.perf_counter()
+        for _ in range(nsteps):
+            call()
+        return (time.perf_counter() - t0) / nsteps, int(s.Nk)
+    finally:
+        os.chdir(cwd)

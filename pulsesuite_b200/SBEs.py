@@ -574,20 +574,16 @@ class SBESolver:
             Re[:] = 2.0 * _e0 * Re / self.area * self.ehint
             Rh[:] = 2.0 * _e0 * Rh / self.area * self.ehint
 
-    def _full_step_batch(self, w0, fields, dt):
-        """One step of wires w0 + 1 .. Nw (1-based) on the full state in one
-        launch set (psb_full_step_batch_f64, psb_full_sources_batch_f64);
-        fields [n][3][Nr] complex wire-space Ex, Ey, Ez.  Returns the five
-        sources (Px, Py, Pz, Re, Rh) of each wire, [n][5][Nr], as _full_step
-        writes them."""
+    def _full_batch_inputs(self, w0, fields, dt):
+        """Device inputs of a batch step of wires w0 + 1 .. Nw: the fields
+        [n][3][Nr] (zero without Optics) and the per-wire parameters [n][4]
+        = yw(w), (-1)^w, the DC shift of the wire's q = 0 field, 0."""
         import torch
 
-        from . import device as _dev
         from .manybody import dc_shift
 
         F = self.full
-        nk, nw = self.Nk, self.Nw
-        n = nw - w0
+        n = self.Nw - w0
         fd = torch.as_tensor(np.ascontiguousarray(fields, dtype=np.complex128), device="cuda")
         if not self.Optics:
             fd.zero_()
@@ -597,7 +593,20 @@ class SBESolver:
             wpar[i, 0], wpar[i, 1] = yw(w), (-1) ** w
             if F["mb"] is not None:
                 wpar[i, 2] = dc_shift(F["mb"].edc, float(np.real(fields[i][0][self.NQ0])), dt)
-        wpd = torch.as_tensor(wpar, device="cuda")
+        return fd, torch.as_tensor(wpar, device="cuda")
+
+    def _full_launch_batch(self, w0, fd, wpd, dt):
+        """Launch the step and the source sums of wires w0 + 1 .. Nw on the
+        current stream (psb_full_step_batch_f64, psb_full_sources_batch_f64)
+        from device-resident fields fd and parameters wpd; the sums land in
+        full["bout"][:n].  No host copies."""
+        import torch
+
+        from . import device as _dev
+
+        F = self.full
+        nk, nw = self.Nk, self.Nw
+        n = nw - w0
         prm = np.zeros(1, dtype=abi.FULL_PARAMS_DTYPE)
         prm["ehint"], prm["dcv"] = self.ehint, self.dcv
         prm["gap"], prm["gam_e"], prm["gam_h"] = self.gap, self.gam_e, self.gam_h
@@ -618,20 +627,32 @@ class SBESolver:
                   float(t0["L"]), float(t0["dens_max"]), int(self.Screened), _dev.ptr(fd),
                   abi.as_ptr(prm), _dev.ptr(wpd), mbd, _dev.ptr(L1), _dev.ptr(L2),
                   _dev.ptr(L3), _dev.ptr(F["bwork"]), F["bwork"].numel(), _dev.stream_ptr())
+        if self.Optics or self.LF:
+            _lib.call("psb_full_sources_batch_f64", n, nk, self.Nr, _dev.ptr(F["kr"]),
+                      _dev.ptr(F["r"]), _dev.ptr(F["window"]), float(self.L), float(self.dcv),
+                      _dev.ptr(wpd), _dev.ptr(L3), _dev.ptr(F["bout"][:n]), _dev.stream_ptr())
+
+    def _full_step_batch(self, w0, fields, dt):
+        """One step of wires w0 + 1 .. Nw (1-based) on the full state in one
+        launch set; fields [n][3][Nr] complex wire-space Ex, Ey, Ez.  Returns
+        the five sources (Px, Py, Pz, Re, Rh) of each wire, [n][5][Nr], as
+        _full_step writes them."""
+        import torch
+
+        n = self.Nw - w0
+        fd, wpd = self._full_batch_inputs(w0, fields, dt)
+        self._full_launch_batch(w0, fd, wpd, dt)
         srcs = np.zeros((n, 5, self.Nr), np.complex128)
         if not (self.Optics or self.LF):
             return srcs
-        out = F["bout"][:n]
-        _lib.call("psb_full_sources_batch_f64", n, nk, self.Nr, _dev.ptr(F["kr"]),
-                  _dev.ptr(F["r"]), _dev.ptr(F["window"]), float(self.L), float(self.dcv),
-                  _dev.ptr(wpd), _dev.ptr(L3), _dev.ptr(out), _dev.stream_ptr())
-        out = out.cpu().numpy()
+        out = self.full["bout"][:n].cpu().numpy()
         if self.Optics:
             # QWPolarization3's factor and transform, all wires at once
             P = out[:, :3] * 2 * self.ehint / self.area / self.L   # contiguous [n][3][Nr]
             wirespace.fftg(P.reshape(3 * n, self.Nr))
             srcs[:, :3] = P
         if self.LF:
+            L3 = self.full["L"][2][w0:]
             diag = torch.diagonal(L3[:, 1:3], dim1=-2, dim2=-1).cpu().numpy()  # [n][2][nk]
             dr = self.r[1] - self.r[0]
             for i in range(n):

@@ -184,29 +184,86 @@ __global__ void calch_kernel(Step s0) {
 }
 
 // dpdt / dCdt / dDdt (SBEs.py:1952-1975, 2318-2337, 2617-2636): one thread
-// per (i, j), the four dot products of each in the reference's order.
-__global__ void derivs_kernel(Step s0) {
+// per (i, j), the four dot products of each in the reference's order (each
+// accumulator runs over k = 0 .. nk-1 in sequence).  One CTA computes a
+// kDT x kDT block of elements: per chunk of kDT values of k, the 18 operand
+// tiles the block's 12 dot products read are staged in shared memory
+// (rows padded by one element against bank conflicts).
+constexpr int kDT = 16, kDTP = kDT + 1;
+enum DTile {  // tile [row block][col block]; I, J the element block, K the k chunk
+  T_HHH_IK, T_HHH_JK, T_HHH_KI, T_HEE_JK, T_HEE_KI, T_HEH_KI, T_HEH_JK, T_HEH_IK, T_HEH_KJ,
+  T_P_KJ, T_P_IK, T_P_KI, T_P_JK, T_C_KJ, T_C_IK, T_D_KI, T_D_IK, T_D_KJ, T_NUM
+};
+constexpr size_t kDerivsSmem = (size_t)T_NUM * kDT * kDTP * sizeof(double2);
+
+__global__ void __launch_bounds__(kDT* kDT) derivs_kernel(Step s0) {
   const Step s = at_wire(s0);
   const int nk = s.nk, n2 = nk * nk;
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= n2) return;
-  const int i = e / nk, j = e - i * nk;
+  extern __shared__ double2 dsm[];
+  const int tx = threadIdx.x % kDT, ty = threadIdx.x / kDT;
+  const int I0 = blockIdx.x * kDT, J0 = blockIdx.z * kDT;
+  const int i = I0 + ty, j = J0 + tx;
   const double2* p = s.L3;
   const double2* C = s.L3 + n2;
   const double2* D = s.L3 + 2 * n2;
   const double2* Heh = s.H;
   const double2* Hee = s.H + n2;
   const double2* Hhh = s.H + 2 * n2;
-  const double hb = s.prm.hbar;
   const double2 z = make_double2(0.0, 0.0);
-  // dp[kh = i][ke = j]
+  auto tile = [&](int t, int r, int c) -> double2& { return dsm[(t * kDT + r) * kDTP + c]; };
+  // tile t of matrix M: rows from block R0 (or the k chunk), columns likewise
+  auto load = [&](int t, const double2* M, int R0, int C0) {
+    const int r = R0 + ty, c = C0 + tx;
+    tile(t, ty, tx) = (r < nk && c < nk) ? M[r * nk + c] : z;
+  };
+  double2 a1 = z, a2 = z, a3 = z, a4 = z;  // dp
+  double2 b1 = z, b2 = z, b3 = z, b4 = z;  // dC
+  double2 c1 = z, c2 = z, c3 = z, c4 = z;  // dD
+  for (int k0 = 0; k0 < nk; k0 += kDT) {
+    load(T_HHH_IK, Hhh, I0, k0);
+    load(T_HHH_JK, Hhh, J0, k0);
+    load(T_HHH_KI, Hhh, k0, I0);
+    load(T_HEE_JK, Hee, J0, k0);
+    load(T_HEE_KI, Hee, k0, I0);
+    load(T_HEH_KI, Heh, k0, I0);
+    load(T_HEH_JK, Heh, J0, k0);
+    load(T_HEH_IK, Heh, I0, k0);
+    load(T_HEH_KJ, Heh, k0, J0);
+    load(T_P_KJ, p, k0, J0);
+    load(T_P_IK, p, I0, k0);
+    load(T_P_KI, p, k0, I0);
+    load(T_P_JK, p, J0, k0);
+    load(T_C_KJ, C, k0, J0);
+    load(T_C_IK, C, I0, k0);
+    load(T_D_KI, D, k0, I0);
+    load(T_D_IK, D, I0, k0);
+    load(T_D_KJ, D, k0, J0);
+    __syncthreads();
+    const int kn = min(kDT, nk - k0);
+    for (int kk = 0; kk < kn; ++kk) {
+      // dp[kh = i][ke = j]
+      a1 = ca(a1, cm(tile(T_HHH_IK, ty, kk), tile(T_P_KJ, kk, tx)));
+      a2 = ca(a2, cm(tile(T_HEE_JK, tx, kk), tile(T_P_IK, ty, kk)));
+      a3 = ca(a3, cm(tile(T_HEH_KI, kk, ty), tile(T_C_KJ, kk, tx)));
+      a4 = ca(a4, cm(tile(T_HEH_JK, tx, kk), tile(T_D_KI, kk, ty)));
+      // dC[k1 = i][k2 = j]
+      b1 = ca(b1, cm(tile(T_HEE_JK, tx, kk), tile(T_C_IK, ty, kk)));
+      b2 = ca(b2, cm(tile(T_HEE_KI, kk, ty), tile(T_C_KJ, kk, tx)));
+      b3 = ca(b3, cm(tile(T_HEH_JK, tx, kk), cconj(tile(T_P_KI, kk, ty))));
+      b4 = ca(b4, cm(cconj(tile(T_HEH_IK, ty, kk)), tile(T_P_KJ, kk, tx)));
+      // dD[k1 = i][k2 = j]
+      c1 = ca(c1, cm(tile(T_HHH_JK, tx, kk), tile(T_D_IK, ty, kk)));
+      c2 = ca(c2, cm(tile(T_HHH_KI, kk, ty), tile(T_D_KJ, kk, tx)));
+      c3 = ca(c3, cm(tile(T_HEH_KJ, kk, tx), cconj(tile(T_P_IK, ty, kk))));
+      c4 = ca(c4, cm(cconj(tile(T_HEH_KI, kk, ty)), tile(T_P_JK, tx, kk)));
+    }
+    __syncthreads();
+  }
+  if (i >= nk || j >= nk) return;
+  const int e = i * nk + j;
+  const double hb = s.prm.hbar;
   {
-    double2 t1 = z, t2 = z, t3 = z, t4 = z;
-    for (int k = 0; k < nk; ++k) t1 = ca(t1, cm(Hhh[i * nk + k], p[k * nk + j]));
-    for (int k = 0; k < nk; ++k) t2 = ca(t2, cm(Hee[j * nk + k], p[i * nk + k]));
-    for (int k = 0; k < nk; ++k) t3 = ca(t3, cm(Heh[k * nk + i], C[k * nk + j]));
-    for (int k = 0; k < nk; ++k) t4 = ca(t4, cm(Heh[j * nk + k], D[k * nk + i]));
-    double2 r = cs(cs(ca(t1, t2), t3), t4);
+    double2 r = cs(cs(ca(a1, a2), a3), a4);
     r = ca(r, Heh[j * nk + i]);
     // GamE[ke] + GamH[kh]: the constant rates, or CalcGammaE/H's
     const double g = s.GamE ? s.GamE[j] + s.GamH[i] : s.prm.gam_e + s.prm.gam_h;
@@ -214,24 +271,8 @@ __global__ void derivs_kernel(Step s0) {
     if (s.OffP) r = ca(r, s.OffP[e]);  // + OffP[kh][ke]
     s.dX[e] = div_ih(r, hb);
   }
-  // dC[k1 = i][k2 = j]
-  {
-    double2 t1 = z, t2 = z, t3 = z, t4 = z;
-    for (int k = 0; k < nk; ++k) t1 = ca(t1, cm(Hee[j * nk + k], C[i * nk + k]));
-    for (int k = 0; k < nk; ++k) t2 = ca(t2, cm(Hee[k * nk + i], C[k * nk + j]));
-    for (int k = 0; k < nk; ++k) t3 = ca(t3, cm(Heh[j * nk + k], cconj(p[k * nk + i])));
-    for (int k = 0; k < nk; ++k) t4 = ca(t4, cm(cconj(Heh[i * nk + k]), p[k * nk + j]));
-    s.dX[n2 + e] = div_ih(cs(ca(cs(t1, t2), t3), t4), hb);
-  }
-  // dD[k1 = i][k2 = j]
-  {
-    double2 t1 = z, t2 = z, t3 = z, t4 = z;
-    for (int k = 0; k < nk; ++k) t1 = ca(t1, cm(Hhh[j * nk + k], D[i * nk + k]));
-    for (int k = 0; k < nk; ++k) t2 = ca(t2, cm(Hhh[k * nk + i], D[k * nk + j]));
-    for (int k = 0; k < nk; ++k) t3 = ca(t3, cm(Heh[k * nk + j], cconj(p[i * nk + k])));
-    for (int k = 0; k < nk; ++k) t4 = ca(t4, cm(cconj(Heh[k * nk + i]), p[j * nk + k]));
-    s.dX[2 * n2 + e] = div_ih(cs(ca(cs(t1, t2), t3), t4), hb);
-  }
+  s.dX[n2 + e] = div_ih(cs(ca(cs(b1, b2), b3), b4), hb);
+  s.dX[2 * n2 + e] = div_ih(cs(ca(cs(c1, c2), c3), c4), hb);
 }
 
 // Leapfrog with neutrality and reshuffle (SBEs.py:5681-5718), one CTA.
@@ -486,19 +527,27 @@ __device__ __forceinline__ double lrtz(double a, double b) { return (b / kPi) / 
 // CalcOffDiagDeph_E2 / _H2 (dephasing.py:226-318): De[q + nk][k] and
 // Dh[q + nk][k] for q in [-nk, nk], with |C_kk|, |D_kk| as occupations and
 // Vsq(q) = V(|q|)^2 for 0 < |q| < nk; one thread per (q, k), the partner
-// momentum p in the reference's order, then the factor pi / hbar.
+// momentum p in the reference's order, then the factor pi / hbar.  The
+// occupations and band energies are staged in shared memory per CTA.
 __global__ void mb_offd_kernel(MBView v0) {
   const MBView v = at_wire(v0);
   const int nk = v.nk, n2 = nk * nk;
+  extern __shared__ double osm[];  // [4][nk]: |C_kk|, |D_kk|, Ee, Eh
+  for (int i = threadIdx.x; i < nk; i += blockDim.x) {
+    const double2 c = v.L[n2 + i * nk + i], d = v.L[2 * n2 + i * nk + i];
+    osm[i] = hypot(c.x, c.y);
+    osm[nk + i] = hypot(d.x, d.y);
+    osm[2 * nk + i] = v.Ee[i];
+    osm[3 * nk + i] = v.Eh[i];
+  }
+  __syncthreads();
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= (2 * nk + 1) * nk) return;
   const int qi = e / nk, k = e - qi * nk, q = qi - nk;
-  const double2* C = v.L + n2;
-  const double2* D = v.L + 2 * n2;
-  const double* Ee = v.Ee;
-  const double* Eh = v.Eh;
-  auto ne = [&](int i) { const double2 c = C[i * nk + i]; return hypot(c.x, c.y); };
-  auto nh = [&](int i) { const double2 c = D[i * nk + i]; return hypot(c.x, c.y); };
+  const double* Ee = osm + 2 * nk;
+  const double* Eh = osm + 3 * nk;
+  auto ne = [&](int i) { return osm[i]; };
+  auto nh = [&](int i) { return osm[nk + i]; };
   const int aq = q < 0 ? -q : q;
   auto vsq = [&](int t) {
     const double x = (aq > 0 && aq < nk) ? v.V3[t * nk + aq] : 0.0;
@@ -1129,11 +1178,21 @@ int full_launch(const Launch& a, cudaStream_t st) {
   }
   if (mb && mb->offdiag_dph) {
     const int nd = (2 * nk + 1) * nk;
-    full::mb_offd_kernel<<<dim3((nd + th - 1) / th, nw), th, 0, st>>>(v);
+    full::mb_offd_kernel<<<dim3((nd + th - 1) / th, nw), th, 4 * (size_t)nk * 8, st>>>(v);
     full::mb_offp_kernel<<<bl, th, 0, st>>>(v);
     s.OffP = v.OffP;
   }
-  full::derivs_kernel<<<bl, th, 0, st>>>(s);
+  {
+    static std::once_flag once;
+    static cudaError_t attr = cudaSuccess;
+    std::call_once(once, [] {
+      attr = cudaFuncSetAttribute(full::derivs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)full::kDerivsSmem);
+    });
+    if (attr != cudaSuccess) return set_error(PSB_ERR_CUDA, "derivs_kernel: shared memory");
+    const int nb = (nk + full::kDT - 1) / full::kDT;
+    full::derivs_kernel<<<dim3(nb, nw, nb), full::kDT * full::kDT, full::kDerivsSmem, st>>>(s);
+  }
   if (relax || dct) {
     // X3, its occupations relaxed (SBEs.py:5688-5695) and shifted by the DC
     // field (SBEs.py:5698-5702), then the rescale
