@@ -132,55 +132,80 @@ __device__ __forceinline__ double vq(const double* V, int n, int nk, int q) {
   return (a > 0 && a < nk) ? V[n * nk + a] : 0.0;
 }
 
-// CalcH (SBEs.py:819-935): one thread per (k1, k2).
-__global__ void calch_kernel(Step s0) {
+// CalcH (SBEs.py:819-935): every element (k1, k2) sums along its diagonal
+// d = k1 - k2 of p, C, D (the exchange terms) and, with LF, along the
+// diagonals d and -d of C and D (the direct terms), each in the reference's
+// order.  One CTA per diagonal and wire: the five diagonals it reads are
+// loaded once into shared memory (they are strided in the row-major
+// matrices), then thread t sums for the element at position t.
+constexpr int kHThreads = 128;
+__global__ void __launch_bounds__(kHThreads) calch_kernel(Step s0) {
   const Step s = at_wire(s0);
   const int nk = s.nk, n2 = nk * nk;
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= n2) return;
-  const int k1 = e / nk, k2 = e - k1 * nk;
+  const int d = (int)blockIdx.x - (nk - 1);     // k1 - k2
+  const int ad = d < 0 ? -d : d, len = nk - ad;  // elements on the diagonal
+  const int o1 = d > 0 ? d : 0, o2 = d < 0 ? -d : 0;  // k1 = t + o1, k2 = t + o2
+  extern __shared__ double2 hsm[];  // [5][len]: p, C, D at row - col = -d; C, D at +d
+  double2* pd = hsm;
+  double2* cd = pd + len;
+  double2* dd = cd + len;
+  double2* cm_ = dd + len;
+  double2* dm = cm_ + len;
   const double2* p = s.L3;
   const double2* C = s.L3 + n2;
   const double2* D = s.L3 + 2 * n2;
+  for (int u = threadIdx.x; u < len; u += kHThreads) {
+    // element u of the run: row o2 + u, column o1 + u (col - row = d), and
+    // the mirrored run row o1 + u, column o2 + u
+    const int a = (o2 + u) * nk + (o1 + u), b = (o1 + u) * nk + (o2 + u);
+    pd[u] = p[a];
+    cd[u] = C[a];
+    dd[u] = D[a];
+    cm_[u] = C[b];
+    dm[u] = D[b];
+  }
+  __syncthreads();
   const double* V = s.V3;
-  double2 heh = s.Meh[e];
-  double2 hee = make_double2(0.0, 0.0), hhh = hee;
-  if (k1 == k2) {
-    hee = make_double2(s.Ee[k1] + s.prm.gap, 0.0);
-    hhh = make_double2(s.Eh[k1], 0.0);
-  }
-  if (s.prm.excitons) {
-    const int qmin = max(-k1, -k2), qmax = min(nk - 1 - k1, nk - 1 - k2);
-    // H^eh: sum_q V_eh(q) p^T[k1+q][k2+q]
-    for (int q = qmin; q <= qmax; ++q)
-      if (q != 0) heh = ca(heh, rs(vq(V, 0, nk, q), p[(k2 + q) * nk + (k1 + q)]));
-    if (s.prm.lf) {
-      for (int q = qmin; q <= qmax; ++q)
-        if (q != 0) hee = cs(hee, rs(vq(V, 1, nk, q), C[(k2 + q) * nk + (k1 + q)]));
-      const int qd = k1 - k2;
-      if (qd != 0) {
-        const int kmin = max(0, -qd), kmax = min(nk - 1, nk - 1 - qd);
-        const double v1 = vq(V, 1, nk, qd), v0 = vq(V, 0, nk, qd), v2 = vq(V, 2, nk, qd);
-        for (int k = kmin; k <= kmax; ++k)
-          hee = ca(hee, cs(rs(v1, C[k * nk + k + qd]), rs(v0, D[(k + qd) * nk + k])));
-        for (int q = qmin; q <= qmax; ++q)
-          if (q != 0) hhh = cs(hhh, rs(vq(V, 2, nk, q), D[(k2 + q) * nk + (k1 + q)]));
-        for (int k = kmin; k <= kmax; ++k)
-          hhh = ca(hhh, cs(rs(v2, D[k * nk + k + qd]), rs(v0, C[(k + qd) * nk + k])));
-      } else {
-        for (int q = qmin; q <= qmax; ++q)
-          if (q != 0) hhh = cs(hhh, rs(vq(V, 2, nk, q), D[(k2 + q) * nk + (k1 + q)]));
-      }
-    } else if (k1 == k2) {
-      for (int q = -k1; q <= nk - 1 - k1; ++q)
-        if (q != 0) hee = cs(hee, rs(vq(V, 1, nk, q), C[(k2 + q) * nk + (k1 + q)]));
-      for (int q = -k1; q <= nk - 1 - k1; ++q)
-        if (q != 0) hhh = cs(hhh, rs(vq(V, 2, nk, q), D[(k2 + q) * nk + (k1 + q)]));
+  for (int t = threadIdx.x; t < len; t += kHThreads) {
+    const int k1 = t + o1, k2 = t + o2, e = k1 * nk + k2;
+    double2 heh = s.Meh[e];
+    double2 hee = make_double2(0.0, 0.0), hhh = hee;
+    if (k1 == k2) {
+      hee = make_double2(s.Ee[k1] + s.prm.gap, 0.0);
+      hhh = make_double2(s.Eh[k1], 0.0);
     }
+    if (s.prm.excitons) {
+      // q runs over qmin .. qmax, i.e. positions u = t + q = 0 .. len - 1
+      // H^eh: sum_q V_eh(q) p^T[k1+q][k2+q] = p[k2+q][k1+q]
+      for (int u = 0; u < len; ++u)
+        if (u != t) heh = ca(heh, rs(vq(V, 0, nk, u - t), pd[u]));
+      if (s.prm.lf) {
+        for (int u = 0; u < len; ++u)
+          if (u != t) hee = cs(hee, rs(vq(V, 1, nk, u - t), cd[u]));
+        if (d != 0) {
+          // direct terms: k = kmin .. kmax, C[k][k + d] and D[k + d][k]
+          const double v1 = vq(V, 1, nk, d), v0 = vq(V, 0, nk, d), v2 = vq(V, 2, nk, d);
+          // with k = kmin + u: C[k][k + d] = cd[u], D[k + d][k] = dm[u],
+          // D[k][k + d] = dd[u], C[k + d][k] = cm_[u]
+          for (int u = 0; u < len; ++u) hee = ca(hee, cs(rs(v1, cd[u]), rs(v0, dm[u])));
+          for (int u = 0; u < len; ++u)
+            if (u != t) hhh = cs(hhh, rs(vq(V, 2, nk, u - t), dd[u]));
+          for (int u = 0; u < len; ++u) hhh = ca(hhh, cs(rs(v2, dd[u]), rs(v0, cm_[u])));
+        } else {
+          for (int u = 0; u < len; ++u)
+            if (u != t) hhh = cs(hhh, rs(vq(V, 2, nk, u - t), dd[u]));
+        }
+      } else if (k1 == k2) {
+        for (int u = 0; u < len; ++u)
+          if (u != t) hee = cs(hee, rs(vq(V, 1, nk, u - t), cd[u]));
+        for (int u = 0; u < len; ++u)
+          if (u != t) hhh = cs(hhh, rs(vq(V, 2, nk, u - t), dd[u]));
+      }
+    }
+    s.H[e] = heh;
+    s.H[n2 + e] = hee;
+    s.H[2 * n2 + e] = hhh;
   }
-  s.H[e] = heh;
-  s.H[n2 + e] = hee;
-  s.H[2 * n2 + e] = hhh;
 }
 
 // dpdt / dCdt / dDdt (SBEs.py:1952-1975, 2318-2337, 2617-2636): one thread
@@ -1169,7 +1194,16 @@ int full_launch(const Launch& a, cudaStream_t st) {
   const int th = 128;
   const dim3 bl((n2 + th - 1) / th, nw), blk((nk + th - 1) / th, nw);
   full::meh_kernel<<<bl, th, 0, st>>>(s);
-  full::calch_kernel<<<bl, th, 0, st>>>(s);
+  {
+    static std::once_flag once;
+    static cudaError_t attr = cudaSuccess;
+    std::call_once(once, [] {
+      attr = cudaFuncSetAttribute(full::calch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  5 * PSB_MAX_NK * 16);
+    });
+    if (attr != cudaSuccess) return set_error(PSB_ERR_CUDA, "calch_kernel: shared memory");
+    full::calch_kernel<<<dim3(2 * nk - 1, nw), full::kHThreads, 5 * (size_t)nk * 16, st>>>(s);
+  }
   // dephasing from the level the right-hand side reads (SBEs.py:5225-5232)
   if (mb && mb->diag_dph) {
     full::mb_gamma_kernel<<<blk, th, 0, st>>>(v);
