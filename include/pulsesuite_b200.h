@@ -418,6 +418,18 @@ int psb_full_sources_batch_f64(int nw, int nk, int nr, const double* d_kr, const
                                const double* d_wpar, const double* d_levels, double* d_out,
                                void* stream);
 
+/*
+ * Host function (no device work): m complex signals z0 [m][n0] on grid
+ * x0[n0] resampled onto x1[n1] by their cubic splines, out [m][n1] (0
+ * outside [min x0, max x0]) -- rescale_1D_dpc with spline_dpc / seval_dpc
+ * (spliner.py:153-188, 1287-1396), the resampling inside Prop2QW / QW2Prop
+ * (qwoptics.py:673-812), with numpy's complex arithmetic (the bits of the
+ * numpy restatement in pulsesuite_b200.wirespace).  Complex values are
+ * interleaved (re, im) doubles.
+ */
+int psb_spline_rows_c128(const double* x0, int n0, const double* z0, int m, const double* x1,
+                         int n1, double* out);
+
 /* ---- split-precision tensor-core form (sm_100a tcgen05, kind::i8) --------- */
 /*
  * The batched form of the same RK4 step: per group of wires sharing one k

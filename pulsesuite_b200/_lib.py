@@ -38,6 +38,7 @@ _SIGNATURES = {
     "psb_full_sources_f64": ([i32, i32, vp, vp, vp, f64, f64, f64, f64, vp, vp, vp], i32),
     "psb_full_mb_scratch_bytes": ([i32], i64),
     "psb_full_batch_work_bytes": ([i32, i32], i64),
+    "psb_spline_rows_c128": ([vp, i32, vp, i32, vp, i32, vp], i32),
     "psb_full_step_batch_f64": ([i32, i32, i32, i32, vp, f64, f64, i32, vp, vp, vp, vp, vp, vp,
                                  vp, vp, i64, vp], i32),
     "psb_full_sources_batch_f64": ([i32, i32, i32, vp, vp, vp, f64, f64, vp, vp, vp, vp], i32),

@@ -16,7 +16,7 @@ REPO = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libpulsesuite_b200.so")
 SOURCES = ["capi.cu", "coulomb.cu", "sbe_f64.cu", "sbe_full.cu", "sbe_split.cu",
-           "sbe_split_wire.cu"]
+           "sbe_split_wire.cu", "wirespace_host.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -43,7 +43,10 @@ def up_to_date():
 def build(force=False, verbose=False):
     if not force and up_to_date():
         return LIB
-    cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
+    # host code without fused multiply-adds (wirespace_host.cu reproduces
+    # numpy's complex arithmetic operation by operation)
+    cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler",
+           "-fPIC,-ffp-contract=off",
            "-I", os.path.join(REPO, "include"), "-o", LIB + ".tmp", *sources(), "-lcudart"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")

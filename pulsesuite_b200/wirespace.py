@@ -125,7 +125,27 @@ def _spline(x, y):
 
 def rescale_rows(x0, Z0, x1):
     """Every row of Z0 (m, len(x0)) resampled from grid x0 onto x1 by its
-    cubic spline, (m, len(x1)); 0 outside [min x0, max x0]."""
+    cubic spline, (m, len(x1)); 0 outside [min x0, max x0].  Runs in the
+    library's host code (psb_spline_rows_c128: the same operations as
+    rescale_rows_numpy, the same bits)."""
+    from . import _lib
+
+    x0 = np.ascontiguousarray(x0, dtype=np.float64)
+    x1 = np.ascontiguousarray(x1, dtype=np.float64)
+    Z0 = np.ascontiguousarray(Z0, dtype=np.complex128)
+    if Z0.ndim != 2 or Z0.shape[-1] != len(x0):
+        raise ValueError("Bad sizes in rescale_1D_dpc")
+    if len(x0) < 2:
+        raise ValueError("Not enough points to spline.")
+    out = np.empty((Z0.shape[0], len(x1)), np.complex128)
+    _lib.call("psb_spline_rows_c128", x0.ctypes.data, len(x0), Z0.ctypes.data, Z0.shape[0],
+              x1.ctypes.data, len(x1), out.ctypes.data)
+    return out
+
+
+def rescale_rows_numpy(x0, Z0, x1):
+    """rescale_rows restated in numpy (the arithmetic psb_spline_rows_c128
+    reproduces)."""
     x0 = np.asarray(x0, dtype=np.float64)
     Z0 = np.asarray(Z0, dtype=np.complex128)
     if Z0.shape[-1] != len(x0):
@@ -178,6 +198,19 @@ def rho_post(re, rh, ne, nh, dr):
         fftg(a)
 
 
+def rho_post_rows(A, N, dr):
+    """rho_post of many densities at once: rows of A (m, nr) with the
+    occupations N (m, nk) they are normalised to; in place.  Each row's sums
+    run over its own contiguous data (numpy's per-row reduction), so every
+    row gets the bits of its own rho_post call."""
+    nr = A.shape[-1]
+    tot = np.sum(np.abs(N), axis=-1) + 1e-50
+    A[...] = A - (np.real(np.sum(A[:, 0:10], axis=-1) + np.sum(A[:, nr - 10:nr], axis=-1))
+                  / 20.0)[:, None]
+    A[...] = A * tot[:, None] / (np.sum(np.abs(A), axis=-1) * dr + QW_SMALL)[:, None]
+    fftg(A)
+
+
 def qw2prop_rows(r, S, RR, plasmonics):
     """qw2prop of m wires at once: S (m, 5, len(r)) wire-space q-space
     sources Px, Py, Pz, re, rh (modified in place) -> (m, 5, len(RR))
@@ -188,23 +221,18 @@ def qw2prop_rows(r, S, RR, plasmonics):
     dRR = RR[1] - RR[0]
     m = S.shape[0]
     ifftg(S)
-    totals = None
+    total = None
     if plasmonics:
-        totals = []
-        for j in range(m):
-            re, rh = S[j, 3], S[j, 4]
-            re[:] = np.abs(re)
-            rh[:] = np.abs(rh)
-            total = (np.sum(re) * dr + np.sum(rh) * dr + QW_SMALL) / 2.0
-            re[:] = re * total / (np.sum(re) * dr + QW_SMALL)
-            rh[:] = rh * total / (np.sum(rh) * dr + QW_SMALL)
-            totals.append(total)
+        # complex arithmetic throughout, as on the reference's complex arrays:
+        # |x| stored as (|x|, 0), sums and divisions in complex128
+        D = np.abs(S[:, 3:5]).astype(np.complex128)   # [m][2][nr], each row contiguous
+        sums = np.sum(D, axis=-1)                     # per wire and density
+        total = (sums[:, 0] * dr + sums[:, 1] * dr + QW_SMALL) / 2.0
+        S[:, 3:5] = D * total[:, None, None] / (sums * dr + QW_SMALL)[:, :, None]
     out = rescale_rows(r, S.reshape(5 * m, -1), RR).reshape(m, 5, -1)
     if plasmonics:
-        for j in range(m):
-            for k in (3, 4):
-                a = np.abs(out[j, k]).astype(np.complex128)
-                out[j, k] = a * totals[j] / (np.sum(a) * dRR + QW_SMALL)
+        D = np.abs(out[:, 3:5]).astype(np.complex128)
+        out[:, 3:5] = D * total[:, None, None] / (np.sum(D, axis=-1) * dRR + QW_SMALL)[:, :, None]
     return out
 
 

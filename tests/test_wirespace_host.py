@@ -47,3 +47,32 @@ def test_row_versions_equal_one_signal_calls():
             one = ws.qw2prop(r, *a, RR, plasmonics)
             for k in range(5):
                 np.testing.assert_array_equal(got[j, k], one[k])
+
+
+def test_library_spline_equals_numpy_restatement():
+    """psb_spline_rows_c128 (host code of the library, used by rescale_rows)
+    gives the bits of the numpy restatement, down to two-point grids."""
+    rng = np.random.default_rng(12)
+    for n0, n1 in ((64, 230), (230, 64), (7, 20), (4, 9), (3, 5), (2, 4)):
+        if n0 > 7:
+            x0, x1 = np.linspace(-5e-8, 5e-8, n0), np.linspace(-6e-8, 6e-8, n1)
+        else:
+            x0, x1 = np.sort(rng.uniform(-1, 1, n0)), np.linspace(-1.2, 1.2, n1)
+        Z = rng.standard_normal((9, n0)) + 1j * rng.standard_normal((9, n0))
+        Z *= 10.0 ** rng.integers(-8, 9, (9, 1))
+        Z[2] = Z[2].real
+        np.testing.assert_array_equal(ws.rescale_rows(x0, Z, x1),
+                                      ws.rescale_rows_numpy(x0, Z, x1))
+
+
+def test_rho_post_rows_equals_one_wire_calls():
+    rng = np.random.default_rng(13)
+    A = rng.standard_normal((6, 230)) + 1j * rng.standard_normal((6, 230))
+    N = rng.uniform(0, 1, (6, 114)) + 1j * rng.standard_normal((6, 114)) * 1e-3
+    got = A.copy()
+    ws.rho_post_rows(got, N, 5e-10)
+    for j in range(0, 6, 2):
+        re, rh = A[j].copy(), A[j + 1].copy()
+        ws.rho_post(re, rh, N[j], N[j + 1], 5e-10)
+        np.testing.assert_array_equal(got[j], re)
+        np.testing.assert_array_equal(got[j + 1], rh)
