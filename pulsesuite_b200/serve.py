@@ -553,10 +553,17 @@ class Server:
                 # finish with the next tick: its end is the tick boundary
                 self.steps_req[g] = min(self.steps_req[g], self.steps_done[g] + self.chunk)
 
-    def run(self, requests, realtime=True, max_inflight_ticks=None, cancels=()):
+    def run(self, requests, realtime=True, max_inflight_ticks=None, cancels=(),
+            longest_first=None):
         """Serve ``requests``.  realtime: arrivals are honoured on the wall
         clock (the Poisson stream), else every request is available from the
         start (throughput / capacity runs).
+
+        longest_first (default: not realtime): each size class admits its
+        waiting solves longest first instead of in arrival order -- for a
+        backlog this shortens the tail in which the last long solves run
+        with few slots busy (longest-processing-time-first scheduling).  A
+        solve's result does not depend on when it is admitted.
 
         Each size class ticks on its own stream as soon as its previous
         ticks allow (at most ``max_inflight_ticks`` queued), so a small
@@ -568,6 +575,8 @@ class Server:
         is applied, as a client withdrawing a request would."""
         if max_inflight_ticks is None:
             max_inflight_ticks = self.max_inflight
+        if longest_first is None:
+            longest_first = not realtime
         assert max_inflight_ticks < self.ring
         queue = sorted(requests, key=lambda r: r.arrival)
         for req in queue:
@@ -584,9 +593,15 @@ class Server:
         self.t_start = time.perf_counter()
         while len(self.results) < n:
             now = time.perf_counter() - self.t_start
+            arrived = qi
             while qi < n and (not realtime or queue[qi].arrival <= now):
                 by_nk[queue[qi].nk].waiting.append(queue[qi])
                 qi += 1
+            if longest_first and qi > arrived:
+                for lane in self.lanes:
+                    if len(lane.waiting) > 1:
+                        lane.waiting = collections.deque(
+                            sorted(lane.waiting, key=lambda r: -r.nsteps))
             while ci < len(cq) and cq[ci][0] <= now:
                 self.cancel(cq[ci][1])
                 ci += 1
