@@ -827,17 +827,24 @@ def serve_section(a, rank, world):
     # the capacity runs queue up to 4 ticks per lane (throughput: the host
     # loop stays ahead of the GPU); the real-time runs keep the default 2
     # (latency: a new request waits behind fewer queued ticks)
-    for form in ("split", "plain"):
+    # the saturated capacity varies by ~10 % from run to run (host loop and
+    # stream interleaving): the split form's is the median of three runs of
+    # the same backlog, all three listed; the plain form's (12 s a run) one
+    for form, reps in (("split", 3), ("plain", 1)):
         srv = serve.Server(form=form, chunk=chunk, max_inflight_ticks=4)
         srv.run(warm, realtime=False)
-        srv.reset_counters()
-        res = srv.run(sat, realtime=False)
-        ok = all(r.status == 0 for r in res)
-        out["capacity"][form] = {"value": srv.throughput(), "seconds": srv.elapsed,
-                                 "requests": len(res), "ticks": srv.tick_count,
-                                 "ticks_in_flight_per_lane": 4,
-                                 "h2d_bytes": srv.h2d_bytes, "d2h_bytes": srv.d2h_bytes,
-                                 "status_ok": ok}
+        runs = []
+        for _ in range(reps):
+            srv.reset_counters()
+            res = srv.run(sat, realtime=False)
+            ok = all(r.status == 0 for r in res)
+            runs.append({"value": srv.throughput(), "seconds": srv.elapsed,
+                         "requests": len(res), "ticks": srv.tick_count,
+                         "ticks_in_flight_per_lane": 4, "h2d_bytes": srv.h2d_bytes,
+                         "d2h_bytes": srv.d2h_bytes, "status_ok": ok})
+        best = sorted(runs, key=lambda r: r["value"])[len(runs) // 2]
+        out["capacity"][form] = dict(best, runs=[r["value"] for r in runs],
+                                     status_ok=all(r["status_ok"] for r in runs))
         del srv
         torch.cuda.synchronize()
     for form, secs in (("split", a.serve_seconds), ("plain", a.plain_serve_seconds)):
