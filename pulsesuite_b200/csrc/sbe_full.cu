@@ -880,34 +880,69 @@ __global__ void mb_shift_kernel(MBView v0) {
   v.shift[d] = make_double2(re / nk, im / nk);
 }
 
-// T[x][a][j] = sum_b X3[x][a][b] s[(j - b) mod nk], one thread per (x, a, j)
-__global__ void mb_shift_rows_kernel(MBView v0) {
+// The two circulant products of the shift, tiled: one CTA per kST x kST
+// block of one matrix (x) of one wire; per chunk of kST summation indices
+// the block's operand tile and the 2 kST - 1 coefficients s[(j - b) mod nk]
+// it needs sit in shared memory.  Each element sums in the old order (the
+// summation index ascending).
+constexpr int kST = 16;
+
+// T[x][a][j] = sum_b X3[x][a][b] s[(j - b) mod nk]
+__global__ void __launch_bounds__(kST* kST) mb_shift_rows_kernel(MBView v0) {
   const MBView v = at_wire(v0);
-  const int nk = v.nk, n2 = nk * nk, e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= 3 * n2) return;
-  const int j = e % nk;
-  const double2* row = v.X3 + (e - j);
+  const int nk = v.nk, n2 = nk * nk, nb = (nk + kST - 1) / kST;
+  const int x = blockIdx.x / (nb * nb), t = blockIdx.x % (nb * nb);
+  const int A0 = (t / nb) * kST, J0 = (t % nb) * kST;
+  const int tx = threadIdx.x % kST, ty = threadIdx.x / kST;
+  __shared__ double2 xt[kST][kST + 1];
+  __shared__ double2 sv[2 * kST - 1];
+  const double2* X = v.X3 + (size_t)x * n2;
+  const int a = A0 + ty, j = J0 + tx;
   double2 acc = make_double2(0.0, 0.0);
-  for (int b = 0; b < nk; ++b) {
-    const int d = j - b < 0 ? j - b + nk : j - b;
-    acc = ca(acc, cm(row[b], v.shift[d]));
+  for (int b0 = 0; b0 < nk; b0 += kST) {
+    const int r = A0 + ty, c = b0 + tx;
+    xt[ty][tx] = (r < nk && c < nk) ? X[r * nk + c] : make_double2(0.0, 0.0);
+    if (threadIdx.x < 2 * kST - 1) {
+      // sv[u] = s[(J0 - b0 - (kST - 1) + u) mod nk]
+      int d = (J0 - b0 - (kST - 1) + (int)threadIdx.x) % nk;
+      if (d < 0) d += nk;
+      sv[threadIdx.x] = v.shift[d];
+    }
+    __syncthreads();
+    const int bn = min(kST, nk - b0);
+    for (int bb = 0; bb < bn; ++bb) acc = ca(acc, cm(xt[ty][bb], sv[tx - bb + kST - 1]));
+    __syncthreads();
   }
-  v.tr[e] = acc;
+  if (a < nk && j < nk) v.tr[(size_t)x * n2 + a * nk + j] = acc;
 }
 
 // X3[x][i][j] = sum_a s[(i - a) mod nk] T[x][a][j]
-__global__ void mb_shift_cols_kernel(MBView v0) {
+__global__ void __launch_bounds__(kST* kST) mb_shift_cols_kernel(MBView v0) {
   const MBView v = at_wire(v0);
-  const int nk = v.nk, n2 = nk * nk, e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= 3 * n2) return;
-  const int x = e / n2, i = (e % n2) / nk, j = e % nk;
-  const double2* col = v.tr + (size_t)x * n2 + j;
+  const int nk = v.nk, n2 = nk * nk, nb = (nk + kST - 1) / kST;
+  const int x = blockIdx.x / (nb * nb), t = blockIdx.x % (nb * nb);
+  const int I0 = (t / nb) * kST, J0 = (t % nb) * kST;
+  const int tx = threadIdx.x % kST, ty = threadIdx.x / kST;
+  __shared__ double2 tt[kST][kST + 1];
+  __shared__ double2 sv[2 * kST - 1];
+  const double2* T = v.tr + (size_t)x * n2;
+  const int i = I0 + ty, j = J0 + tx;
   double2 acc = make_double2(0.0, 0.0);
-  for (int a = 0; a < nk; ++a) {
-    const int d = i - a < 0 ? i - a + nk : i - a;
-    acc = ca(acc, cm(v.shift[d], col[(size_t)a * nk]));
+  for (int a0 = 0; a0 < nk; a0 += kST) {
+    const int r = a0 + ty, c = J0 + tx;
+    tt[ty][tx] = (r < nk && c < nk) ? T[r * nk + c] : make_double2(0.0, 0.0);
+    if (threadIdx.x < 2 * kST - 1) {
+      // sv[u] = s[(I0 - a0 - (kST - 1) + u) mod nk]
+      int d = (I0 - a0 - (kST - 1) + (int)threadIdx.x) % nk;
+      if (d < 0) d += nk;
+      sv[threadIdx.x] = v.shift[d];
+    }
+    __syncthreads();
+    const int an = min(kST, nk - a0);
+    for (int aa = 0; aa < an; ++aa) acc = ca(acc, cm(sv[ty - aa + kST - 1], tt[aa][tx]));
+    __syncthreads();
   }
-  v.X3[e] = acc;
+  if (i < nk && j < nk) v.X3[(size_t)x * n2 + i * nk + j] = acc;
 }
 
 // without lf only the diagonals move: T[x][a] = sum_n s[(a - n) mod nk] X3[x][n][n]
@@ -1240,8 +1275,10 @@ int full_launch(const Launch& a, cudaStream_t st) {
     if (dct) {
       full::mb_shift_kernel<<<blk, th, 0, st>>>(v);
       if (a.params->lf) {
-        full::mb_shift_rows_kernel<<<b3, th, 0, st>>>(v);
-        full::mb_shift_cols_kernel<<<b3, th, 0, st>>>(v);
+        const int nb = (nk + full::kST - 1) / full::kST;
+        const dim3 bt(3 * nb * nb, nw);
+        full::mb_shift_rows_kernel<<<bt, full::kST * full::kST, 0, st>>>(v);
+        full::mb_shift_cols_kernel<<<bt, full::kST * full::kST, 0, st>>>(v);
       } else {
         const dim3 bd((3 * nk + th - 1) / th, nw);
         full::mb_shift_diag_kernel<<<bd, th, 0, st>>>(v);
