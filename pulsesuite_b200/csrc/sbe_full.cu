@@ -716,6 +716,9 @@ __global__ void __launch_bounds__(kRateThreads) mb_rates_kernel(MBView v0) {
   double acc[4] = {0.0, 0.0, 0.0, 0.0};  // WinE, WoutE, WinH, WoutH
   if (v.mb.ehs) {
     const int k = k0 + 1;  // MBCE: k; MBCH: kp
+    // two q1 per iteration keep twice the C reads in flight (each
+    // accumulator still adds in q1 order)
+#pragma unroll 2
     for (int q1 = 1; q1 <= nk; ++q1) {
       for (int q2 = threadIdx.x + 1; q2 <= nk; q2 += kRateThreads) {
         {  // electrons (MBCE)

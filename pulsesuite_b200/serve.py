@@ -228,6 +228,7 @@ class Server:
             base += cap[nk]
             off += cap[nk] * nk
         self.nslots = base
+        self.slot_off_arr = np.asarray(self.slot_off, dtype=np.int64)
         self.n_state = off
         w = np.zeros(self.nslots, dtype=abi.WIRE_DTYPE)
         for ti, nk in enumerate(self.nks):
@@ -284,7 +285,8 @@ class Server:
         self.steps_done = np.zeros(self.nslots, dtype=np.int64)  # per slot, of its solve
         self.steps_req = np.zeros(self.nslots, dtype=np.int64)
         self._ar = {nk: torch.arange(nk, dtype=torch.int64, device="cuda") for nk in self.nks}
-        self.pending = []  # retiring batches: (event, entries, host buffers)
+        self.pending = []  # retiring batches: (event, entries, host views, pinned buffer)
+        self._pin_free = []  # pinned host buffers whose contents were collected
         self.results = []
         # launch arguments that do not change between ticks
         self._common = (device.ptr(self.d_tables), len(self.h_tables), device.ptr(self.tabdata),
@@ -364,30 +366,32 @@ class Server:
         """Admit as many of the lane's waiting requests as slots and budget
         allow; returns the staged admission or None.  Their wire descriptors
         and zeroed state reach the device with this tick's staged copy."""
-        recs, slots = [], []
+        reqs, slots = [], []
         while lane.waiting:
             req = lane.waiting[0]
             nbytes = request_bytes(req.nk, req.nsteps, self.form)
             sl = self.pool.try_take(req.nk, nbytes)
             if sl is None:
-                break  # first come, first served within the class
+                break  # the class's slots or the byte budget are used up
             lane.waiting.popleft()
             g = self.cls_base[req.nk] + sl
-            rec = wire_record(req, self.grids[lane.ti], table=lane.ti, off=self.slot_off[g],
-                              p_off=g * self.max_steps)
-            self.h_wires[g] = rec[0]
-            recs.append(rec)
+            reqs.append(req)
             slots.append(g)
             self.active[g] = [req, 0, now, nbytes]
-            self.steps_done[g] = 0
-            self.steps_req[g] = req.nsteps
             lane.mask[sl] = True
-            lane.nactive += 1
         if not slots:
             return None
-        return (st.add(np.concatenate(recs)), st.add(np.asarray(slots, dtype=np.int64)),
-                st.add(np.asarray([self.slot_off[g] for g in slots], dtype=np.int64)),
-                len(slots))
+        # the descriptors of every admitted solve in one pass (the same
+        # values wire_record gives one request)
+        g = np.asarray(slots, dtype=np.int64)
+        offs = self.slot_off_arr[g]
+        recs = wire_records(reqs, self.grids[lane.ti], table=lane.ti, offs=offs,
+                            p_offs=g * self.max_steps)
+        self.h_wires[g] = recs
+        self.steps_done[g] = 0
+        self.steps_req[g] = [r.nsteps for r in reqs]
+        lane.nactive += len(slots)
+        return st.add(recs), st.add(g), st.add(offs), len(slots)
 
     def _tick(self, lane, now):
         """Admit, advance and retire one size class by ``chunk`` steps, all
@@ -407,7 +411,7 @@ class Server:
         r_fin = r_foff = None
         if fin.size:
             r_fin = st.add(fin)
-            r_foff = st.add(np.asarray([self.slot_off[g] for g in fin], dtype=np.int64))
+            r_foff = st.add(self.slot_off_arr[fin])
         nk, ti = lane.nk, lane.ti
         if self.form == "split":
             # the classes share the SMs, so the choice sees every lane's load
@@ -476,17 +480,23 @@ class Server:
         lane.mask[fin - lane.base] = False
         lane.nactive -= len(fin)
         rows = self._rows(foff_t, lane.nk)
-        Pg = self.P.view(self.nslots, self.max_steps, 2).index_select(0, fin_t)
+        # P(t) records up to the longest of these solves, not max_steps
+        smax = max(e[1].nsteps for e in entries)
+        Pg = self.P.view(self.nslots, self.max_steps, 2)[:, :smax].index_select(0, fin_t)
         yg = self.y.index_select(0, rows)
         wgr = self._wires_rows.index_select(0, fin_t)
         ev0 = torch.cuda.Event()
         ev0.record(torch.cuda.current_stream())
         cs = self.copy_stream
         cs.wait_event(ev0)
+        # one pinned buffer from the pool for the three copies
+        nP, ny = Pg.numel() * 8, yg.numel() * 8
+        nbuf = nP + ny + wgr.numel()
+        hbuf = self._pinned(nbuf)
+        hP = hbuf[:nP].view(torch.float64).view(Pg.shape)
+        hy = hbuf[nP:nP + ny].view(torch.float64).view(yg.shape)
+        hw = hbuf[nP + ny:nbuf].view(wgr.shape)
         with torch.cuda.stream(cs):
-            hP = torch.empty(Pg.shape, dtype=torch.float64, pin_memory=True)
-            hy = torch.empty(yg.shape, dtype=torch.float64, pin_memory=True)
-            hw = torch.empty(wgr.shape, dtype=torch.uint8, pin_memory=True)
             hP.copy_(Pg, non_blocking=True)
             hy.copy_(yg, non_blocking=True)
             hw.copy_(wgr, non_blocking=True)
@@ -496,30 +506,45 @@ class Server:
             ev = torch.cuda.Event()
             ev.record(cs)
         self.d2h_bytes += (hP.numel() + hy.numel()) * 8 + hw.numel()
-        self.pending.append((ev, entries, hP, hy, hw))
+        self.pending.append((ev, entries, (hP, hy, hw), hbuf))
+
+    def _pinned(self, nbytes):
+        """A pinned host byte buffer of at least nbytes: a collected one from
+        the pool when one fits (at most 4x larger), else a new one of the
+        next power of two (>= 1 MiB).  Sizes are multiples of 8, so float64
+        views at 8-byte offsets stay aligned."""
+        for i, buf in enumerate(self._pin_free):
+            if nbytes <= buf.numel() <= 4 * max(nbytes, 1 << 20):
+                return self._pin_free.pop(i)
+        size = 1 << max(20, (int(nbytes) - 1).bit_length())
+        return self.torch.empty(size, dtype=self.torch.uint8, pin_memory=True)
 
     def _collect(self, block=False):
         keep = []
         for item in self.pending:
-            ev, entries, hP, hy, hw = item
+            ev, entries, (hP, hy, hw), hbuf = item
             if block:
                 ev.synchronize()
             elif not ev.query():
                 keep.append(item)
                 continue
             now = time.perf_counter() - self.t_start
-            P, Y = hP.numpy(), hy.numpy()
-            W = hw.numpy().reshape(-1).view(abi.WIRE_DTYPE)
+            # one copy of each block out of the pinned buffer, which goes
+            # back to the pool; every result is a view into these copies
+            P, Y = hP.numpy().copy(), hy.numpy().copy()
+            W = hw.numpy().reshape(-1).view(abi.WIRE_DTYPE).copy()
+            self._pin_free.append(hbuf)
+            st_all = W["status"].astype(np.int64)
             o = 0
             for i, (g, req, done, admitted, nbytes) in enumerate(entries):
-                status, nsteps = int(W["status"][i]), req.nsteps
+                status, nsteps = int(st_all[i]), req.nsteps
                 if req.rid in self._cancelled:
                     self._cancelled.discard(req.rid)
                     status, nsteps = STATUS_CANCELLED, min(req.nsteps, int(done))
-                p = P[i, :nsteps]
+                # P(t) rows (re, im) viewed as complex128
+                p = P[i, :nsteps].view(np.complex128).reshape(-1)
                 self.results.append(Result(req.rid, req.nk, nsteps, req.arrival, admitted, now,
-                                           status, p[:, 0] + 1j * p[:, 1],
-                                           Y[o:o + req.nk].copy()))
+                                           status, p, Y[o:o + req.nk]))
                 o += req.nk
                 self.pool.give_back(req.nk, g - self.cls_base[req.nk], nbytes)
         self.pending = keep
@@ -636,6 +661,32 @@ class Server:
         """Completed wire*k*steps per second of the run."""
         work = sum(r.nk * r.nsteps for r in self.results)
         return work / self.elapsed if self.elapsed > 0 else 0.0
+
+
+def wire_records(reqs, grid, table=0, offs=0, p_offs=0):
+    """wire_record of many requests at once (elementwise the same arithmetic,
+    so each record has the bits wire_record gives it)."""
+    n = len(reqs)
+    rec = np.zeros(n, dtype=abi.WIRE_DTYPE)
+    det = np.array([r.det_eV for r in reqs], dtype=np.float64)
+    T2 = np.array([r.T2 for r in reqs], dtype=np.float64)
+    theta = np.array([r.theta for r in reqs], dtype=np.float64)
+    fwhm = np.array([r.fwhm for r in reqs], dtype=np.float64)
+    mscale = grid.ehint * grid.dcv / 2.0
+    rec["table"] = table
+    rec["npulse"] = 1
+    rec["off"] = offs
+    rec["gap"] = -det * EV
+    rec["gamma"] = 1.0 / T2
+    rec["mscale"] = mscale
+    rec["pscale"] = grid.pscale
+    from .grid import gaussian_amplitude
+
+    rec["amp"][:, 0] = gaussian_amplitude(theta, fwhm, mscale)
+    rec["t0"][:, 0] = 3.0 * fwhm
+    rec["fwhm"][:, :] = fwhm[:, None]
+    rec["p_off"] = p_offs
+    return rec
 
 
 def wire_record(req, grid, table=0, off=0, p_off=0):
