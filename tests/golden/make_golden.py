@@ -3,8 +3,9 @@
 Run in a container that holds the reference source (default
 /root/reference/src, override with PULSESUITE_REF_SRC):
 
-    python tests/golden/make_golden.py            # small cases (a minute)
+    python tests/golden/make_golden.py            # small cases (a few minutes)
     python tests/golden/make_golden.py --full-c0  # + the 4000-step Nk=128 RK4 run (~10 min)
+    python tests/golden/make_golden.py --only manybody,transport   # selected groups
 
 The reference does not import cleanly in this image, so three shims are set
 up first, exactly the minimum needed:
@@ -26,7 +27,12 @@ Cases (all stored as .npz next to this script):
                   (rotating-frame drive, the benchmark configurations' physics)
   leapfrog_*.npz  SBESolver._sbe_calculator, the reference's own driver
   solver_*.npz    the SBESolver API with LF on: source terms, levels, backup files
-  qwcalc_*.npz    QWCalculator driven by propagation-space fields (full-matrix state)
+  qwcalc_*.npz    QWCalculator driven by propagation-space fields (full-matrix state),
+                  plain, with DiagDph/OffDiagDph/EHs/Phonon (qwcalc_manybody_*), and
+                  with Recomb and DCTrans in a DC field, LF on and off (qwcalc_mb_dc_*)
+  manybody_units_nk32.npz  the many-body functions (CalcGammaE/H, OffDiagDephasing2,
+                  MBCE/MBCH, MBPE/MBPH, SpontEmission) on random levels, and the
+                  emission / DC host tables of the reference's modules
 """
 
 import argparse
