@@ -18,10 +18,11 @@ freepot)``); the module-level calls read them from module state, set here by
 The exchange sums over k' (the O(Nk^2) part) run in the sm_100a FP64 kernel
 through ``psb_calch_f64``; the O(Nk) elementwise derivatives in one launch of
 ``psb_diag_derivs_f64``.  Arrays may be numpy arrays or tensors; results come
-back as numpy (in place for CalcH, as the reference does).  Off-diagonal
-states (a k-dependent field along the wire) need the full-matrix right-hand
-side, which this package does not provide: such inputs raise
-NotImplementedError.
+back as numpy (in place for CalcH, as the reference does).  These module
+functions take diagonal states only: an off-diagonal state (a k-dependent
+field along the wire) raises NotImplementedError here; its full-matrix
+right-hand side runs inside ``SBESolver`` (psb_full_step_f64 and the batched
+psb_full_step_batch_f64), which moves to it by itself.
 
 For time integration use ``batch.WireBatch`` (RK4 or the reference's
 leapfrog over many wires); these functions exist for callers that step the
@@ -61,8 +62,8 @@ def _diag_of(name, m, tol=0.0):
     d = np.diag(m)
     off = m - np.diag(d)
     if np.max(np.abs(off), initial=0.0) > tol * max(1.0, np.max(np.abs(d), initial=0.0)):
-        raise NotImplementedError(f"{name} is not diagonal in k: the full-matrix SBE "
-                                  "right-hand side is not provided by pulsesuite_b200")
+        raise NotImplementedError(f"{name} is not diagonal in k: these module functions take "
+                                  "diagonal states; SBESolver steps full-matrix states")
     return d
 
 
