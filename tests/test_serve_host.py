@@ -57,3 +57,18 @@ def test_wires_per_cta_choice():
     assert serve.choose_wires_per_cta({}, 148) == {}
     # the cost model scales unlisted sizes by Nk^2 from the nearest entry
     assert abs(serve.split_cta_cost(2048, 4) - 4 * serve.SPLIT_CTA_MS[(1024, 4)]) < 1e-12
+
+
+def test_wire_records_equal_one_request_records():
+    """Admission builds a tick's descriptors in one pass (wire_records); each
+    record has the bytes wire_record gives its request alone."""
+    from pulsesuite_b200 import grid as pgrid
+
+    reqs = serve.poisson_stream(rate=2000.0, seconds=0.3, seed=11, chunk=50)
+    g = pgrid.wire_grid(128)
+    offs = np.arange(len(reqs), dtype=np.int64) * 128
+    p_offs = np.arange(len(reqs), dtype=np.int64) * 4000
+    batch = serve.wire_records(reqs, g, table=1, offs=offs, p_offs=p_offs)
+    one = np.concatenate([serve.wire_record(r, g, table=1, off=int(o), p_off=int(p))
+                          for r, o, p in zip(reqs, offs, p_offs)])
+    assert batch.dtype == one.dtype and batch.tobytes() == one.tobytes()
